@@ -1,0 +1,346 @@
+"""Benchmark: Mpaths/s of the path-tracing hot path at 1080p.
+
+One step = one frame of the large plain render: 1920x1080, 16 spp, depth 8,
+64 instances of a 158,420-triangle displaced sphere (10.14M triangles, a
+649 MB flattened BVH), 8 procedural 2048^2 textures, GGX / dielectric /
+Lambert materials and an environment light with a sun lobe.  The frame is
+PathTracer::execute (wavefront: generate, extend, shade, shadow, finalize)
+followed by the fused reduce + accumulate + tonemap resolve.  Synthetic,
+seeded inputs stand in for the reference's USD scenes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl strelka|reference]
+
+N > 1 runs under torchrun, one rank per GPU: every rank renders its own
+frames (distinct sample seeds) of the same scene, so per-GPU work is fixed
+(weak scaling) and there is no collective on the data path.  Rank 0 prints
+one JSON line.
+
+--impl reference times the reference's algorithm on the host cores: the
+oracle's C restatement of the shaders (the reference's HLSL cannot run here:
+there is no Vulkan device or software renderer), all host threads, on a
+bounded sample of each frame's paths.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Mpaths/s at 1080p"
+UNIT = "Mpaths/s"
+
+
+def workload_config(args):
+    return {
+        "workload": "large plain render: 1920x1080, 16 spp, depth 8, 64 instances x 158,420-tri displaced sphere "
+                    "(10.14M tris), 8x 2048^2 RGBA8 textures, GGX/dielectric/Lambert, 1024x512 HDR env with sun lobe",
+        "width": args.width, "height": args.height, "spp": args.spp, "max_depth": args.depth,
+        "instances": args.instances, "triangles": None, "mode": args.mode,
+        "l2": "inputs larger than L2 (649 MB BVH, 128 MB textures per frame)",
+    }
+
+
+def make_scene(args):
+    from strelka_b200 import scenes
+
+    return scenes.large(width=args.width, height=args.height, instances=args.instances, frequency=args.frequency,
+                        num_textures=8, tex_size=2048, env_width=1024, env_height=512, max_depth=args.depth,
+                        spp=args.spp, seed=0)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.strip().split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for k, name in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(hs, args, budget_s: float):
+    """Times the oracle (fast build, all host threads) on evenly spread slices
+    of the frame's sample indices; returns Mpaths/s and the sample size."""
+    import oracle
+
+    view = oracle.SceneView(hs)
+    p = hs.param(frameNumber=0)
+    total = args.width * args.height * args.spp
+    threads = os.cpu_count() or 1
+    slices = 64
+    per = 64
+    oracle.pathtrace(view, p, threads=threads, first=0, count=per, fast=True)  # warm-up
+    t0 = time.perf_counter()
+    done = 0
+    while True:
+        for k in range(slices):
+            first = (k * total) // slices
+            oracle.pathtrace(view, p, threads=threads, first=first, count=per, fast=True)
+            done += per
+        el = time.perf_counter() - t0
+        if el > budget_s or done >= total:
+            break
+        per = min(per * 2, total // slices)
+    return done / el / 1e6, done, threads, el
+
+
+def run_reference(args):
+    """--impl reference: rank 0 times the oracle on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    hs = make_scene(args)
+    vals = []
+    for step in range(args.warmup + args.steps):
+        v, n, threads, el = cpu_baseline(hs, args, budget_s=args.ref_step_seconds)
+        if step >= args.warmup:
+            vals.append((v, n, el))
+    value = statistics.median(v for v, _, _ in vals)
+    n = vals[-1][1]
+    cfg = workload_config(args)
+    cfg["triangles"] = hs.num_triangles
+    cfg["parallelism"] = "host cores"
+    sample = (f"{n} paths per step in 64 evenly spaced slices of the frame's {args.width * args.height * args.spp} "
+              f"sample indices, oracle C restatement (-O3 -ffp-contract=fast), OpenMP")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(el for _, _, el in vals),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="strelka", choices=["strelka", "reference"])
+    ap.add_argument("--mode", default="wavefront", choices=["wavefront", "megakernel"])
+    ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--spp", type=int, default=16)
+    ap.add_argument("--depth", type=int, default=8)
+    ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--frequency", type=int, default=89)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--ref-step-seconds", type=float, default=4.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "strelka" else args.warmup
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    from strelka_b200 import abi
+    from strelka_b200.render import DeviceScene, PathTracer, accumulation_param, resolve, tonemap_param
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    hs = make_scene(args)
+    ds = DeviceScene(hs)
+    W, H, S = args.width, args.height, args.spp
+    total = W * H * S
+    mode = abi.MODE_WAVEFRONT if args.mode == "wavefront" else abi.MODE_MEGAKERNEL
+    pt = PathTracer(mode=mode, chunk_paths=args.chunk, profile=True)
+    sb = torch.empty(total * 3, dtype=torch.float32, device="cuda")
+    hist = torch.zeros(W * H * 4, dtype=torch.float32, device="cuda")
+    acc = torch.zeros(W * H * 4, dtype=torch.float32, device="cuda")
+    rgba8 = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
+    tp = tonemap_param(W, H, 1)
+    stream = torch.cuda.current_stream()
+
+    def frame(it):
+        # PtRender::drawFrame (src/render/ptrender.cpp:735-862) for one view
+        p = hs.param(frameNumber=rank * 100000 + it, iteration=it)
+        pt.execute(ds.desc(p, sb), total, 1, it, stream)
+        ap_ = accumulation_param(W, H, it)
+        resolve(p, sb, tp, ap_ if it > 0 else None, hist if it > 0 else None, acc, None, rgba8, stream)
+        return p
+
+    for it in range(args.warmup):
+        frame(it)
+    torch.cuda.synchronize()
+    st = pt.device_status()
+    if st != 0:
+        raise RuntimeError(f"device status {st:#x}")
+
+    # ---- device-timed region: inputs resident in HBM -------------------------
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    pt.kernel_times(stream)  # reset the per-launch records
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ext_ms = 0.0
+    launches = 0
+    for k in range(args.steps):
+        frame(args.warmup + k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    el_ms = e0.elapsed_time(e1)
+    # per-kernel CUDA-event times summed over every launch of the timed region
+    times = pt.kernel_times(stream)
+    if dist:
+        t = torch.tensor([el_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el_ms = float(t.item())
+
+    value = world * total * args.steps / (el_ms * 1e-3) / 1e6
+
+    # ---- extend-kernel roofline: replay the timed frames with counters -------
+    ext_ms = times["extend"][0]
+    ext_launches = times["extend"][1]
+    launches = sum(c for _, c in times.values()) + args.steps  # + one resolve per frame
+    pt_count = PathTracer(mode=mode, chunk_paths=args.chunk, count=True)
+    for k in range(args.steps):
+        pt_count.execute(ds.desc(hs.param(frameNumber=rank * 100000 + args.warmup + k), sb), total, 1, 0, stream)
+    cnt = pt_count.counters(stream)
+    pt_count.close()
+    # algorithmic bytes of the closest-hit traversal: 32 B per inner node,
+    # 32 + 48 B per leaf (node + triangle), 32 B ray in, 20 B hit out
+    bytes_alg = 32 * cnt["extend_inner"] + 80 * cnt["extend_leaf"] + 52 * cnt["extend_rays"]
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = json.load(open(peaks_path))["hbm_gbs"]
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = bytes_alg / (ext_ms * 1e-3) / 1e9 if ext_ms > 0 else None
+
+    # ---- end to end through the C ABI: host param in, tonemapped RGBA8 out ---
+    host_img = torch.empty(W * H * 4, dtype=torch.uint8, pin_memory=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for k in range(args.steps):
+        frame(args.warmup + args.steps + k)
+        host_img.copy_(rgba8, non_blocking=True)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = world * total * args.steps / (e2e_ms * 1e-3) / 1e6
+    img = host_img.numpy()
+    if not (img[3::4] == 255).all():
+        raise RuntimeError("resolve produced no image")
+    st = pt.device_status()
+    if st != 0:
+        raise RuntimeError(f"device status {st:#x}")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, n, threads, el = cpu_baseline(hs, args, budget_s=args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{n} paths of the frame ({n / total * 100:.3f}%), 64 evenly spaced slices of the sample "
+                         f"indices, {el:.1f} s, oracle C restatement -O3 -ffp-contract=fast, OpenMP"}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    cfg = workload_config(args)
+    cfg["triangles"] = hs.num_triangles
+    cfg["parallelism"] = f"replicas x{world} (independent frames per GPU)" if world > 1 else "single GPU"
+    param_bytes = 336 + 416 + 16
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded procedural scene, see config.workload)", "config": cfg,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "kernel": "extend (closest-hit traversal)", "peak_source": peak_src,
+                     "bytes_alg_timed_region": bytes_alg, "kernel_ms_timed_region": ext_ms,
+                     "kernel_launches_timed_region": ext_launches, "visits": cnt},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": param_bytes, "d2h_bytes_per_step": W * H * 4},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "kernel_ms_per_frame": {k: v[0] / args.steps for k, v in times.items() if v[1]},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

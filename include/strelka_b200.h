@@ -1,0 +1,443 @@
+/*
+ * strelka_b200.h — C ABI of the B200 (sm_100a) path-tracing hot path.
+ *
+ * This is the drop-in boundary for Strelka's render-pass API.  The reference
+ * records four compute passes per frame, each through
+ *     ComputePass<T>::execute(VkCommandBuffer&, const XDesc&, w, h, frameIndex)
+ * (include/render/computepass.h:8-164, called from src/render/ptrender.cpp:735-862).
+ * Here each pass is one extern "C" function taking the same constants struct,
+ * the same buffers (as device pointers instead of Buffer and Image handles), the
+ * same (w, h, frameIndex) triple and a cudaStream_t in place of the command
+ * buffer.  Buffers stay owned by the caller, as they are owned by the
+ * reference's ResourceManager; the passes only read and write them.
+ *
+ * Every entry point returns an int status: 0 = OK (STRELKA_OK), otherwise a
+ * STRELKA_ERR_* code; strelka_get_last_error() returns the message of the most
+ * recent failure on the calling thread.  Kernels never trap: out-of-range
+ * indices and over-long traversals set a device status word that the host
+ * reads with strelka_pathtracer_get_device_status().
+ *
+ * All structs below are byte-identical to the reference's shader structs; the
+ * static asserts at the end of this file pin sizes and offsets.
+ *
+ * Matrices are column-major (the glm layout the reference uploads raw): the
+ * element in row r, column c is m[c*4 + r], and a shader mul(M, v) is the
+ * matrix-vector product M·v.
+ */
+#ifndef STRELKA_B200_H
+#define STRELKA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Status codes (replace Result{eOk,eFail,eOutOfMemory}, include/render/common.h:338-343) */
+enum {
+    STRELKA_OK = 0,
+    STRELKA_ERR_INVALID_ARGUMENT = 1,
+    STRELKA_ERR_OUT_OF_MEMORY = 2,
+    STRELKA_ERR_CUDA = 3,
+    STRELKA_ERR_NO_DEVICE = 4,
+    STRELKA_ERR_DEVICE_BOUNDS = 5,   /* a kernel saw an out-of-range index */
+    STRELKA_ERR_TIMEOUT = 6,         /* a traversal or queue wait hit its iteration cap */
+    STRELKA_ERR_UNSUPPORTED = 7
+};
+
+/* Device status bits (strelka_pathtracer_get_device_status). */
+enum {
+    STRELKA_DEV_OK = 0,
+    STRELKA_DEV_NODE_OOB = 1u << 0,     /* node index >= numNodes */
+    STRELKA_DEV_INSTANCE_OOB = 1u << 1, /* instance id >= numInstances */
+    STRELKA_DEV_INDEX_OOB = 1u << 2,    /* ib offset or vertex index out of range */
+    STRELKA_DEV_MATERIAL_OOB = 1u << 3, /* material id / arg block offset out of range */
+    STRELKA_DEV_LIGHT_OOB = 1u << 4,    /* light id >= light capacity */
+    STRELKA_DEV_TRAVERSAL_CAP = 1u << 5,/* traversal exceeded 2*numNodes+2 visits (cycle) */
+    STRELKA_DEV_TEXTURE_OOB = 1u << 6,
+    STRELKA_DEV_QUEUE_TIMEOUT = 1u << 7
+};
+
+/* ------------------------------------------------------------------------- */
+/* Shared shader structs                                                     */
+
+typedef struct StrelkaFloat4 { float x, y, z, w; } StrelkaFloat4;
+typedef struct StrelkaFloat4x4 { float m[16]; } StrelkaFloat4x4;
+
+/* shaders/pathtracerparam.h:20-43 (336 bytes) */
+typedef struct PathTracerParam {
+    StrelkaFloat4x4 viewToWorld;
+    StrelkaFloat4x4 clipToView;
+    StrelkaFloat4x4 viewToClip;
+    StrelkaFloat4x4 worldToView;
+    StrelkaFloat4 camPos;
+    int32_t dimension[2];
+    float invDimension[2];
+    uint32_t frameNumber;
+    uint32_t maxDepth;
+    uint32_t debug;
+    uint32_t numLights;
+    int32_t len;
+    int32_t spp;
+    int32_t iteration;
+    uint32_t stratifiedSamplingType; /* 0 centre, 1 random, 2 stratified, 3 CMJ */
+    StrelkaFloat4 pad0;
+} PathTracerParam;
+
+/* shaders/accumulationparam.h:19-34 (416 bytes) */
+typedef struct AccumulationParam {
+    StrelkaFloat4x4 prevViewToWorld;
+    StrelkaFloat4x4 prevClipToView;
+    StrelkaFloat4x4 prevWorldToView;
+    StrelkaFloat4x4 prevViewToClip;
+    StrelkaFloat4x4 viewToWorld;
+    StrelkaFloat4x4 clipToView;
+    int32_t dimension[2];
+    uint32_t frameNumber;
+    uint32_t iteration;
+    float alpha;
+    float isPt;
+    float pad1;
+    float pad2;
+} AccumulationParam;
+
+/* shaders/tonemapparam.h:17-22 (16 bytes) */
+typedef struct Tonemapparam {
+    int32_t dimension[2];
+    uint32_t tonemapperType; /* 0 Reinhard, 1 ACESFitted, 2 ACESFilm */
+    uint32_t pad0;
+} Tonemapparam;
+
+/* shaders/raytracing.h:27-33, include/render/bvh.h:18-24 (32 bytes).
+ * Inner node: instId == -1, bounds valid, the left child is the next node,
+ * nodeOffset is the escape index (next sibling or uncle, -1 at the end).
+ * Leaf: instId = instance id, minBounds[0] holds the bits of the
+ * per-instance triangle index, nodeOffset is the escape index. */
+typedef struct BVHNode {
+    float minBounds[3];
+    int32_t instId;
+    float maxBounds[3];
+    int32_t nodeOffset;
+} BVHNode;
+
+/* shaders/raytracing.h:17-25, include/scene/scene.h:54-63 (32 bytes) */
+typedef struct Vertex {
+    float position[3];
+    uint32_t tangent; /* 10/10/12-bit packed, shaders/pack.h:4-14 */
+    uint32_t normal;  /* 10/10/12-bit packed */
+    uint32_t uv;      /* 16/16-bit packed, shaders/pack.h:16-24 */
+    float pad0;
+    float pad1;
+} Vertex;
+
+/* shaders/instanceconstants.h:19-28 (208 bytes) */
+typedef struct InstanceConstants {
+    StrelkaFloat4x4 objectToWorld;
+    StrelkaFloat4x4 worldToObject;
+    StrelkaFloat4x4 normalMatrix;
+    int32_t materialId; /* -1 for light emitter instances */
+    int32_t indexOffset;
+    int32_t indexCount;
+    int32_t lightId; /* -1 unless the instance is a light's emitter mesh */
+} InstanceConstants;
+
+/* shaders/lights.h:10-19 (112 bytes).  type 0 rect (points = 4 corners),
+ * 1 disc (points[0].x radius, [1] centre, [2..3] axes, normal),
+ * 2 sphere (points[0].x radius, [1] centre). */
+typedef struct UniformLight {
+    StrelkaFloat4 points[4];
+    StrelkaFloat4 color;
+    StrelkaFloat4 normal;
+    int32_t type;
+    float pad0;
+    float pad2;
+    float pad3;
+} UniformLight;
+
+/* shaders/materials.h:17-23 (16 bytes) */
+typedef struct MdlMaterial {
+    int32_t arg_block_offset;       /* bytes into mdl_argument_block */
+    int32_t ro_data_segment_offset; /* bytes into mdl_ro_data_segment */
+    int32_t functionId;             /* STRELKA_FN_* */
+    int32_t pad1;
+} MdlMaterial;
+
+/* shaders/materials.h:27-34 (16 bytes) */
+typedef struct Mdl_resource_info {
+    uint32_t gpu_resource_array_start; /* texture slot in matTextures */
+    uint32_t pad0;
+    uint32_t pad1;
+    uint32_t pad2;
+} Mdl_resource_info;
+
+/* shaders/ray.h:12-16 (32 bytes): o.xyz origin, o.w max distance, d.xyz direction */
+typedef struct Ray {
+    StrelkaFloat4 o;
+    StrelkaFloat4 d;
+} Ray;
+
+/* shaders/raytracing.h:90-96 (20 bytes) */
+typedef struct Hit {
+    float bary[2];
+    float t;
+    uint32_t instId;
+    uint32_t primId;
+} Hit;
+
+/* include/render/bvh.h:31-36 (20 bytes): one world-space triangle corner */
+typedef struct BVHInputPosition {
+    float pos[3];
+    uint32_t instId;
+    uint32_t primId;
+} BVHInputPosition;
+
+/* ------------------------------------------------------------------------- */
+/* Native material table.  The reference fills the MDL tables with code and
+ * argument blocks generated by the MDL SDK (src/materialmanager/
+ * mdlHlslCodeGen.cpp:32-81), which is not available.  The table ABI is kept
+ * (MdlMaterial, argument block, ro-data, resource infos, texture array); the
+ * functionId selects one of the native BSDFs below, and the argument block at
+ * arg_block_offset holds one StrelkaMaterialArgs record (project-defined). */
+enum {
+    STRELKA_FN_LAMBERT = 0,        /* cosine-sampled Lambert, shaders/pathtracer.hlsl:176-234 */
+    STRELKA_FN_GGX_CONDUCTOR = 1,  /* GGX microfacet metal, Schlick Fresnel */
+    STRELKA_FN_GGX_DIELECTRIC = 2, /* GGX rough dielectric (reflect + refract) */
+    STRELKA_FN_COUNT = 3
+};
+
+typedef struct StrelkaMaterialArgs {
+    float base_color[3];          /* albedo / F0 / transmission tint (linear) */
+    float roughness;              /* GGX alpha = roughness^2 */
+    float emission[3];            /* EDF radiance; zero for non-emissive */
+    float ior;                    /* dielectric index of refraction */
+    uint32_t base_color_texture;  /* MDL resource id: 0 none, else mdl_resource_infos[id-1] */
+    uint32_t pad[3];
+} StrelkaMaterialArgs;            /* 48 bytes */
+
+/* One bindless texture: RGBA8 sRGB texels in device memory, row-major,
+ * sampled bilinearly with REPEAT wrapping at lod 0 (the reference's MDL
+ * sampler, include/texturemanager/texturemanager.h:24-44). */
+typedef struct StrelkaTexture {
+    const uint8_t* rgba8;
+    uint32_t width;
+    uint32_t height;
+    uint64_t pad;
+} StrelkaTexture;
+
+/* Optional environment light (the reference adds zero on a miss,
+ * shaders/pathtracerMdl.hlsl:389-399).  Lat-long RGBA32F map with
+ * importance-sampling tables from strelka_envmap_build_cdf_host(). */
+typedef struct StrelkaEnvMap {
+    const float* rgba32f;       /* width*height*4 floats */
+    const float* marginal_cdf;  /* height+1 floats */
+    const float* conditional_cdf; /* height*(width+1) floats */
+    uint32_t width;
+    uint32_t height;
+    float integral;             /* sum of luminance*sin(theta) weights */
+    float pad;
+} StrelkaEnvMap;
+
+/* ------------------------------------------------------------------------- */
+/* Pass descriptors: include/render/pathtracer.h:9-31, reduction.h:10-16,
+ * accumulation.h:9-15, tonemap.h:11-16.  Pointers are device pointers. */
+
+typedef struct PathTracerDesc {
+    PathTracerParam constants;
+    const BVHNode* bvhNodes;      uint32_t numNodes;
+    uint32_t numVertices;         const Vertex* vb;
+    const uint32_t* ib;           uint32_t numIndices;
+    uint32_t numInstances;        const InstanceConstants* instanceConst;
+    const UniformLight* lights;   uint32_t lightCapacity;
+    uint32_t pad0;
+    float* sampleBuffer;          /* W*H*spp*3 floats, [(pixel*spp + s)*3 + c] */
+    const uint8_t* mdl_ro_data_segment; uint64_t roDataBytes;
+    const uint8_t* mdl_argument_block;  uint64_t argBlockBytes;
+    const Mdl_resource_info* mdl_resource_infos; uint32_t numResourceInfos;
+    uint32_t numMaterials;        const MdlMaterial* mdl_mdlMaterial;
+    const StrelkaTexture* matTextures; /* device array of numTextures entries */
+    uint32_t numTextures;         uint32_t pad1;
+    const StrelkaEnvMap* envMap;  /* host pointer to a descriptor, or NULL: black miss */
+    uint64_t sceneVersion;        /* bump when any scene buffer changes */
+} PathTracerDesc;
+
+typedef struct ReductionDesc {
+    PathTracerParam constants;
+    const float* sampleBuffer;    /* W*H*spp*3 */
+    float* result;                /* W*H RGBA32F */
+} ReductionDesc;
+
+typedef struct AccumulationDesc {
+    AccumulationParam constants;
+    const float* input;           /* RGBA32F */
+    const float* history;         /* RGBA32F */
+    float* output;                /* RGBA32F */
+} AccumulationDesc;
+
+typedef struct TonemapDesc {
+    Tonemapparam constants;
+    const float* input;           /* RGBA32F */
+    float* output;                /* RGBA32F */
+} TonemapDesc;
+
+/* ------------------------------------------------------------------------- */
+/* Path tracer pass object (replaces PathTracer : ComputePass<PathTracerParam>,
+ * include/render/pathtracer.h:33-50, src/render/pathtracer.cpp:1-94).  The
+ * object caches scene-derived device data (a leaf triangle table) keyed by
+ * PathTracerDesc.sceneVersion and the buffer pointers, and owns the
+ * wavefront path queues. */
+
+enum {
+    STRELKA_MODE_WAVEFRONT = 0,  /* generate / extend / shade / shadow kernels */
+    STRELKA_MODE_MEGAKERNEL = 1  /* one thread per (pixel, sample), like computeMain */
+};
+
+typedef struct StrelkaPathTracerConfig {
+    uint32_t mode;            /* STRELKA_MODE_* */
+    uint32_t chunkPaths;      /* wavefront: paths in flight per chunk (0 = auto) */
+    uint32_t blockSize;       /* threads per block (0 = auto) */
+    uint32_t flags;           /* STRELKA_PT_* */
+} StrelkaPathTracerConfig;
+
+enum {
+    STRELKA_PT_PROFILE = 1u << 0, /* record per-kernel CUDA events (strelka_pathtracer_get_kernel_times) */
+    STRELKA_PT_COUNT = 1u << 1    /* count traversal visits (strelka_pathtracer_get_counters) */
+};
+
+typedef struct StrelkaPathTracer StrelkaPathTracer;
+
+/* PathTracer::initialize (src/render/pathtracer.cpp:62-92). */
+int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, StrelkaPathTracer** out);
+int strelka_pathtracer_destroy(StrelkaPathTracer* pt);
+
+/* PathTracer::execute (src/render/pathtracer.cpp:50-59).  As in the reference,
+ * w = W*H*spp threads of work and h = 1; writes desc->sampleBuffer. */
+int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTracerDesc* desc,
+                               uint32_t w, uint32_t h, uint64_t frameIndex, void* stream);
+
+/* Reads and clears the device status word (STRELKA_DEV_* bits); synchronises
+ * the stream first. */
+int strelka_pathtracer_get_device_status(StrelkaPathTracer* pt, void* stream, uint32_t* status);
+
+/* Per-kernel timing when STRELKA_PT_PROFILE is set: for each kernel class
+ * ("generate","extend","shade","shadow","finalize","megakernel","prep") the
+ * CUDA-event milliseconds summed over every launch since the previous call,
+ * and the launch count; clears the records.  Returns the number of classes. */
+int strelka_pathtracer_get_kernel_times(StrelkaPathTracer* pt, void* stream, float* ms_out,
+                                        uint32_t* launches_out, uint32_t capacity);
+
+/* Traversal counters accumulated since the last call when STRELKA_PT_COUNT is
+ * set: {extend inner-node visits, extend leaf visits, shadow inner visits,
+ * shadow leaf visits, extend rays, shadow rays}.  Resets them.  Returns 6. */
+int strelka_pathtracer_get_counters(StrelkaPathTracer* pt, void* stream, unsigned long long* out,
+                                    uint32_t capacity);
+
+/* ReductionPass::execute (src/render/reduction.cpp, shaders/reduction.hlsl:9-32); w = W*H. */
+int strelka_reduction_execute(const ReductionDesc* desc, uint32_t w, uint32_t h,
+                              uint64_t frameIndex, void* stream);
+
+/* Accumulation::execute (src/render/accumulation.cpp, shaders/accumulation.hlsl:86-108); w = W, h = H. */
+int strelka_accumulation_execute(const AccumulationDesc* desc, uint32_t w, uint32_t h,
+                                 uint64_t frameIndex, void* stream);
+
+/* Tonemap::execute (src/render/tonemap.cpp, shaders/tonemap.hlsl:66-88); w = W, h = H. */
+int strelka_tonemap_execute(const TonemapDesc* desc, uint32_t w, uint32_t h,
+                            uint64_t frameIndex, void* stream);
+
+/* Fused reduce + accumulate + tonemap in one pass over the sample buffer.
+ * Equivalent, bit for bit, to the three passes above run in sequence
+ * (src/render/ptrender.cpp:780-862); accumulation is applied when
+ * accumulate != 0.  Writes the accumulated image (RGBA32F) to accOutput and the
+ * tonemapped image to tonemapOutput (RGBA32F) and/or tonemapRGBA8 (either may be NULL). */
+int strelka_resolve_execute(const PathTracerParam* ptParam, const float* sampleBuffer,
+                            int accumulate, const AccumulationParam* accParam, const float* history,
+                            float* accOutput, const Tonemapparam* tmParam, float* tonemapOutput,
+                            uint8_t* tonemapRGBA8, void* stream);
+
+/* ------------------------------------------------------------------------- */
+/* Ray queries over the flattened BVH (the closestHit / anyHit functions of
+ * shaders/raytracing.h:198-286, exposed for the traversal microbenchmark). */
+
+enum {
+    STRELKA_TRACE_CLOSEST = 0,
+    STRELKA_TRACE_ANY = 1,          /* first hit in depth-first order with t < tmax */
+    STRELKA_TRACE_COUNT = 1u << 4,  /* also count inner/leaf visits into counters[2] */
+    STRELKA_TRACE_REFINE = 1u << 5  /* closest: recompute t/bary of the winner in float-float */
+};
+
+typedef struct TraceDesc {
+    const BVHNode* bvhNodes;      uint32_t numNodes;
+    uint32_t numVertices;         const Vertex* vb;
+    const uint32_t* ib;           uint32_t numIndices;
+    uint32_t numInstances;        const InstanceConstants* instanceConst;
+    const Ray* rays;              /* device */
+    Hit* hits;                    /* device */
+    uint32_t numRays;
+    uint32_t flags;               /* STRELKA_TRACE_* */
+    unsigned long long* counters; /* device, 2 entries: inner visits, leaf visits (COUNT) */
+    uint64_t sceneVersion;
+} TraceDesc;
+
+/* Uses the same scene cache as the path tracer object. */
+int strelka_trace_execute(StrelkaPathTracer* pt, const TraceDesc* desc, void* stream);
+
+/* Same query with host buffers for rays and hits: copies rays in, traces,
+ * copies hits out on the given stream, and synchronises it. */
+int strelka_trace_host(StrelkaPathTracer* pt, const TraceDesc* desc, const Ray* hostRays,
+                       Hit* hostHits, void* stream);
+
+/* ------------------------------------------------------------------------- */
+/* Host-side scene preparation (replaces BvhBuilder, include/render/bvh.h:38-46). */
+
+/* SAH BVH over world-space triangles (3 consecutive positions per triangle),
+ * emitting the reference's flattened depth-first layout with escape indices
+ * (src/render/bvh.cpp:169-235).  *outNodes is allocated with malloc; free it
+ * with strelka_host_free. */
+int strelka_bvh_build(const BVHInputPosition* positions, uint32_t numPositions,
+                      BVHNode** outNodes, uint32_t* outNumNodes);
+void strelka_host_free(void* p);
+
+/* ------------------------------------------------------------------------- */
+/* Errors and versioning */
+int strelka_get_last_error(char* buffer, size_t capacity);
+int strelka_version(void);
+/* Sizes of every struct above, for bindings to check their layouts:
+ * returns sizeof for names "PathTracerParam", "BVHNode", ... or 0. */
+size_t strelka_sizeof(const char* struct_name);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+/* Layout pins. */
+#ifdef __cplusplus
+#define STRELKA_STATIC_ASSERT(c, m) static_assert(c, m)
+#else
+#define STRELKA_STATIC_ASSERT(c, m) _Static_assert(c, m)
+#endif
+STRELKA_STATIC_ASSERT(sizeof(PathTracerParam) == 336, "PathTracerParam size");
+STRELKA_STATIC_ASSERT(offsetof(PathTracerParam, camPos) == 256, "camPos offset");
+STRELKA_STATIC_ASSERT(offsetof(PathTracerParam, dimension) == 272, "dimension offset");
+STRELKA_STATIC_ASSERT(offsetof(PathTracerParam, frameNumber) == 288, "frameNumber offset");
+STRELKA_STATIC_ASSERT(offsetof(PathTracerParam, len) == 304, "len offset");
+STRELKA_STATIC_ASSERT(offsetof(PathTracerParam, stratifiedSamplingType) == 316, "sst offset");
+STRELKA_STATIC_ASSERT(sizeof(AccumulationParam) == 416, "AccumulationParam size");
+STRELKA_STATIC_ASSERT(offsetof(AccumulationParam, dimension) == 384, "acc dimension offset");
+STRELKA_STATIC_ASSERT(offsetof(AccumulationParam, alpha) == 400, "acc alpha offset");
+STRELKA_STATIC_ASSERT(sizeof(Tonemapparam) == 16, "Tonemapparam size");
+STRELKA_STATIC_ASSERT(sizeof(BVHNode) == 32, "BVHNode size");
+STRELKA_STATIC_ASSERT(sizeof(Vertex) == 32, "Vertex size");
+STRELKA_STATIC_ASSERT(sizeof(InstanceConstants) == 208, "InstanceConstants size");
+STRELKA_STATIC_ASSERT(offsetof(InstanceConstants, materialId) == 192, "materialId offset");
+STRELKA_STATIC_ASSERT(sizeof(UniformLight) == 112, "UniformLight size");
+STRELKA_STATIC_ASSERT(offsetof(UniformLight, type) == 96, "light type offset");
+STRELKA_STATIC_ASSERT(sizeof(MdlMaterial) == 16, "MdlMaterial size");
+STRELKA_STATIC_ASSERT(sizeof(Mdl_resource_info) == 16, "Mdl_resource_info size");
+STRELKA_STATIC_ASSERT(sizeof(Ray) == 32, "Ray size");
+STRELKA_STATIC_ASSERT(sizeof(Hit) == 20, "Hit size");
+STRELKA_STATIC_ASSERT(sizeof(BVHInputPosition) == 20, "BVHInputPosition size");
+STRELKA_STATIC_ASSERT(sizeof(StrelkaMaterialArgs) == 48, "StrelkaMaterialArgs size");
+STRELKA_STATIC_ASSERT(sizeof(StrelkaTexture) == 24, "StrelkaTexture size");
+
+#endif /* STRELKA_B200_H */

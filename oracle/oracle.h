@@ -1,0 +1,118 @@
+/*
+ * oracle.h — CPU restatement of Strelka's path-tracing shader math.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path:
+ * only the tests, the smoke check and the CPU-baseline leg of the benchmark
+ * may load it.  Nothing in the product links or calls it.
+ *
+ * Parity status: the reference's shaders cannot run on this machine (they
+ * need Slang and a Vulkan device) and its tests hold no golden vectors for
+ * this path, so the restatement is pinned by the reference's own known-answer
+ * cases (the slab tests of tests/intersection/aabb.cpp:16-106), by
+ * hand-computed RNG states, by analytic checks (white furnace, tonemap
+ * formulas at chosen points) and by golden fixtures generated from this file.
+ *
+ * Every function cites the reference lines it restates.  Floating-point
+ * evaluation follows the source expressions left to right with no fused
+ * multiply-add (build with -ffp-contract=off); sin/cos/acos are this
+ * project's own correctly-reduced polynomial versions, which the CUDA kernels
+ * implement identically, so the two sides agree bit for bit.
+ */
+#ifndef STRELKA_ORACLE_H
+#define STRELKA_ORACLE_H
+
+#include <stdint.h>
+#include <stddef.h>
+#include "../include/strelka_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OracleTexture {
+    const uint8_t* rgba8; /* host texels */
+    uint32_t width, height;
+} OracleTexture;
+
+typedef struct OracleEnvMap {
+    const float* rgba32f;
+    const float* marginal_cdf;
+    const float* conditional_cdf;
+    uint32_t width, height;
+    float integral;
+} OracleEnvMap;
+
+/* All pointers are host pointers. */
+typedef struct OracleScene {
+    const BVHNode* nodes; uint32_t numNodes;
+    const Vertex* vb; uint32_t numVertices;
+    const uint32_t* ib; uint32_t numIndices;
+    const InstanceConstants* instances; uint32_t numInstances;
+    const UniformLight* lights; uint32_t lightCapacity;
+    const uint8_t* argBlock; uint64_t argBlockBytes;
+    const MdlMaterial* materials; uint32_t numMaterials;
+    const Mdl_resource_info* resourceInfos; uint32_t numResourceInfos;
+    const OracleTexture* textures; uint32_t numTextures;
+    const OracleEnvMap* envMap; /* NULL: black miss */
+} OracleScene;
+
+/* random.h:14-48 */
+uint32_t oracle_jenkins_hash(uint32_t x);
+uint32_t oracle_init_rng(uint32_t px, uint32_t py, uint32_t width, uint32_t frame);
+uint32_t oracle_xorshift(uint32_t* state);
+float oracle_rand(uint32_t* state);
+/* helper.h:117-163 */
+uint32_t oracle_permute(uint32_t i, uint32_t l, uint32_t p);
+float oracle_randfloat(uint32_t i, uint32_t p);
+
+/* own transcendental functions (shared definition with the kernels) */
+float oracle_sinf(float x);
+float oracle_cosf(float x);
+float oracle_acosf(float x);
+
+/* pack.h:4-33 */
+void oracle_unpack_normal(uint32_t v, float out[3]);
+void oracle_unpack_uv(uint32_t v, float out[2]);
+/* helper.h:12-28 */
+void oracle_offset_ray(const float p[3], const float n[3], float out[3]);
+/* ray.h:19-33 */
+int oracle_intersect_ray_box(const float o[3], const float invdir[3], const float pmin[3],
+                             const float pmax[3], float* t);
+/* raytracing.h:36-88 */
+int oracle_ray_triangle(const float o[3], const float d[3], const float v0[3], const float e0[3],
+                        const float e1[3], float* t, float* u, float* v);
+
+/* raytracing.h:198-286 over n rays.  mode 0 closest, 1 any.  found[i] = 0/1.
+ * prune != 0 replays the GPU's closest-hit pruning rule (for visit counts).
+ * counters (may be NULL) gets {inner visits, leaf visits} summed. */
+int oracle_trace(const OracleScene* s, const Ray* rays, uint32_t n, Hit* hits, uint8_t* found,
+                 int mode, int prune, unsigned long long* counters, int nthreads);
+
+/* FP64 Möller–Trumbore of ray i against triangle (instId[i], primId[i]),
+ * same formula as raytracing.h:36-88 evaluated in double (no thresholds). */
+int oracle_intersect_fp64(const OracleScene* s, const Ray* rays, const uint32_t* instIds,
+                          const uint32_t* primIds, uint32_t n, double* t, double* u, double* v);
+
+/* pathtracerMdl.hlsl:406-423 computeMain over idx in [0, W*H*spp):
+ * writes sampleBuffer[(idx)*3 + c]. */
+int oracle_pathtrace(const PathTracerParam* p, const OracleScene* s, float* sampleBuffer,
+                     int nthreads);
+/* Same, for the sub-range of sample indices [first, first+count). */
+int oracle_pathtrace_range(const PathTracerParam* p, const OracleScene* s, float* sampleBuffer,
+                           uint64_t first, uint64_t count, int nthreads);
+
+/* reduction.hlsl:9-32 */
+int oracle_reduce(const PathTracerParam* p, const float* sampleBuffer, float* rgba32f);
+/* accumulation.hlsl:86-97 */
+int oracle_accumulate(const AccumulationParam* p, const float* input, const float* history,
+                      float* output);
+/* tonemap.hlsl:9-88 */
+int oracle_tonemap(const Tonemapparam* p, const float* input, float* output);
+
+/* texture lookup, mdl_runtime.hlsl:173-208 (REPEAT, no crop) */
+void oracle_tex_lookup(const OracleTexture* t, float u, float v, float out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

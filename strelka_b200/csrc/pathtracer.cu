@@ -1,0 +1,776 @@
+// pathtracer.cu — the path tracer pass (megakernel and wavefront forms) and
+// the ray-query microbenchmark entry points, sm_100a.
+//
+// PathTracer::execute (src/render/pathtracer.cpp:50-59) dispatches
+// computeMain (shaders/pathtracerMdl.hlsl:406-423) over W*H*spp threads.
+// Here the same work runs either as
+//   * a megakernel: one thread per (pixel, sample), the reference's shape, or
+//   * a wavefront: per chunk of paths, generate -> [extend -> shade -> shadow]
+//     x maxDepth -> finalize, each a separate kernel over structure-of-arrays
+//     path state, with the surviving paths compacted by warp ballot into a
+//     queue between bounces.
+// Both forms call the same shade()/apply_shadow() device code.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.h"
+#include "refine.cuh"
+#include "shading.cuh"
+
+using namespace sb;
+
+namespace {
+
+constexpr int kExtendBlock = 128;
+constexpr int kShadeBlock = 128;
+constexpr int kSmallBlock = 256;
+
+enum KernelClass { KC_GENERATE = 0, KC_EXTEND, KC_SHADE, KC_SHADOW, KC_FINALIZE, KC_MEGAKERNEL, KC_PREP, KC_COUNT };
+const char* kKernelNames[KC_COUNT] = {"generate", "extend", "shade", "shadow", "finalize", "megakernel", "prep"};
+
+// ---------------------------------------------------------------------------
+// Scene preparation: leaf triangle table, raytracing.h:134-153 per leaf node.
+__global__ void k_prep_tris(const float4* __restrict__ nodes, uint32_t numNodes, const InstanceConstants* __restrict__ inst,
+                            uint32_t numInstances, const uint32_t* __restrict__ ib, uint32_t numIndices,
+                            const Vertex* __restrict__ vb, uint32_t numVertices, float4* __restrict__ tris,
+                            uint32_t* status)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x) {
+        const float4 lo = nodes[2 * (size_t)i];
+        const float4 hi = nodes[2 * (size_t)i + 1];
+        const uint32_t instId = __float_as_uint(lo.w);
+        float4* out = &tris[3 * (size_t)i];
+        if (instId == SB_INVALID) {
+            // inner node: the slot is never read; record the bounds sanity only
+            uint32_t esc = __float_as_uint(hi.w);
+            if (esc != SB_INVALID && esc >= numNodes) atomicOr(status, STRELKA_DEV_NODE_OOB);
+            continue;
+        }
+        const float qnan = __int_as_float(0x7fc00000);
+        float4 bad = make_float4(qnan, qnan, qnan, 0.0f);
+        uint32_t esc = __float_as_uint(hi.w);
+        if (esc != SB_INVALID && esc >= numNodes) atomicOr(status, STRELKA_DEV_NODE_OOB);
+        if (instId >= numInstances) {
+            atomicOr(status, STRELKA_DEV_INSTANCE_OOB);
+            out[0] = bad; out[1] = bad; out[2] = bad;
+            continue;
+        }
+        const InstanceConstants* ic = &inst[instId];
+        const uint32_t prim = __float_as_uint(lo.x);
+        const uint32_t base = (uint32_t)ic->indexOffset + prim * 3u;
+        if ((uint64_t)base + 2 >= numIndices) {
+            atomicOr(status, STRELKA_DEV_INDEX_OOB);
+            out[0] = bad; out[1] = bad; out[2] = bad;
+            continue;
+        }
+        const uint32_t i0 = ib[base], i1 = ib[base + 1], i2 = ib[base + 2];
+        if (i0 >= numVertices || i1 >= numVertices || i2 >= numVertices) {
+            atomicOr(status, STRELKA_DEV_INDEX_OOB);
+            out[0] = bad; out[1] = bad; out[2] = bad;
+            continue;
+        }
+        const float* m = ic->objectToWorld.m;
+        v3 v0 = mat_mul_point(m, V(vb[i0].position[0], vb[i0].position[1], vb[i0].position[2]), 1.0f);
+        v3 e0 = vsub(mat_mul_point(m, V(vb[i1].position[0], vb[i1].position[1], vb[i1].position[2]), 1.0f), v0);
+        v3 e1 = vsub(mat_mul_point(m, V(vb[i2].position[0], vb[i2].position[1], vb[i2].position[2]), 1.0f), v0);
+        out[0] = f4(v0, __uint_as_float(instId));
+        out[1] = f4(e0, __uint_as_float(prim));
+        out[2] = f4(e1, 0.0f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Megakernel: computeMain, one thread per (pixel, sample).
+__global__ void __launch_bounds__(kExtendBlock) k_megakernel(DevScene s, PathTracerParam ubo, float* __restrict__ sampleBuffer,
+                                                             uint64_t first, uint64_t count)
+{
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint64_t idx = first + t;
+    PathState ps;
+    init_path(ubo, idx, ps);
+    const int maxDepth = (int)ubo.maxDepth;
+    while (ps.depth < maxDepth) {
+        HitRec h;
+        uint32_t a = 0, b = 0;
+        bool found = s.numNodes != 0 && trace_closest<false>(s, ps.ro, ps.tmax, ps.rd, h, a, b);
+        ShadowReq sr;
+        bool cont = shade(s, ubo, ps, found, h, sr);
+        if (sr.kind != 0 && shadow_visible(s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
+        if (!cont) break;
+        ++ps.depth;
+    }
+    sampleBuffer[idx * 3 + 0] = ps.color.x;
+    sampleBuffer[idx * 3 + 1] = ps.color.y;
+    sampleBuffer[idx * 3 + 2] = ps.color.z;
+}
+
+// ---------------------------------------------------------------------------
+// Wavefront state (structure of arrays, one slot per path of the chunk).
+struct Wave {
+    float4* ray_o;   // origin, tmax
+    float4* ray_d;   // direction, last BSDF pdf
+    float4* thr;     // throughput, flags (depth | specular << 16 | inside << 17)
+    float4* col;     // color
+    uint32_t* rng;
+    float4* hit;     // u, v, t, instId (SB_INVALID = miss)
+    uint32_t* hitPrim;
+    uint32_t* queue[2];
+    float4* sh_o;    // origin, tmax
+    float4* sh_d;    // direction, slot
+    float4* sh_cd;   // diffuse contribution, kind
+    float4* sh_cg;   // glossy contribution
+    uint32_t* counters;  // [0],[1] queue sizes, [2] shadow queue size
+};
+
+__device__ __forceinline__ uint32_t pack_flags(const PathState& ps)
+{
+    return (uint32_t)ps.depth | ((uint32_t)ps.specular << 16) | ((uint32_t)ps.inside << 17);
+}
+
+__global__ void __launch_bounds__(kSmallBlock) k_generate(PathTracerParam ubo, Wave w, uint64_t first, uint32_t n)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.counters[0] = n;
+        w.counters[1] = 0;
+        w.counters[2] = 0;
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        PathState ps;
+        init_path(ubo, first + i, ps);
+        w.ray_o[i] = f4(ps.ro, ps.tmax);
+        w.ray_d[i] = f4(ps.rd, ps.lastPdf);
+        w.thr[i] = f4(ps.throughput, __uint_as_float(pack_flags(ps)));
+        w.col[i] = f4(ps.color, 0.0f);
+        w.rng[i] = ps.rng;
+        w.queue[0][i] = i;
+    }
+}
+
+// extend: closest-hit query for every queued path.
+template <bool COUNT>
+__global__ void __launch_bounds__(kExtendBlock) k_extend(DevScene s, Wave w, int qin, unsigned long long* visitCounters)
+{
+    uint32_t nR = 0;
+    const uint32_t count = w.counters[qin];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.counters[qin ^ 1] = 0;  // consumed by shade(k-1); refilled by shade(k)
+    }
+    const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
+    uint32_t nI = 0, nL = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t slot = q[i];
+        const float4 o = w.ray_o[slot];
+        const float4 d = w.ray_d[slot];
+        HitRec h;
+        bool found = s.numNodes != 0 && trace_closest<COUNT>(s, xyz(o), o.w, xyz(d), h, nI, nL);
+        w.hit[slot] = found ? make_float4(h.u, h.v, h.t, __uint_as_float(h.instId))
+                            : make_float4(0.0f, 0.0f, 1e9f, __uint_as_float(SB_INVALID));
+        w.hitPrim[slot] = found ? h.primId : SB_INVALID;
+        if (COUNT) ++nR;
+    }
+    if (COUNT) {
+        atomicAdd(&visitCounters[0], (unsigned long long)nI);
+        atomicAdd(&visitCounters[1], (unsigned long long)nL);
+        atomicAdd(&visitCounters[4], (unsigned long long)nR);
+    }
+}
+
+__device__ __forceinline__ uint32_t warp_push(uint32_t* counter, bool pred)
+{
+    const unsigned mask = __ballot_sync(0xffffffffu, pred);
+    const int lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (mask != 0) {
+        const int leader = __ffs(mask) - 1;
+        if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, leader);
+    }
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// shade: one bounce of shading for every queued path; pushes surviving
+// paths to the other queue and next-event requests to the shadow queue.
+__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerParam ubo, Wave w, int qin)
+{
+    const uint32_t count = w.counters[qin];
+    const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
+    uint32_t* qout = qin ? w.queue[0] : w.queue[1];
+    const int maxDepth = (int)ubo.maxDepth;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
+        const uint32_t i = base + (threadIdx.x & 31u);
+        const bool valid = i < count;
+        bool cont = false;
+        ShadowReq sr;
+        sr.kind = 0;
+        uint32_t slot = 0;
+        if (valid) {
+            slot = q[i];
+            const float4 o = w.ray_o[slot];
+            const float4 d = w.ray_d[slot];
+            const float4 t4 = w.thr[slot];
+            const float4 c4 = w.col[slot];
+            PathState ps;
+            ps.ro = xyz(o);
+            ps.tmax = o.w;
+            ps.rd = xyz(d);
+            ps.lastPdf = d.w;
+            ps.throughput = xyz(t4);
+            const uint32_t fl = __float_as_uint(t4.w);
+            ps.depth = (int)(fl & 0xffffu);
+            ps.specular = (fl >> 16) & 1u;
+            ps.inside = (fl >> 17) & 1u;
+            ps.color = xyz(c4);
+            ps.rng = w.rng[slot];
+            const float4 h4 = w.hit[slot];
+            HitRec h;
+            h.u = h4.x;
+            h.v = h4.y;
+            h.t = h4.z;
+            h.instId = __float_as_uint(h4.w);
+            h.primId = w.hitPrim[slot];
+            const bool found = h.instId != SB_INVALID;
+            cont = shade(s, ubo, ps, found, h, sr);
+            if (cont) {
+                ++ps.depth;
+                cont = ps.depth < maxDepth;
+            }
+            w.ray_o[slot] = f4(ps.ro, ps.tmax);
+            w.ray_d[slot] = f4(ps.rd, ps.lastPdf);
+            w.thr[slot] = f4(ps.throughput, __uint_as_float(pack_flags(ps)));
+            w.col[slot] = f4(ps.color, 0.0f);
+            w.rng[slot] = ps.rng;
+        }
+        const uint32_t qpos = warp_push(&w.counters[qin ^ 1], cont);
+        if (cont) qout[qpos] = slot;
+        const bool hasShadow = sr.kind != 0;
+        const uint32_t spos = warp_push(&w.counters[2], hasShadow);
+        if (hasShadow) {
+            w.sh_o[spos] = f4(sr.o, sr.tmax);
+            w.sh_d[spos] = f4(sr.d, __uint_as_float(slot));
+            w.sh_cd[spos] = f4(sr.cd, __uint_as_float((uint32_t)sr.kind));
+            w.sh_cg[spos] = f4(sr.cg, 0.0f);
+        }
+    }
+}
+
+// shadow: any-hit query for every next-event request; adds visible ones.
+template <bool COUNT>
+__global__ void __launch_bounds__(kExtendBlock) k_shadow(DevScene s, Wave w, unsigned long long* visitCounters)
+{
+    const uint32_t count = w.counters[2];
+    uint32_t nI = 0, nL = 0, nR = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float4 o = w.sh_o[i];
+        const float4 d = w.sh_d[i];
+        const float4 cd = w.sh_cd[i];
+        const int kind = (int)__float_as_uint(cd.w);
+        bool visible;
+        if (COUNT) {
+            ++nR;
+            HitRec h;
+            h.instId = SB_INVALID;
+            bool occl = trace_any<true>(s, xyz(o), o.w, xyz(d), h, nI, nL);
+            visible = !occl || (kind == 1 && h.instId < s.numInstances && __ldg(&s.inst[h.instId].lightId) != -1);
+        } else {
+            visible = shadow_visible(s, kind, xyz(o), o.w, xyz(d));
+        }
+        if (visible) {
+            const uint32_t slot = __float_as_uint(d.w);
+            const float4 cg = w.sh_cg[i];
+            v3 c = xyz(w.col[slot]);
+            apply_shadow(c, xyz(cd), xyz(cg));
+            w.col[slot] = f4(c, 0.0f);
+        }
+    }
+    if (COUNT) {
+        atomicAdd(&visitCounters[2], (unsigned long long)nI);
+        atomicAdd(&visitCounters[3], (unsigned long long)nL);
+        atomicAdd(&visitCounters[5], (unsigned long long)nR);
+    }
+}
+
+__global__ void __launch_bounds__(kSmallBlock) k_reset_shadow(Wave w) { w.counters[2] = 0; }
+
+__global__ void __launch_bounds__(kSmallBlock) k_finalize(Wave w, float* __restrict__ sampleBuffer, uint64_t first, uint32_t n)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 c = w.col[i];
+        float* o = sampleBuffer + (first + i) * 3;
+        o[0] = c.x;
+        o[1] = c.y;
+        o[2] = c.z;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Ray-query microbenchmark kernels.
+template <bool ANY, bool COUNT, bool REFINE>
+__global__ void __launch_bounds__(kExtendBlock) k_trace(DevScene s, const float4* __restrict__ rays, Hit* __restrict__ hits,
+                                                        uint32_t n, unsigned long long* counters)
+{
+    uint32_t nI = 0, nL = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o = __ldg(&rays[2 * (size_t)i]);
+        const float4 d = __ldg(&rays[2 * (size_t)i + 1]);
+        HitRec h;
+        h.u = 0.0f;
+        h.v = 0.0f;
+        h.t = ANY ? 0.0f : 1e9f;
+        h.instId = SB_INVALID;
+        h.primId = SB_INVALID;
+        bool found = false;
+        if (s.numNodes != 0)
+            found = ANY ? trace_any<COUNT>(s, xyz(o), o.w, xyz(d), h, nI, nL)
+                        : trace_closest<COUNT>(s, xyz(o), o.w, xyz(d), h, nI, nL);
+        if (REFINE && found) refine_hit(s, xyz(o), xyz(d), h.instId, h.primId, h.t, h.u, h.v);
+        if (!found) {
+            h.instId = SB_INVALID;
+            h.primId = SB_INVALID;
+            if (!ANY) {
+                h.t = 1e9f;
+                h.u = 0.0f;
+                h.v = 0.0f;
+            }
+        }
+        uint32_t* out = reinterpret_cast<uint32_t*>(&hits[i]);
+        out[0] = __float_as_uint(h.u);
+        out[1] = __float_as_uint(h.v);
+        out[2] = __float_as_uint(h.t);
+        out[3] = h.instId;
+        out[4] = h.primId;
+    }
+    if (COUNT) {
+        atomicAdd(&counters[0], (unsigned long long)nI);
+        atomicAdd(&counters[1], (unsigned long long)nL);
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Pass object.
+struct StrelkaPathTracer {
+    StrelkaPathTracerConfig cfg{};
+    int device = 0;
+    int numSMs = 148;
+    // scene cache
+    uint64_t sceneVersion = ~0ull;
+    const void* keyNodes = nullptr;
+    const void* keyVb = nullptr;
+    const void* keyIb = nullptr;
+    const void* keyInst = nullptr;
+    uint32_t keyNumNodes = 0;
+    float4* tris = nullptr;
+    size_t trisCap = 0;  // nodes
+    float* srgbLut = nullptr;
+    uint32_t* status = nullptr;
+    // wavefront
+    Wave wave{};
+    size_t waveCap = 0;
+    std::vector<void*> waveAllocs;
+    // environment descriptor copy
+    StrelkaEnvMap env{};
+    // profiling
+    struct Rec { int kc; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> eventPool;
+    size_t eventsUsed = 0;
+    int extendGrid = 0, shadeGrid = 0, smallGrid = 0;
+    unsigned long long* visitCounters = nullptr;  // 6 entries (STRELKA_PT_COUNT)
+};
+
+namespace {
+
+void free_wave(StrelkaPathTracer* pt)
+{
+    for (void* p : pt->waveAllocs) cudaFree(p);
+    pt->waveAllocs.clear();
+    pt->wave = Wave{};
+    pt->waveCap = 0;
+}
+
+template <typename T>
+int walloc(StrelkaPathTracer* pt, T** p, size_t n)
+{
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(wavefront state)");
+    pt->waveAllocs.push_back(q);
+    *p = static_cast<T*>(q);
+    return STRELKA_OK;
+}
+
+int ensure_wave(StrelkaPathTracer* pt, size_t cap)
+{
+    if (pt->waveCap >= cap) return STRELKA_OK;
+    free_wave(pt);
+    Wave& w = pt->wave;
+    int rc;
+    if ((rc = walloc(pt, &w.ray_o, cap)) || (rc = walloc(pt, &w.ray_d, cap)) || (rc = walloc(pt, &w.thr, cap)) ||
+        (rc = walloc(pt, &w.col, cap)) || (rc = walloc(pt, &w.rng, cap)) || (rc = walloc(pt, &w.hit, cap)) ||
+        (rc = walloc(pt, &w.hitPrim, cap)) || (rc = walloc(pt, &w.queue[0], cap)) || (rc = walloc(pt, &w.queue[1], cap)) ||
+        (rc = walloc(pt, &w.sh_o, cap)) || (rc = walloc(pt, &w.sh_d, cap)) || (rc = walloc(pt, &w.sh_cd, cap)) ||
+        (rc = walloc(pt, &w.sh_cg, cap)) || (rc = walloc(pt, &w.counters, 4))) {
+        free_wave(pt);
+        return rc;
+    }
+    pt->waveCap = cap;
+    return STRELKA_OK;
+}
+
+cudaEvent_t next_event(StrelkaPathTracer* pt)
+{
+    if (pt->eventsUsed == pt->eventPool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        pt->eventPool.push_back(e);
+    }
+    return pt->eventPool[pt->eventsUsed++];
+}
+
+struct Timer {
+    StrelkaPathTracer* pt;
+    int kc;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    Timer(StrelkaPathTracer* p, int k, cudaStream_t s) : pt(p), kc(k), st(s)
+    {
+        if (pt->cfg.flags & STRELKA_PT_PROFILE) {
+            a = next_event(pt);
+            if (a) cudaEventRecord(a, st);
+        }
+    }
+    ~Timer()
+    {
+        if (a) {
+            cudaEvent_t b = next_event(pt);
+            if (b) {
+                cudaEventRecord(b, st);
+                pt->recs.push_back({kc, a, b});
+            }
+        }
+    }
+};
+
+void srgb_lut_host(float* lut)
+{
+    for (int i = 0; i < 256; ++i) {
+        float x = (float)i / 255.0f;
+        lut[i] = x <= 0.04045f ? x / 12.92f : powf((x + 0.055f) / 1.055f, 2.4f);
+    }
+}
+
+int check_scene_desc(const PathTracerDesc* d)
+{
+    if (!d) return fail(STRELKA_ERR_INVALID_ARGUMENT, "desc is NULL");
+    if (d->numNodes > (1u << 30)) return fail(STRELKA_ERR_INVALID_ARGUMENT, "numNodes %u exceeds 2^30", d->numNodes);
+    if (d->numNodes && (!d->bvhNodes || !d->vb || !d->ib || !d->instanceConst))
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "scene buffers must be non-NULL when numNodes > 0");
+    if (reinterpret_cast<uintptr_t>(d->bvhNodes) & 15) return fail(STRELKA_ERR_INVALID_ARGUMENT, "bvhNodes must be 16-byte aligned");
+    return STRELKA_OK;
+}
+
+// Refreshes the derived leaf-triangle table when the scene changed.
+int ensure_scene(StrelkaPathTracer* pt, const BVHNode* nodes, uint32_t numNodes, const Vertex* vb, uint32_t numVertices,
+                 const uint32_t* ib, uint32_t numIndices, const InstanceConstants* inst, uint32_t numInstances,
+                 uint64_t version, cudaStream_t st)
+{
+    if (pt->sceneVersion == version && pt->keyNodes == nodes && pt->keyVb == vb && pt->keyIb == ib && pt->keyInst == inst &&
+        pt->keyNumNodes == numNodes && pt->tris)
+        return STRELKA_OK;
+    if (numNodes > pt->trisCap || !pt->tris) {
+        if (pt->tris) cudaFree(pt->tris);
+        pt->tris = nullptr;
+        size_t cap = std::max<size_t>(numNodes, 1);
+        SB_CUDA_TRY(cudaMalloc(&pt->tris, cap * 3 * sizeof(float4)));
+        pt->trisCap = cap;
+    }
+    if (numNodes) {
+        Timer t(pt, KC_PREP, st);
+        int grid = std::min<int>((numNodes + 255) / 256, pt->numSMs * 16);
+        k_prep_tris<<<grid, 256, 0, st>>>(reinterpret_cast<const float4*>(nodes), numNodes, inst, numInstances, ib, numIndices,
+                                          vb, numVertices, pt->tris, pt->status);
+        SB_CUDA_TRY(cudaGetLastError());
+    }
+    pt->sceneVersion = version;
+    pt->keyNodes = nodes;
+    pt->keyVb = vb;
+    pt->keyIb = ib;
+    pt->keyInst = inst;
+    pt->keyNumNodes = numNodes;
+    return STRELKA_OK;
+}
+
+DevScene make_scene(StrelkaPathTracer* pt, const PathTracerDesc* d)
+{
+    DevScene s{};
+    s.nodes = reinterpret_cast<const float4*>(d->bvhNodes);
+    s.tris = pt->tris;
+    s.numNodes = d->numNodes;
+    s.numVertices = d->numVertices;
+    s.vb = d->vb;
+    s.ib = d->ib;
+    s.numIndices = d->numIndices;
+    s.numInstances = d->numInstances;
+    s.inst = d->instanceConst;
+    s.lights = d->lights;
+    s.lightCapacity = d->lights ? d->lightCapacity : 0;
+    s.numMaterials = d->mdl_mdlMaterial ? d->numMaterials : 0;
+    s.argBlock = d->mdl_argument_block;
+    s.argBlockBytes = d->mdl_argument_block ? d->argBlockBytes : 0;
+    s.materials = d->mdl_mdlMaterial;
+    s.resInfos = d->mdl_resource_infos;
+    s.numResInfos = d->mdl_resource_infos ? d->numResourceInfos : 0;
+    s.numTextures = d->matTextures ? d->numTextures : 0;
+    s.textures = d->matTextures;
+    s.srgbLut = pt->srgbLut;
+    s.hasEnv = d->envMap != nullptr;
+    if (d->envMap) s.env = *d->envMap;
+    s.status = pt->status;
+    return s;
+}
+
+int occupancy_grid(const void* fn, int block, int numSMs)
+{
+    int perSM = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, block, 0) != cudaSuccess || perSM < 1) perSM = 1;
+    return perSM * numSMs;
+}
+
+}  // namespace
+
+extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, StrelkaPathTracer** out)
+{
+    if (!out) return fail(STRELKA_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(STRELKA_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+    auto* pt = new StrelkaPathTracer();
+    if (config) pt->cfg = *config;
+    if (pt->cfg.mode > STRELKA_MODE_MEGAKERNEL) {
+        delete pt;
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "unknown mode %u", config->mode);
+    }
+    pt->device = dev;
+    cudaDeviceGetAttribute(&pt->numSMs, cudaDevAttrMultiProcessorCount, dev);
+    float lut[256];
+    srgb_lut_host(lut);
+    if (cudaMalloc(&pt->srgbLut, sizeof(lut)) != cudaSuccess || cudaMalloc(&pt->status, sizeof(uint32_t)) != cudaSuccess) {
+        strelka_pathtracer_destroy(pt);
+        return fail(STRELKA_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+    }
+    cudaMemcpy(pt->srgbLut, lut, sizeof(lut), cudaMemcpyHostToDevice);
+    cudaMemset(pt->status, 0, sizeof(uint32_t));
+    if (cudaMalloc(&pt->visitCounters, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+        strelka_pathtracer_destroy(pt);
+        return fail(STRELKA_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+    }
+    cudaMemset(pt->visitCounters, 0, 8 * sizeof(unsigned long long));
+    pt->extendGrid = occupancy_grid((const void*)k_extend<false>, kExtendBlock, pt->numSMs);
+    pt->shadeGrid = occupancy_grid((const void*)k_shade, kShadeBlock, pt->numSMs);
+    pt->smallGrid = pt->numSMs * 8;
+    *out = pt;
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
+{
+    if (!pt) return STRELKA_OK;
+    free_wave(pt);
+    if (pt->tris) cudaFree(pt->tris);
+    if (pt->srgbLut) cudaFree(pt->srgbLut);
+    if (pt->status) cudaFree(pt->status);
+    if (pt->visitCounters) cudaFree(pt->visitCounters);
+    for (cudaEvent_t e : pt->eventPool) cudaEventDestroy(e);
+    delete pt;
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTracerDesc* desc, uint32_t w, uint32_t h,
+                                          uint64_t frameIndex, void* stream)
+{
+    (void)frameIndex;
+    if (!pt) return fail(STRELKA_ERR_INVALID_ARGUMENT, "path tracer is NULL");
+    int rc = check_scene_desc(desc);
+    if (rc) return rc;
+    const PathTracerParam& ubo = desc->constants;
+    if (ubo.dimension[0] <= 0 || ubo.dimension[1] <= 0 || ubo.spp <= 0)
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "dimension and spp must be positive");
+    const uint64_t total = (uint64_t)ubo.dimension[0] * (uint64_t)ubo.dimension[1] * (uint64_t)ubo.spp;
+    if (total > 0xFFFFFFFFull) return fail(STRELKA_ERR_INVALID_ARGUMENT, "W*H*spp exceeds 2^32");
+    if ((uint64_t)w * (h ? h : 1) != total)
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "w*h (%u*%u) must equal W*H*spp (%llu)", w, h, (unsigned long long)total);
+    if (!desc->sampleBuffer) return fail(STRELKA_ERR_INVALID_ARGUMENT, "sampleBuffer is NULL");
+    if (desc->envMap) {
+        const StrelkaEnvMap* e = desc->envMap;
+        if (!e->rgba32f || !e->marginal_cdf || !e->conditional_cdf || e->width == 0 || e->height == 0)
+            return fail(STRELKA_ERR_INVALID_ARGUMENT, "incomplete environment map");
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    rc = ensure_scene(pt, desc->bvhNodes, desc->numNodes, desc->vb, desc->numVertices, desc->ib, desc->numIndices,
+                      desc->instanceConst, desc->numInstances, desc->sceneVersion, st);
+    if (rc) return rc;
+    DevScene s = make_scene(pt, desc);
+
+    if (pt->cfg.mode == STRELKA_MODE_MEGAKERNEL) {
+        Timer t(pt, KC_MEGAKERNEL, st);
+        const uint64_t blocks = (total + kExtendBlock - 1) / kExtendBlock;
+        k_megakernel<<<(unsigned)blocks, kExtendBlock, 0, st>>>(s, ubo, desc->sampleBuffer, 0, total);
+        SB_CUDA_TRY(cudaGetLastError());
+        return STRELKA_OK;
+    }
+
+    // wavefront
+    size_t chunk = pt->cfg.chunkPaths ? pt->cfg.chunkPaths : (size_t)1 << 22;
+    chunk = std::min<size_t>(chunk, total);
+    rc = ensure_wave(pt, chunk);
+    if (rc) return rc;
+    const int maxDepth = (int)ubo.maxDepth;
+    for (uint64_t first = 0; first < total; first += chunk) {
+        const uint32_t n = (uint32_t)std::min<uint64_t>(chunk, total - first);
+        {
+            Timer t(pt, KC_GENERATE, st);
+            int grid = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, pt->smallGrid);
+            k_generate<<<grid, kSmallBlock, 0, st>>>(ubo, pt->wave, first, n);
+        }
+        for (int depth = 0; depth < maxDepth; ++depth) {
+            const int qin = depth & 1;
+            const int gridE = std::min<int>((n + kExtendBlock - 1) / kExtendBlock, pt->extendGrid);
+            const int gridS = std::min<int>((n + kShadeBlock - 1) / kShadeBlock, pt->shadeGrid);
+            const bool count = (pt->cfg.flags & STRELKA_PT_COUNT) != 0;
+            {
+                Timer t(pt, KC_EXTEND, st);
+                if (count) k_extend<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, qin, pt->visitCounters);
+                else k_extend<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, qin, nullptr);
+            }
+            {
+                Timer t(pt, KC_SHADE, st);
+                k_shade<<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->wave, qin);
+            }
+            {
+                Timer t(pt, KC_SHADOW, st);
+                if (count) k_shadow<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, pt->visitCounters);
+                else k_shadow<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, nullptr);
+                k_reset_shadow<<<1, 1, 0, st>>>(pt->wave);
+            }
+        }
+        {
+            Timer t(pt, KC_FINALIZE, st);
+            int grid = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, pt->smallGrid);
+            k_finalize<<<grid, kSmallBlock, 0, st>>>(pt->wave, desc->sampleBuffer, first, n);
+        }
+        SB_CUDA_TRY(cudaGetLastError());
+    }
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_pathtracer_get_device_status(StrelkaPathTracer* pt, void* stream, uint32_t* status)
+{
+    if (!pt || !status) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    SB_CUDA_TRY(cudaStreamSynchronize(st));
+    SB_CUDA_TRY(cudaMemcpy(status, pt->status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    SB_CUDA_TRY(cudaMemset(pt->status, 0, sizeof(uint32_t)));
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_pathtracer_get_kernel_times(StrelkaPathTracer* pt, void* stream, float* ms_out, uint32_t* launches_out,
+                                                   uint32_t capacity)
+{
+    if (!pt) return -STRELKA_ERR_INVALID_ARGUMENT;
+    cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    std::vector<float> ms(KC_COUNT, 0.0f);
+    std::vector<uint32_t> cnt(KC_COUNT, 0);
+    for (auto& r : pt->recs) {
+        float t = 0.0f;
+        if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+            ms[r.kc] += t;
+            cnt[r.kc] += 1;
+        }
+    }
+    for (uint32_t i = 0; i < capacity && i < (uint32_t)KC_COUNT; ++i) {
+        if (ms_out) ms_out[i] = ms[i];
+        if (launches_out) launches_out[i] = cnt[i];
+    }
+    pt->recs.clear();
+    pt->eventsUsed = 0;
+    return KC_COUNT;
+}
+
+extern "C" int strelka_pathtracer_get_counters(StrelkaPathTracer* pt, void* stream, unsigned long long* out,
+                                               uint32_t capacity)
+{
+    if (!pt || (!out && capacity)) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned long long tmp[6];
+    SB_CUDA_TRY(cudaMemcpyAsync(tmp, pt->visitCounters, sizeof(tmp), cudaMemcpyDeviceToHost, st));
+    SB_CUDA_TRY(cudaStreamSynchronize(st));
+    SB_CUDA_TRY(cudaMemsetAsync(pt->visitCounters, 0, sizeof(tmp), st));
+    for (uint32_t i = 0; i < capacity && i < 6; ++i) out[i] = tmp[i];
+    return 6;
+}
+
+extern "C" const char* strelka_kernel_class_name(int i) { return (i >= 0 && i < KC_COUNT) ? kKernelNames[i] : ""; }
+
+// ---------------------------------------------------------------------------
+extern "C" int strelka_trace_execute(StrelkaPathTracer* pt, const TraceDesc* d, void* stream)
+{
+    if (!pt || !d) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (d->numNodes > (1u << 30)) return fail(STRELKA_ERR_INVALID_ARGUMENT, "numNodes exceeds 2^30");
+    if (d->numNodes && (!d->bvhNodes || !d->vb || !d->ib || !d->instanceConst))
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "scene buffers must be non-NULL when numNodes > 0");
+    if (d->numRays && (!d->rays || !d->hits)) return fail(STRELKA_ERR_INVALID_ARGUMENT, "rays/hits NULL");
+    if ((d->flags & STRELKA_TRACE_COUNT) && !d->counters) return fail(STRELKA_ERR_INVALID_ARGUMENT, "counters NULL");
+    if ((d->flags & STRELKA_TRACE_REFINE) && (d->flags & STRELKA_TRACE_ANY))
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "refine applies to closest-hit queries only");
+    if (reinterpret_cast<uintptr_t>(d->rays) & 15) return fail(STRELKA_ERR_INVALID_ARGUMENT, "rays must be 16-byte aligned");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = ensure_scene(pt, d->bvhNodes, d->numNodes, d->vb, d->numVertices, d->ib, d->numIndices, d->instanceConst,
+                          d->numInstances, d->sceneVersion, st);
+    if (rc) return rc;
+    if (d->numRays == 0) return STRELKA_OK;
+    PathTracerDesc pd{};
+    pd.bvhNodes = d->bvhNodes;
+    pd.numNodes = d->numNodes;
+    pd.vb = d->vb;
+    pd.numVertices = d->numVertices;
+    pd.ib = d->ib;
+    pd.numIndices = d->numIndices;
+    pd.instanceConst = d->instanceConst;
+    pd.numInstances = d->numInstances;
+    DevScene s = make_scene(pt, &pd);
+    const bool any = (d->flags & 1u) != 0;
+    const bool cnt = (d->flags & STRELKA_TRACE_COUNT) != 0;
+    const bool refine = (d->flags & STRELKA_TRACE_REFINE) != 0;
+    const int grid = std::min<int>((d->numRays + kExtendBlock - 1) / kExtendBlock, pt->extendGrid);
+    const float4* rays = reinterpret_cast<const float4*>(d->rays);
+    Timer t(pt, KC_EXTEND, st);
+    if (any && cnt) k_trace<true, true, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, d->counters);
+    else if (any) k_trace<true, false, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, nullptr);
+    else if (refine && cnt)
+        k_trace<false, true, true><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, d->counters);
+    else if (refine) k_trace<false, false, true><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, nullptr);
+    else if (cnt) k_trace<false, true, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, d->counters);
+    else k_trace<false, false, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, nullptr);
+    SB_CUDA_TRY(cudaGetLastError());
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_trace_host(StrelkaPathTracer* pt, const TraceDesc* desc, const Ray* hostRays, Hit* hostHits, void* stream)
+{
+    if (!pt || !desc || (desc->numRays && (!hostRays || !hostHits)))
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!desc->rays || !desc->hits) return fail(STRELKA_ERR_INVALID_ARGUMENT, "device staging rays/hits are NULL");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    SB_CUDA_TRY(cudaMemcpyAsync((void*)desc->rays, hostRays, (size_t)desc->numRays * sizeof(Ray), cudaMemcpyHostToDevice, st));
+    int rc = strelka_trace_execute(pt, desc, stream);
+    if (rc) return rc;
+    SB_CUDA_TRY(cudaMemcpyAsync(hostHits, desc->hits, (size_t)desc->numRays * sizeof(Hit), cudaMemcpyDeviceToHost, st));
+    SB_CUDA_TRY(cudaStreamSynchronize(st));
+    return STRELKA_OK;
+}

@@ -1,0 +1,216 @@
+// post.cu — reduction, accumulation and tonemap passes, sm_100a.
+//
+// ReductionPass   shaders/reduction.hlsl:9-32     (mean of spp samples)
+// Accumulation    shaders/accumulation.hlsl:86-97 (progressive running mean)
+// Tonemap         shaders/tonemap.hlsl:9-88       (Reinhard / ACESFitted / ACESFilm)
+// and strelka_resolve_execute, which runs the three as one pass over the
+// sample buffer with the same per-pixel arithmetic (so its output equals the
+// three passes run in sequence) and optionally also writes RGBA8.
+#include <cstdint>
+
+#include "common.h"
+#include "device_math.cuh"
+
+using namespace sb;
+
+namespace {
+
+__device__ __forceinline__ v3 reduce_pixel(const float* __restrict__ sb, uint64_t pixel, int spp, float invSpp)
+{
+    float r = 0.0f, g = 0.0f, b = 0.0f;
+    const float* p = sb + pixel * (uint64_t)spp * 3;
+    for (int s = 0; s < spp; ++s) {
+        r += invSpp * __ldg(p + 3 * s + 0);
+        g += invSpp * __ldg(p + 3 * s + 1);
+        b += invSpp * __ldg(p + 3 * s + 2);
+    }
+    return V(r, g, b);
+}
+
+__device__ __forceinline__ v3 accumulate_pixel(v3 cur, v3 prev, float wHistory, float wNew)
+{
+    return V(prev.x * wHistory + cur.x * wNew, prev.y * wHistory + cur.y * wNew, prev.z * wHistory + cur.z * wNew);
+}
+
+// tonemap.hlsl:9-64
+__device__ __forceinline__ v3 aces_fitted(v3 c)
+{
+    v3 a = V((0.59719f * c.x + 0.35458f * c.y) + 0.04823f * c.z, (0.07600f * c.x + 0.90834f * c.y) + 0.01566f * c.z,
+             (0.02840f * c.x + 0.13383f * c.y) + 0.83777f * c.z);
+    float v[3] = {a.x, a.y, a.z}, r[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float aa = v[i] * (v[i] + 0.0245786f) - 0.000090537f;
+        float bb = v[i] * (0.983729f * v[i] + 0.4329510f) + 0.238081f;
+        r[i] = aa / bb;
+    }
+    v3 o = V((1.60475f * r[0] + -0.53108f * r[1]) + -0.07367f * r[2], (-0.10208f * r[0] + 1.10813f * r[1]) + -0.00605f * r[2],
+             (-0.00327f * r[0] + -0.07276f * r[1]) + 1.07602f * r[2]);
+    return V(fsat(o.x), fsat(o.y), fsat(o.z));
+}
+__device__ __forceinline__ float aces_film1(float x)
+{
+    const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+    return fsat((x * (a * x + b)) / (x * (c * x + d) + e));
+}
+__device__ __forceinline__ v3 reinhard(v3 c)
+{
+    float lum = (c.x * 0.299f + c.y * 0.587f) + c.z * 0.114f;
+    float r = lum / (lum + 1.0f);
+    float k = r / lum;
+    return V(c.x * k, c.y * k, c.z * k);
+}
+__device__ __forceinline__ bool tonemap_pixel(uint32_t type, v3 c, v3& out)
+{
+    if (type == 0) out = reinhard(c);
+    else if (type == 1) out = aces_fitted(c);
+    else if (type == 2) out = V(aces_film1(c.x), aces_film1(c.y), aces_film1(c.z));
+    else return false;
+    return true;
+}
+
+__device__ __forceinline__ uint8_t to_u8(float x)
+{
+    float s = fsat(x) * 255.0f + 0.5f;
+    return (uint8_t)(int)s;
+}
+
+__global__ void k_reduce(const float* __restrict__ sb, float4* __restrict__ out, uint32_t npix, int spp)
+{
+    const float invSpp = 1.0f / (float)spp;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+        v3 c = reduce_pixel(sb, i, spp, invSpp);
+        out[i] = make_float4(c.x, c.y, c.z, 1.0f);
+    }
+}
+
+__global__ void k_accumulate(const float4* __restrict__ in, const float4* __restrict__ hist, float4* __restrict__ out,
+                             uint32_t npix, float wHistory, float wNew)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+        v3 r = accumulate_pixel(xyz(in[i]), xyz(hist[i]), wHistory, wNew);
+        out[i] = make_float4(r.x, r.y, r.z, 1.0f);
+    }
+}
+
+__global__ void k_tonemap(const float4* __restrict__ in, float4* __restrict__ out, uint32_t npix, uint32_t type)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+        v3 r;
+        if (tonemap_pixel(type, xyz(in[i]), r)) out[i] = make_float4(r.x, r.y, r.z, 1.0f);
+    }
+}
+
+__global__ void k_resolve(const float* __restrict__ sb, int spp, uint32_t npix, int accumulate, const float4* __restrict__ hist,
+                          float wHistory, float wNew, float4* __restrict__ accOut, uint32_t tmType, float4* __restrict__ tmOut,
+                          uchar4* __restrict__ tm8)
+{
+    const float invSpp = 1.0f / (float)spp;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+        v3 c = reduce_pixel(sb, i, spp, invSpp);
+        if (accumulate) c = accumulate_pixel(c, xyz(hist[i]), wHistory, wNew);
+        if (accOut) accOut[i] = make_float4(c.x, c.y, c.z, 1.0f);
+        v3 t;
+        if (tonemap_pixel(tmType, c, t)) {
+            if (tmOut) tmOut[i] = make_float4(t.x, t.y, t.z, 1.0f);
+            if (tm8) tm8[i] = make_uchar4(to_u8(t.x), to_u8(t.y), to_u8(t.z), 255);
+        }
+    }
+}
+
+int grid_for(uint32_t n)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    uint32_t blocks = (n + 255) / 256;
+    uint32_t cap = (uint32_t)sms * 16;
+    return (int)(blocks < cap ? (blocks ? blocks : 1) : cap);
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+}  // namespace
+
+extern "C" int strelka_reduction_execute(const ReductionDesc* d, uint32_t w, uint32_t h, uint64_t frameIndex, void* stream)
+{
+    (void)frameIndex;
+    if (!d || !d->sampleBuffer || !d->result) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    const PathTracerParam& p = d->constants;
+    if (p.dimension[0] <= 0 || p.dimension[1] <= 0 || p.spp <= 0) return fail(STRELKA_ERR_INVALID_ARGUMENT, "bad dimension/spp");
+    const uint64_t npix = (uint64_t)p.dimension[0] * (uint64_t)p.dimension[1];
+    if ((uint64_t)w * (h ? h : 1) != npix) return fail(STRELKA_ERR_INVALID_ARGUMENT, "w*h must equal W*H");
+    if (!aligned16(d->result)) return fail(STRELKA_ERR_INVALID_ARGUMENT, "result must be 16-byte aligned");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_reduce<<<grid_for((uint32_t)npix), 256, 0, st>>>(d->sampleBuffer, reinterpret_cast<float4*>(d->result), (uint32_t)npix,
+                                                      p.spp);
+    SB_CUDA_TRY(cudaGetLastError());
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_accumulation_execute(const AccumulationDesc* d, uint32_t w, uint32_t h, uint64_t frameIndex, void* stream)
+{
+    (void)frameIndex;
+    if (!d || !d->input || !d->history || !d->output) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    const AccumulationParam& p = d->constants;
+    if (p.dimension[0] <= 0 || p.dimension[1] <= 0) return fail(STRELKA_ERR_INVALID_ARGUMENT, "bad dimension");
+    if ((int64_t)w != p.dimension[0] || (int64_t)h != p.dimension[1])
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "w,h must equal the dimension");
+    if (!aligned16(d->input) || !aligned16(d->history) || !aligned16(d->output))
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "images must be 16-byte aligned");
+    const uint32_t npix = (uint32_t)p.dimension[0] * (uint32_t)p.dimension[1];
+    // accumulation.hlsl:88-89
+    const float wHistory = (float)p.iteration / (float)(p.iteration + 1u);
+    const float wNew = 1.0f / (float)(p.iteration + 1u);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_accumulate<<<grid_for(npix), 256, 0, st>>>(reinterpret_cast<const float4*>(d->input),
+                                                 reinterpret_cast<const float4*>(d->history),
+                                                 reinterpret_cast<float4*>(d->output), npix, wHistory, wNew);
+    SB_CUDA_TRY(cudaGetLastError());
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_tonemap_execute(const TonemapDesc* d, uint32_t w, uint32_t h, uint64_t frameIndex, void* stream)
+{
+    (void)frameIndex;
+    if (!d || !d->input || !d->output) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    const Tonemapparam& p = d->constants;
+    if (p.dimension[0] <= 0 || p.dimension[1] <= 0) return fail(STRELKA_ERR_INVALID_ARGUMENT, "bad dimension");
+    if ((int64_t)w != p.dimension[0] || (int64_t)h != p.dimension[1])
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "w,h must equal the dimension");
+    if (!aligned16(d->input) || !aligned16(d->output)) return fail(STRELKA_ERR_INVALID_ARGUMENT, "images must be 16-byte aligned");
+    const uint32_t npix = (uint32_t)p.dimension[0] * (uint32_t)p.dimension[1];
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_tonemap<<<grid_for(npix), 256, 0, st>>>(reinterpret_cast<const float4*>(d->input), reinterpret_cast<float4*>(d->output),
+                                              npix, p.tonemapperType);
+    SB_CUDA_TRY(cudaGetLastError());
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_resolve_execute(const PathTracerParam* pp, const float* sampleBuffer, int accumulate,
+                                       const AccumulationParam* ap, const float* history, float* accOutput,
+                                       const Tonemapparam* tp, float* tonemapOutput, uint8_t* tonemapRGBA8, void* stream)
+{
+    if (!pp || !sampleBuffer || !tp) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (pp->dimension[0] <= 0 || pp->dimension[1] <= 0 || pp->spp <= 0)
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "bad dimension/spp");
+    if (accumulate && (!ap || !history)) return fail(STRELKA_ERR_INVALID_ARGUMENT, "accumulation needs param and history");
+    if (tp->dimension[0] != pp->dimension[0] || tp->dimension[1] != pp->dimension[1])
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "tonemap dimension mismatch");
+    if ((accOutput && !aligned16(accOutput)) || (tonemapOutput && !aligned16(tonemapOutput)) ||
+        (history && !aligned16(history)) || (tonemapRGBA8 && (reinterpret_cast<uintptr_t>(tonemapRGBA8) & 3)))
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "misaligned image");
+    const uint32_t npix = (uint32_t)pp->dimension[0] * (uint32_t)pp->dimension[1];
+    float wH = 0.0f, wN = 1.0f;
+    if (accumulate) {
+        wH = (float)ap->iteration / (float)(ap->iteration + 1u);
+        wN = 1.0f / (float)(ap->iteration + 1u);
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_resolve<<<grid_for(npix), 256, 0, st>>>(sampleBuffer, pp->spp, npix, accumulate, reinterpret_cast<const float4*>(history),
+                                              wH, wN, reinterpret_cast<float4*>(accOutput), tp->tonemapperType,
+                                              reinterpret_cast<float4*>(tonemapOutput),
+                                              reinterpret_cast<uchar4*>(tonemapRGBA8));
+    SB_CUDA_TRY(cudaGetLastError());
+    return STRELKA_OK;
+}

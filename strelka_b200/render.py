@@ -1,0 +1,228 @@
+"""Python mirror of Strelka's render-pass API over the C ABI.
+
+The reference records its passes as ``ComputePass<T>::execute(cmd, desc, w,
+h, frameIndex)`` (include/render/computepass.h:8-164):
+
+* ``PathTracer``     include/render/pathtracer.h:33-50, src/render/pathtracer.cpp
+* ``ReductionPass``  include/render/reduction.h, src/render/reduction.cpp
+* ``Accumulation``   include/render/accumulation.h, src/render/accumulation.cpp
+* ``Tonemap``        include/render/tonemap.h, src/render/tonemap.cpp
+
+The classes below keep those names, descriptor contents and argument meaning;
+a CUDA stream (an int handle, 0 = the legacy default stream) stands in for
+the command buffer.  Device buffers are torch CUDA tensors (plumbing only);
+all work runs in ``libstrelka_b200.so`` and raises :class:`abi.StrelkaError`
+on any failure status.
+
+:class:`DeviceScene` plays the role of the reference's ResourceManager for
+the scene buffers created at frame 0 (src/render/ptrender.cpp:412-667).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _stream_handle(stream) -> C.c_void_p:
+    if stream is None:
+        return C.c_void_p(0)
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(stream.cuda_stream)
+
+
+def to_device(arr: np.ndarray, device="cuda"):
+    """Copies a numpy array to a uint8 CUDA tensor (16-byte aligned by the allocator)."""
+    torch = _torch()
+    a = np.ascontiguousarray(arr)
+    t = torch.from_numpy(a.view(np.uint8).reshape(-1).copy())
+    return t.to(device)
+
+
+def ptr(t) -> int:
+    return 0 if t is None else int(t.data_ptr())
+
+
+class DeviceScene:
+    """Device copies of a HostScene's buffers plus the descriptor fields."""
+
+    _version = 1
+
+    def __init__(self, hs, device="cuda", with_env: bool = True):
+        torch = _torch()
+        self.hs = hs
+        self.device = device
+        self.nodes = to_device(hs.nodes if hs.nodes.size else np.zeros(32, np.uint8), device)
+        self.vb = to_device(hs.vb if hs.vb.size else np.zeros(32, np.uint8), device)
+        self.ib = to_device(hs.ib if hs.ib.size else np.zeros(1, np.uint32), device)
+        self.instances = to_device(hs.instances if hs.instances.size else np.zeros(208, np.uint8), device)
+        self.lights = to_device(hs.lights, device)
+        self.materials = to_device(hs.materials if hs.materials.size else np.zeros(16, np.uint8), device)
+        self.args = to_device(hs.arg_block if hs.arg_block.size else np.zeros(48, np.uint8), device)
+        self.resinfo = to_device(hs.resource_infos if hs.resource_infos.size else np.zeros(16, np.uint8), device)
+        self.tex_data = [to_device(t, device) for t in hs.textures]
+        texs = (abi.StrelkaTexture * max(len(hs.textures), 1))()
+        for i, (t, d) in enumerate(zip(hs.textures, self.tex_data)):
+            texs[i] = abi.StrelkaTexture(ptr(d), t.shape[1], t.shape[0], 0)
+        self.tex_table = to_device(np.frombuffer(texs, np.uint8), device)
+        self.env = None
+        if with_env and hs.env is not None:
+            self.env_rgba = to_device(hs.env, device)
+            self.env_marg = to_device(hs.env_marginal, device)
+            self.env_cond = to_device(hs.env_conditional, device)
+            self.env = abi.StrelkaEnvMap(ptr(self.env_rgba), ptr(self.env_marg), ptr(self.env_cond), hs.env.shape[1],
+                                         hs.env.shape[0], hs.env_integral, 0.0)
+        self.version = DeviceScene._version
+        DeviceScene._version += 1
+        torch.cuda.synchronize()
+
+    def desc(self, param, sample_buffer) -> abi.PathTracerDesc:
+        hs = self.hs
+        d = abi.PathTracerDesc()
+        d.constants = param
+        d.bvhNodes = ptr(self.nodes)
+        d.numNodes = hs.num_nodes
+        d.vb = ptr(self.vb)
+        d.numVertices = hs.num_vertices
+        d.ib = ptr(self.ib)
+        d.numIndices = hs.ib.size
+        d.instanceConst = ptr(self.instances)
+        d.numInstances = hs.num_instances
+        d.lights = ptr(self.lights)
+        d.lightCapacity = hs.lights.size // 112
+        d.sampleBuffer = ptr(sample_buffer)
+        d.mdl_argument_block = ptr(self.args)
+        d.argBlockBytes = hs.arg_block.size
+        d.mdl_resource_infos = ptr(self.resinfo)
+        d.numResourceInfos = hs.resource_infos.size // 16
+        d.mdl_mdlMaterial = ptr(self.materials)
+        d.numMaterials = hs.num_materials
+        d.matTextures = ptr(self.tex_table) if hs.textures else 0
+        d.numTextures = len(hs.textures)
+        d.envMap = C.cast(C.pointer(self.env), C.c_void_p).value if self.env is not None else None
+        d.sceneVersion = self.version
+        return d
+
+    def trace_desc(self, rays, hits, flags: int, counters=None) -> abi.TraceDesc:
+        hs = self.hs
+        d = abi.TraceDesc()
+        d.bvhNodes = ptr(self.nodes)
+        d.numNodes = hs.num_nodes
+        d.vb = ptr(self.vb)
+        d.numVertices = hs.num_vertices
+        d.ib = ptr(self.ib)
+        d.numIndices = hs.ib.size
+        d.instanceConst = ptr(self.instances)
+        d.numInstances = hs.num_instances
+        d.rays = ptr(rays)
+        d.hits = ptr(hits)
+        d.numRays = 0 if rays is None else rays.numel() * rays.element_size() // 32
+        d.flags = flags
+        d.counters = ptr(counters)
+        d.sceneVersion = self.version
+        return d
+
+
+class PathTracer:
+    """PathTracer pass (include/render/pathtracer.h:33-50)."""
+
+    def __init__(self, mode: int = abi.MODE_WAVEFRONT, chunk_paths: int = 0, profile: bool = False,
+                 count: bool = False):
+        self.lib = abi.load()
+        flags = (abi.PT_PROFILE if profile else 0) | (abi.PT_COUNT if count else 0)
+        cfg = abi.StrelkaPathTracerConfig(mode, chunk_paths, 0, flags)
+        h = C.c_void_p()
+        abi.check(self.lib.strelka_pathtracer_create(C.byref(cfg), C.byref(h)))
+        self.handle = h
+
+    def execute(self, desc: abi.PathTracerDesc, w: int, h: int, frame_index: int = 0, stream=None) -> None:
+        abi.check(self.lib.strelka_pathtracer_execute(self.handle, C.byref(desc), w, h, frame_index,
+                                                      _stream_handle(stream)))
+
+    def trace(self, desc: abi.TraceDesc, stream=None) -> None:
+        abi.check(self.lib.strelka_trace_execute(self.handle, C.byref(desc), _stream_handle(stream)))
+
+    def device_status(self, stream=None) -> int:
+        st = C.c_uint32(0)
+        abi.check(self.lib.strelka_pathtracer_get_device_status(self.handle, _stream_handle(stream), C.byref(st)))
+        return st.value
+
+    def kernel_times(self, stream=None) -> dict:
+        n = len(abi.KERNEL_CLASSES)
+        ms = (C.c_float * n)()
+        cnt = (C.c_uint32 * n)()
+        self.lib.strelka_pathtracer_get_kernel_times(self.handle, _stream_handle(stream), ms, cnt, n)
+        return {name: (ms[i], cnt[i]) for i, name in enumerate(abi.KERNEL_CLASSES)}
+
+    def counters(self, stream=None) -> dict:
+        """Traversal visit counters since the last call (needs count=True)."""
+        out = (C.c_uint64 * 6)()
+        self.lib.strelka_pathtracer_get_counters(self.handle, _stream_handle(stream), out, 6)
+        keys = ["extend_inner", "extend_leaf", "shadow_inner", "shadow_leaf", "extend_rays", "shadow_rays"]
+        return {k: int(out[i]) for i, k in enumerate(keys)}
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.strelka_pathtracer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ReductionPass:
+    """ReductionPass (shaders/reduction.hlsl:9-32)."""
+
+    def execute(self, desc: abi.ReductionDesc, w: int, h: int, frame_index: int = 0, stream=None) -> None:
+        abi.check(abi.load().strelka_reduction_execute(C.byref(desc), w, h, frame_index, _stream_handle(stream)))
+
+
+class Accumulation:
+    """Accumulation (shaders/accumulation.hlsl:86-108)."""
+
+    def execute(self, desc: abi.AccumulationDesc, w: int, h: int, frame_index: int = 0, stream=None) -> None:
+        abi.check(abi.load().strelka_accumulation_execute(C.byref(desc), w, h, frame_index, _stream_handle(stream)))
+
+
+class Tonemap:
+    """Tonemap (shaders/tonemap.hlsl:66-88)."""
+
+    def execute(self, desc: abi.TonemapDesc, w: int, h: int, frame_index: int = 0, stream=None) -> None:
+        abi.check(abi.load().strelka_tonemap_execute(C.byref(desc), w, h, frame_index, _stream_handle(stream)))
+
+
+def resolve(pt_param, sample_buffer, tm_param, acc_param=None, history=None, acc_out=None, tonemap_out=None,
+            rgba8_out=None, stream=None) -> None:
+    """Fused reduce + accumulate + tonemap (strelka_resolve_execute)."""
+    lib = abi.load()
+    acc = acc_param is not None
+    abi.check(lib.strelka_resolve_execute(C.byref(pt_param), ptr(sample_buffer), 1 if acc else 0,
+                                          C.byref(acc_param) if acc else None, ptr(history), ptr(acc_out),
+                                          C.byref(tm_param), ptr(tonemap_out), ptr(rgba8_out), _stream_handle(stream)))
+
+
+def accumulation_param(width: int, height: int, iteration: int) -> abi.AccumulationParam:
+    """The fields PtRender::drawFrame fills (src/render/ptrender.cpp:805-825) that the kernel reads."""
+    p = abi.AccumulationParam()
+    p.dimension[0] = width
+    p.dimension[1] = height
+    p.iteration = iteration
+    p.alpha = 0.1
+    p.isPt = 1.0
+    return p
+
+
+def tonemap_param(width: int, height: int, kind: int) -> abi.Tonemapparam:
+    return abi.Tonemapparam((width, height), kind, 0)

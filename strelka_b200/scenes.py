@@ -1,0 +1,159 @@
+"""Host-side synthetic scenes (wrappers over ``strelka_scene_*``).
+
+A :class:`HostScene` owns numpy copies of the buffers the reference uploads
+at frame 0 (vertices, indices, instance constants, lights, MDL material
+tables, textures, the environment map and the flattened BVH) plus a
+``PathTracerParam`` template holding the camera.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+
+
+def _np(ptr, count: int, ctype) -> np.ndarray:
+    """Copies `count` elements of a ctypes array pointer into a uint8 numpy array."""
+    nbytes = count * C.sizeof(ctype)
+    if nbytes == 0 or not ptr:
+        return np.zeros(0, np.uint8)
+    buf = (C.c_uint8 * nbytes).from_address(C.addressof(ptr.contents))
+    return np.frombuffer(buf, dtype=np.uint8).copy()
+
+
+@dataclass
+class HostScene:
+    vb: np.ndarray            # uint8, numVertices * 32
+    ib: np.ndarray            # uint32
+    instances: np.ndarray     # uint8, numInstances * 208
+    lights: np.ndarray        # uint8, max(numLights, 1) * 112
+    num_lights: int
+    materials: np.ndarray     # uint8, numMaterials * 16
+    arg_block: np.ndarray     # uint8
+    resource_infos: np.ndarray  # uint8, n * 16
+    textures: list = field(default_factory=list)  # list of (H, W, 4) uint8
+    env: np.ndarray | None = None           # (H, W, 4) float32
+    env_marginal: np.ndarray | None = None  # float32 H+1
+    env_conditional: np.ndarray | None = None  # float32 H*(W+1)
+    env_integral: float = 0.0
+    nodes: np.ndarray = None  # uint8, numNodes * 32
+    num_triangles: int = 0
+    camera: abi.PathTracerParam = None
+
+    @property
+    def num_vertices(self) -> int:
+        return self.vb.size // 32
+
+    @property
+    def num_nodes(self) -> int:
+        return self.nodes.size // 32
+
+    @property
+    def num_instances(self) -> int:
+        return self.instances.size // 208
+
+    @property
+    def num_materials(self) -> int:
+        return self.materials.size // 16
+
+    def param(self, **kw) -> abi.PathTracerParam:
+        """A copy of the camera parameter block with fields overridden by `kw`."""
+        p = abi.PathTracerParam()
+        C.memmove(C.byref(p), C.byref(self.camera), C.sizeof(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+
+def _from_c(hs: abi.StrelkaHostScene) -> HostScene:
+    lib = abi.load()
+    try:
+        textures = []
+        for i in range(hs.numTextures):
+            w, h = hs.texWidth[i], hs.texHeight[i]
+            buf = (C.c_uint8 * (w * h * 4)).from_address(C.cast(hs.textures[i], C.c_void_p).value)
+            textures.append(np.frombuffer(buf, np.uint8).reshape(h, w, 4).copy())
+        env = marg = cond = None
+        if hs.envRGBA:
+            W, H = hs.envWidth, hs.envHeight
+            env = np.ctypeslib.as_array(hs.envRGBA, shape=(H * W * 4,)).reshape(H, W, 4).copy()
+            marg = np.ctypeslib.as_array(hs.envMarginalCdf, shape=(H + 1,)).copy()
+            cond = np.ctypeslib.as_array(hs.envConditionalCdf, shape=(H * (W + 1),)).copy()
+        cam = abi.PathTracerParam()
+        C.memmove(C.byref(cam), C.byref(hs.camera), C.sizeof(cam))
+        return HostScene(
+            vb=_np(hs.vb, hs.numVertices, abi.Vertex),
+            ib=_np(hs.ib, hs.numIndices, C.c_uint32).view(np.uint32),
+            instances=_np(hs.instances, hs.numInstances, abi.InstanceConstants),
+            lights=_np(hs.lights, max(hs.numLights, 1), abi.UniformLight),
+            num_lights=hs.numLights,
+            materials=_np(hs.materials, hs.numMaterials, abi.MdlMaterial),
+            arg_block=_np(hs.argBlock, hs.argBlockBytes, C.c_uint8),
+            resource_infos=_np(hs.resourceInfos, hs.numResourceInfos, abi.Mdl_resource_info),
+            textures=textures,
+            env=env, env_marginal=marg, env_conditional=cond, env_integral=hs.envIntegral,
+            nodes=_np(hs.nodes, hs.numNodes, abi.BVHNode),
+            num_triangles=hs.numTriangles,
+            camera=cam,
+        )
+    finally:
+        lib.strelka_scene_free(C.byref(hs))
+
+
+def cornell(width: int = 512, height: int = 512, sphere_levels: int = 4, light_side: float = 0.25,
+            light_radiance: float = 15.0, max_depth: int = 4, spp: int = 1) -> HostScene:
+    lib = abi.load()
+    cfg = abi.StrelkaCornellConfig(width, height, sphere_levels, light_side, light_radiance, max_depth, spp, 1, 0)
+    hs = abi.StrelkaHostScene()
+    abi.check(lib.strelka_scene_cornell(C.byref(cfg), C.byref(hs)))
+    return _from_c(hs)
+
+
+def soup(num_tris: int, seed: int = 0) -> HostScene:
+    lib = abi.load()
+    hs = abi.StrelkaHostScene()
+    abi.check(lib.strelka_scene_soup(num_tris, seed, C.byref(hs)))
+    return _from_c(hs)
+
+
+def large(width: int = 1920, height: int = 1080, instances: int = 64, frequency: int = 89, num_textures: int = 8,
+          tex_size: int = 2048, env_width: int = 1024, env_height: int = 512, max_depth: int = 8, spp: int = 16,
+          seed: int = 0) -> HostScene:
+    lib = abi.load()
+    cfg = abi.StrelkaLargeConfig(width, height, instances, frequency, num_textures, tex_size, env_width, env_height,
+                                 max_depth, spp, seed)
+    hs = abi.StrelkaHostScene()
+    abi.check(lib.strelka_scene_large(C.byref(cfg), C.byref(hs)))
+    return _from_c(hs)
+
+
+def rays_soup(n: int, seed: int = 1, shadow: bool = False) -> np.ndarray:
+    """(n, 8) float32 rays: origin xyz, tmax, direction xyz, 0."""
+    lib = abi.load()
+    out = np.zeros((n, 8), np.float32)
+    abi.check(lib.strelka_rays_soup(n, seed, 1 if shadow else 0, out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+def bvh_build(positions: np.ndarray, inst_ids: np.ndarray, prim_ids: np.ndarray) -> np.ndarray:
+    """SAH BVH over world-space triangle corners (positions (3N, 3) float32);
+    returns the flattened nodes as uint8 (numNodes * 32)."""
+    lib = abi.load()
+    n = positions.shape[0]
+    arr = (abi.BVHInputPosition * max(n, 1))()
+    raw = np.frombuffer(arr, dtype=np.uint8).reshape(max(n, 1), 20)
+    if n:
+        raw[:n, 0:12] = np.ascontiguousarray(positions, np.float32).view(np.uint8).reshape(n, 12)
+        raw[:n, 12:16] = np.ascontiguousarray(inst_ids, np.uint32).view(np.uint8).reshape(n, 4)
+        raw[:n, 16:20] = np.ascontiguousarray(prim_ids, np.uint32).view(np.uint8).reshape(n, 4)
+    out = C.POINTER(abi.BVHNode)()
+    cnt = C.c_uint32(0)
+    abi.check(lib.strelka_bvh_build(arr, n, C.byref(out), C.byref(cnt)))
+    if cnt.value == 0:
+        return np.zeros(0, np.uint8)
+    nodes = _np(out, cnt.value, abi.BVHNode)
+    lib.strelka_host_free(C.cast(out, C.c_void_p))
+    return nodes

@@ -1,0 +1,111 @@
+"""Host-injected faults: corrupt BVHs, out-of-range ids, empty scenes and bad
+arguments end in error statuses, never in a hang or a device fault.
+
+The reference's traversal loops have no bound (a cycle in nodeOffset spins
+forever); here every traversal stops after 2*numNodes+2 visits and raises
+STRELKA_DEV_TRAVERSAL_CAP, and every fetch is range-checked first."""
+import numpy as np
+import pytest
+
+from gpu_util import interior_rays
+from strelka_b200 import abi, scenes
+from strelka_b200.render import DeviceScene, PathTracer, to_device
+
+pytestmark = pytest.mark.gpu
+
+
+def trace(torch, pt, ds, rays, flags=abi.TRACE_CLOSEST):
+    n = rays.shape[0]
+    r = to_device(rays)
+    h = torch.zeros(n * 20, dtype=torch.uint8, device="cuda")
+    pt.trace(ds.trace_desc(r, h, flags))
+    status = pt.device_status()
+    return h.cpu().numpy().view(np.uint32).reshape(n, 5), status
+
+
+def corrupt(s, fn):
+    import copy
+    c = copy.copy(s)
+    c.nodes = s.nodes.copy()
+    fn(c.nodes.view(np.int32).reshape(-1, 8))
+    return c
+
+
+@pytest.fixture(scope="module")
+def base(cuda):
+    return scenes.cornell(16, 16, sphere_levels=2)
+
+
+def first_leaf(i):
+    return int(np.nonzero(i[:, 3] != -1)[0][0])
+
+
+def test_cycle_hits_the_visit_cap(cuda, base):
+    def make_cycle(i):
+        i[first_leaf(i), 7] = 0  # leaf escape back to the root
+    s = corrupt(base, make_cycle)
+    pt = PathTracer()
+    ds = DeviceScene(s)
+    rays = interior_rays(2000, 1)
+    _, status = trace(cuda, pt, ds, rays)
+    assert status & abi.DEV_TRAVERSAL_CAP
+    _, status = trace(cuda, pt, ds, rays, abi.TRACE_ANY)
+    assert status & abi.DEV_TRAVERSAL_CAP
+
+
+def test_escape_out_of_range(cuda, base):
+    def bad_escape(i):
+        i[first_leaf(i), 7] = i.shape[0] + 5
+    s = corrupt(base, bad_escape)
+    pt = PathTracer()
+    _, status = trace(cuda, pt, DeviceScene(s), interior_rays(2000, 2))
+    assert status & abi.DEV_NODE_OOB
+
+
+def test_instance_out_of_range(cuda, base):
+    def bad_inst(i):
+        i[first_leaf(i), 3] = 100000
+    s = corrupt(base, bad_inst)
+    pt = PathTracer()
+    hits, status = trace(cuda, pt, DeviceScene(s), interior_rays(2000, 3))
+    assert status & abi.DEV_INSTANCE_OOB
+    assert not (hits[:, 3] == 100000).any()
+
+
+def test_light_capacity(cuda, base):
+    # numLights beyond the light buffer: the pass reports LIGHT_OOB instead of reading past it
+    ds = DeviceScene(base)
+    p = base.param(spp=1, maxDepth=3, numLights=5)
+    total = 16 * 16
+    sb = cuda.zeros(total * 3, dtype=cuda.float32, device="cuda")
+    pt = PathTracer(mode=abi.MODE_MEGAKERNEL)
+    pt.execute(ds.desc(p, sb), total, 1, 0)
+    assert pt.device_status() & abi.DEV_LIGHT_OOB
+
+
+def test_empty_scene(cuda, base):
+    import copy
+    s = copy.copy(base)
+    s.nodes = np.zeros(0, np.uint8)
+    ds = DeviceScene(s)
+    pt = PathTracer()
+    hits, status = trace(cuda, pt, ds, interior_rays(100, 4))
+    assert status == 0 and (hits[:, 3] == 0xFFFFFFFF).all()
+    p = base.param(spp=1, maxDepth=4)
+    sb = cuda.full((16 * 16 * 3,), 5.0, dtype=cuda.float32, device="cuda")
+    pt.execute(ds.desc(p, sb), 16 * 16, 1, 0)
+    assert pt.device_status() == 0
+    assert (sb.cpu().numpy() == 0).all()
+
+
+def test_bad_execute_arguments(cuda, base):
+    ds = DeviceScene(base)
+    p = base.param(spp=2, maxDepth=4)
+    sb = cuda.zeros(16 * 16 * 2 * 3, dtype=cuda.float32, device="cuda")
+    pt = PathTracer()
+    with pytest.raises(abi.StrelkaError) as e:
+        pt.execute(ds.desc(p, sb), 16 * 16, 1, 0)  # w must be W*H*spp
+    assert e.value.code == abi.ERR_INVALID_ARGUMENT
+    d = ds.desc(p, None)
+    with pytest.raises(abi.StrelkaError):
+        pt.execute(d, 16 * 16 * 2, 1, 0)

@@ -1,0 +1,116 @@
+"""The path tracer pass on the GPU against the oracle's restatement of
+computeMain / pathTraceCameraRays (shaders/pathtracerMdl.hlsl:165-423) on
+the same scene, parameters and RNG seeds.
+
+Bar: relMSE <= 1e-4 of the sample buffer (BASELINE image parity), and, since
+both sides evaluate the same operation sequence, nearly every sample is
+bit-identical (a rare closest-hit tie may send one path elsewhere)."""
+import numpy as np
+import pytest
+
+import oracle
+from gpu_util import bits_equal_fraction, relmse
+from strelka_b200 import abi, scenes
+from strelka_b200.render import DeviceScene, PathTracer
+
+pytestmark = pytest.mark.gpu
+
+RELMSE_BAR = 1e-4
+EXACT_BAR = 0.999
+
+
+@pytest.fixture(scope="module")
+def cornell(cuda):
+    s = scenes.cornell(40, 32, sphere_levels=4)
+    return s, oracle.SceneView(s), DeviceScene(s)
+
+
+def render(torch, s, ds, param, mode, chunk=0):
+    total = param.dimension[0] * param.dimension[1] * param.spp
+    sb = torch.full((total * 3,), -7.0, dtype=torch.float32, device="cuda")
+    pt = PathTracer(mode=mode, chunk_paths=chunk)
+    pt.execute(ds.desc(param, sb), total, 1, 0)
+    status = pt.device_status()
+    torch.cuda.synchronize()
+    return sb.cpu().numpy(), status
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_MEGAKERNEL, abi.MODE_WAVEFRONT])
+@pytest.mark.parametrize("sst", [0, 1, 2, 3])
+def test_cornell_sampling_types(cuda, cornell, mode, sst):
+    s, view, ds = cornell
+    p = s.param(spp=2, maxDepth=4, frameNumber=5, stratifiedSamplingType=sst)
+    g, status = render(cuda, s, ds, p, mode, chunk=777)
+    r = oracle.pathtrace(view, p)
+    assert status == 0
+    assert np.isfinite(g).all()
+    assert relmse(g, r) <= RELMSE_BAR
+    assert bits_equal_fraction(g, r) >= EXACT_BAR
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_MEGAKERNEL, abi.MODE_WAVEFRONT])
+def test_cornell_deep_russian_roulette(cuda, cornell, mode):
+    # depth 8 exercises Russian roulette (depth > 3, pathtracerMdl.hlsl:374-382)
+    s, view, ds = cornell
+    p = s.param(spp=4, maxDepth=8, frameNumber=11, stratifiedSamplingType=1)
+    g, status = render(cuda, s, ds, p, mode)
+    r = oracle.pathtrace(view, p)
+    assert status == 0
+    assert relmse(g, r) <= RELMSE_BAR
+    assert bits_equal_fraction(g, r) >= EXACT_BAR
+
+
+def test_megakernel_equals_wavefront(cuda, cornell):
+    s, view, ds = cornell
+    p = s.param(spp=3, maxDepth=6, frameNumber=2, stratifiedSamplingType=1)
+    a, _ = render(cuda, s, ds, p, abi.MODE_MEGAKERNEL)
+    b, _ = render(cuda, s, ds, p, abi.MODE_WAVEFRONT, chunk=1000)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_debug_normals(cuda, cornell):
+    # ubo.debug == 1 returns (N + 1) / 2 of the first surface hit
+    s, view, ds = cornell
+    p = s.param(spp=1, maxDepth=4, debug=1)
+    g, _ = render(cuda, s, ds, p, abi.MODE_WAVEFRONT)
+    r = oracle.pathtrace(view, p)
+    assert bits_equal_fraction(g, r) >= EXACT_BAR
+
+
+def test_no_lights_terminates(cuda, cornell):
+    # numLights == 0 (no environment): the reference breaks after the first
+    # hit's emission (lightPdf = 0 * (1/0) = NaN)
+    s, view, ds = cornell
+    p = s.param(spp=1, maxDepth=4, numLights=0)
+    g, _ = render(cuda, s, ds, p, abi.MODE_MEGAKERNEL)
+    r = oracle.pathtrace(view, p)
+    assert np.array_equal(g.view(np.uint32), r.view(np.uint32))
+
+
+def test_large_scene_small(cuda):
+    # the large-render generator at toy size: instanced GGX / dielectric /
+    # textured Lambert spheres under an environment light
+    s = scenes.large(width=48, height=32, instances=6, frequency=6, num_textures=2, tex_size=64, env_width=64,
+                     env_height=32, max_depth=6, spp=2, seed=3)
+    view = oracle.SceneView(s)
+    ds = DeviceScene(s)
+    p = s.param(frameNumber=1)
+    for mode in (abi.MODE_MEGAKERNEL, abi.MODE_WAVEFRONT):
+        g, status = render(cuda, s, ds, p, mode)
+        r = oracle.pathtrace(view, p)
+        assert status == 0
+        assert relmse(g, r) <= RELMSE_BAR
+        assert bits_equal_fraction(g, r) >= 0.995
+
+
+def test_golden_fixture(cuda):
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "cornell_64x64.npz")
+    gold = np.load(path)
+    s = scenes.cornell(64, 64, sphere_levels=4)
+    ds = DeviceScene(s)
+    p = s.param(spp=int(gold["spp"]), maxDepth=int(gold["max_depth"]), frameNumber=int(gold["frame"]),
+                stratifiedSamplingType=int(gold["sst"]))
+    g, _ = render(cuda, s, ds, p, abi.MODE_WAVEFRONT)
+    assert relmse(g, gold["samples"]) <= RELMSE_BAR
+    assert bits_equal_fraction(g, gold["samples"]) >= EXACT_BAR

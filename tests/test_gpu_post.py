@@ -1,0 +1,98 @@
+"""Reduction, accumulation and tonemap passes on the GPU against the oracle,
+bit for bit; the fused resolve equals the three passes in sequence."""
+import numpy as np
+import pytest
+
+import oracle
+from strelka_b200 import abi
+from strelka_b200.render import (Accumulation, ReductionPass, Tonemap, accumulation_param, ptr, resolve,
+                                 tonemap_param, to_device)
+
+pytestmark = pytest.mark.gpu
+
+W, H, SPP = 37, 23, 5
+
+
+def dev(torch, a):
+    return to_device(np.ascontiguousarray(a, np.float32)).view(torch.float32)
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def data(cuda):
+    rng = np.random.default_rng(0)
+    sb = (rng.gamma(0.5, 1.0, W * H * SPP * 3)).astype(np.float32)
+    sb[::97] = 0.0
+    hist = np.concatenate([rng.uniform(0, 3, (W * H, 3)), np.ones((W * H, 1))], 1).astype(np.float32).ravel()
+    p = abi.PathTracerParam()
+    p.dimension[0], p.dimension[1], p.spp = W, H, SPP
+    return sb, hist, p
+
+
+def test_reduction(cuda, data):
+    sb, _, p = data
+    out = cuda.zeros(W * H * 4, dtype=cuda.float32, device="cuda")
+    d = abi.ReductionDesc(p, ptr(dev(cuda, sb)), ptr(out))
+    sbd = dev(cuda, sb)
+    d.sampleBuffer = ptr(sbd)
+    ReductionPass().execute(d, W * H, 1, 0)
+    assert np.array_equal(host(out).view(np.uint32), oracle.reduce(p, sb).view(np.uint32))
+
+
+@pytest.mark.parametrize("iteration", [0, 1, 7, 1000])
+def test_accumulation(cuda, data, iteration):
+    sb, hist, p = data
+    cur = oracle.reduce(p, sb)
+    ap = accumulation_param(W, H, iteration)
+    out = cuda.zeros(W * H * 4, dtype=cuda.float32, device="cuda")
+    a, b = dev(cuda, cur), dev(cuda, hist)
+    Accumulation().execute(abi.AccumulationDesc(ap, ptr(a), ptr(b), ptr(out)), W, H, 0)
+    assert np.array_equal(host(out).view(np.uint32), oracle.accumulate(ap, cur, hist).view(np.uint32))
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_tonemap(cuda, data, kind):
+    sb, _, p = data
+    img = oracle.reduce(p, sb)
+    tp = tonemap_param(W, H, kind)
+    out = cuda.zeros(W * H * 4, dtype=cuda.float32, device="cuda")
+    a = dev(cuda, img)
+    Tonemap().execute(abi.TonemapDesc(tp, ptr(a), ptr(out)), W, H, 0)
+    ref = oracle.tonemap(tp, img)
+    g = host(out)
+    both_nan = np.isnan(g) & np.isnan(ref)
+    assert np.array_equal(g.view(np.uint32)[~both_nan], ref.view(np.uint32)[~both_nan])
+    assert np.array_equal(np.isnan(g), np.isnan(ref))
+
+
+@pytest.mark.parametrize("accumulate", [False, True])
+def test_resolve_equals_sequence(cuda, data, accumulate):
+    sb, hist, p = data
+    tp = tonemap_param(W, H, 1)
+    ap = accumulation_param(W, H, 3)
+    cur = oracle.reduce(p, sb)
+    acc = oracle.accumulate(ap, cur, hist) if accumulate else cur
+    tm = oracle.tonemap(tp, acc)
+    sbd, hd = dev(cuda, sb), dev(cuda, hist)
+    acc_out = cuda.zeros(W * H * 4, dtype=cuda.float32, device="cuda")
+    tm_out = cuda.zeros(W * H * 4, dtype=cuda.float32, device="cuda")
+    rgba8 = cuda.zeros(W * H * 4, dtype=cuda.uint8, device="cuda")
+    resolve(p, sbd, tp, ap if accumulate else None, hd if accumulate else None, acc_out, tm_out, rgba8)
+    assert np.array_equal(host(acc_out).view(np.uint32), acc.view(np.uint32))
+    assert np.array_equal(host(tm_out).view(np.uint32), tm.view(np.uint32))
+    q = (np.clip(tm, 0, 1) * np.float32(255) + np.float32(0.5)).astype(np.int32).astype(np.uint8)
+    q[3::4] = 255
+    assert np.array_equal(host(rgba8), q)
+
+
+def test_bad_arguments(cuda, data):
+    sb, _, p = data
+    out = cuda.zeros(W * H * 4, dtype=cuda.float32, device="cuda")
+    sbd = dev(cuda, sb)
+    d = abi.ReductionDesc(p, ptr(sbd), ptr(out))
+    with pytest.raises(abi.StrelkaError) as e:
+        ReductionPass().execute(d, W * H + 1, 1, 0)
+    assert e.value.code == abi.ERR_INVALID_ARGUMENT

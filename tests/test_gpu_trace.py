@@ -1,0 +1,107 @@
+"""Ray queries on the GPU against the oracle's restatement of closestHit /
+anyHit (shaders/raytracing.h:198-286): closest-hit primitive ids match bit
+for bit except on ties within 1e-6 relative; any-hit records match exactly
+(same depth-first order); visit counters match the oracle replaying the
+GPU's traversal rule."""
+import numpy as np
+import pytest
+
+import oracle
+from gpu_util import compare_closest, interior_rays
+from strelka_b200 import abi, scenes
+from strelka_b200.render import DeviceScene, PathTracer, to_device
+
+pytestmark = pytest.mark.gpu
+
+
+def run_trace(torch, pt, ds, rays, flags):
+    n = rays.shape[0]
+    rays_d = to_device(rays)
+    hits_d = torch.zeros(n * 20, dtype=torch.uint8, device="cuda")
+    cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+    pt.trace(ds.trace_desc(rays_d, hits_d, flags, cnt))
+    torch.cuda.synchronize()
+    return hits_d.cpu().numpy().view(np.uint32).reshape(n, 5), cnt.cpu().numpy().astype(np.uint64)
+
+
+@pytest.fixture(scope="module")
+def soup_setup(cuda):
+    s = scenes.soup(200_000, 0)
+    return s, oracle.SceneView(s), DeviceScene(s), PathTracer()
+
+
+@pytest.fixture(scope="module")
+def cornell_setup(cuda):
+    s = scenes.cornell(16, 16, sphere_levels=4)
+    return s, oracle.SceneView(s), DeviceScene(s), PathTracer()
+
+
+def test_closest_soup(cuda, soup_setup):
+    s, view, ds, pt = soup_setup
+    rays = scenes.rays_soup(100_000, 1)
+    g, _ = run_trace(cuda, pt, ds, rays, abi.TRACE_CLOSEST)
+    o, found, _ = oracle.trace(view, rays)
+    assert found.sum() > 1000
+    compare_closest(g, o)
+    assert pt.device_status() == 0
+
+
+def test_closest_interior_cornell(cuda, cornell_setup):
+    s, view, ds, pt = cornell_setup
+    rays = interior_rays(100_000, 3)
+    g, _ = run_trace(cuda, pt, ds, rays, abi.TRACE_CLOSEST)
+    o, found, _ = oracle.trace(view, rays)
+    assert found.mean() > 0.99
+    ties = compare_closest(g, o)
+    assert ties < 50
+    # exact t and barycentrics wherever the primitive agrees
+    same = (g[:, 3:] == o[:, 3:]).all(1) & found
+    assert (g[same, :3] == o[same, :3]).all()
+
+
+@pytest.mark.parametrize("shadow", [False, True])
+def test_any_hit_exact(cuda, soup_setup, shadow):
+    s, view, ds, pt = soup_setup
+    rays = scenes.rays_soup(100_000, 2, shadow=shadow)
+    g, _ = run_trace(cuda, pt, ds, rays, abi.TRACE_ANY)
+    o, found, _ = oracle.trace(view, rays, any_hit=True)
+    assert found.sum() > 100
+    assert np.array_equal(g, o)
+
+
+def test_visit_counters(cuda, soup_setup):
+    s, view, ds, pt = soup_setup
+    rays = scenes.rays_soup(50_000, 4)
+    _, cg = run_trace(cuda, pt, ds, rays, abi.TRACE_CLOSEST | abi.TRACE_COUNT)
+    _, _, co = oracle.trace(view, rays, prune=True)
+    assert np.array_equal(cg, co)
+    rays = scenes.rays_soup(50_000, 5, shadow=True)
+    _, cg = run_trace(cuda, pt, ds, rays, abi.TRACE_ANY | abi.TRACE_COUNT)
+    _, _, co = oracle.trace(view, rays, any_hit=True)
+    assert np.array_equal(cg, co)
+
+
+def test_refine_within_2ulp_of_fp64(cuda, cornell_setup):
+    s, view, ds, pt = cornell_setup
+    rays = interior_rays(20_000, 7)
+    g, _ = run_trace(cuda, pt, ds, rays, abi.TRACE_CLOSEST | abi.TRACE_REFINE)
+    found = g[:, 3] != 0xFFFFFFFF
+    t64, u64, v64 = oracle.intersect_fp64(view, rays[found], g[found, 3], g[found, 4])
+    for col, ref in ((2, t64), (0, u64), (1, v64)):
+        got = g[found, col].view(np.float32).astype(np.float64)
+        ulp = np.spacing(np.abs(ref).astype(np.float32)).astype(np.float64)
+        err = np.abs(got - ref) / ulp
+        assert np.percentile(err, 100) <= 2.0, (col, err.max())
+
+
+def test_host_buffers_entry(cuda, cornell_setup):
+    import ctypes as C
+    s, view, ds, pt = cornell_setup
+    rays = interior_rays(1000, 11)
+    stage_r = cuda.zeros(1000 * 32, dtype=cuda.uint8, device="cuda")
+    stage_h = cuda.zeros(1000 * 20, dtype=cuda.uint8, device="cuda")
+    hits = np.zeros((1000, 5), np.uint32)
+    desc = ds.trace_desc(stage_r, stage_h, abi.TRACE_CLOSEST)
+    abi.check(abi.load().strelka_trace_host(pt.handle, C.byref(desc), rays.ctypes.data, hits.ctypes.data, None))
+    o, _, _ = oracle.trace(view, rays)
+    compare_closest(hits, o)
