@@ -157,6 +157,7 @@ __global__ void __launch_bounds__(kExtendBlock) k_extend(DevScene s, Wave w, int
     const uint32_t count = w.counters[qin];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         w.counters[qin ^ 1] = 0;  // consumed by shade(k-1); refilled by shade(k)
+        w.counters[2] = 0;        // consumed by shadow(k-1); refilled by shade(k)
     }
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
     uint32_t nI = 0, nL = 0;
@@ -292,8 +293,6 @@ __global__ void __launch_bounds__(kExtendBlock) k_shadow(DevScene s, Wave w, uns
         atomicAdd(&visitCounters[5], (unsigned long long)nR);
     }
 }
-
-__global__ void __launch_bounds__(kSmallBlock) k_reset_shadow(Wave w) { w.counters[2] = 0; }
 
 __global__ void __launch_bounds__(kSmallBlock) k_finalize(Wave w, float* __restrict__ sampleBuffer, uint64_t first, uint32_t n)
 {
@@ -656,7 +655,6 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
                 Timer t(pt, KC_SHADOW, st);
                 if (count) k_shadow<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, pt->visitCounters);
                 else k_shadow<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, nullptr);
-                k_reset_shadow<<<1, 1, 0, st>>>(pt->wave);
             }
         }
         {

@@ -51,7 +51,7 @@ def test_closest_interior_cornell(cuda, cornell_setup):
     rays = interior_rays(100_000, 3)
     g, _ = run_trace(cuda, pt, ds, rays, abi.TRACE_CLOSEST)
     o, found, _ = oracle.trace(view, rays)
-    assert found.mean() > 0.99
+    assert found.mean() > 0.8  # the box's front face is open
     ties = compare_closest(g, o)
     assert ties < 50
     # exact t and barycentrics wherever the primitive agrees
