@@ -625,7 +625,9 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
     }
 
     // wavefront
-    size_t chunk = pt->cfg.chunkPaths ? pt->cfg.chunkPaths : (size_t)1 << 22;
+    // default: the whole frame in flight (160 bytes of state per path; a
+    // 1080p x 16 spp frame is 33.2M paths, 5.3 GB)
+    size_t chunk = pt->cfg.chunkPaths ? pt->cfg.chunkPaths : (size_t)1 << 25;
     chunk = std::min<size_t>(chunk, total);
     rc = ensure_wave(pt, chunk);
     if (rc) return rc;
