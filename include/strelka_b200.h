@@ -387,6 +387,21 @@ int strelka_trace_execute(StrelkaPathTracer* pt, const TraceDesc* desc, void* st
 int strelka_trace_host(StrelkaPathTracer* pt, const TraceDesc* desc, const Ray* hostRays,
                        Hit* hostHits, void* stream);
 
+/* Allocation-free variant of strelka_trace_execute; this entry point has no
+ * counterpart in the reference.  For callers that cannot have the library
+ * allocate device memory (an engine whose allocator owns the whole heap, a
+ * real-time loop that cannot afford cudaMalloc's implicit synchronisation):
+ * it needs no pass object and keeps its scratch (the derived leaf-triangle
+ * table) in a fixed 12 MiB __device__ array that every GPU loading the
+ * library holds until exit.  Scenes above 262,144 BVH nodes (131,072
+ * triangles) are rejected with STRELKA_ERR_INVALID_ARGUMENT; flags other
+ * than STRELKA_TRACE_ANY are rejected with STRELKA_ERR_UNSUPPORTED.  The
+ * first call on a device looks up the scratch address for that device, so
+ * make it before starting any stream capture.  All calls share the scratch:
+ * calls that overlap on the GPU race.  deviceStatus (a device word, may be
+ * NULL) receives this call's STRELKA_DEV_* bits. */
+int strelka_trace_execute_noalloc(const TraceDesc* desc, uint32_t* deviceStatus, void* stream);
+
 /* ------------------------------------------------------------------------- */
 /* Host-side scene preparation (replaces BvhBuilder, include/render/bvh.h:38-46). */
 

@@ -243,6 +243,7 @@ SIGNATURES = {
                                           vp, C.POINTER(Tonemapparam), vp, vp, vp]),
     "strelka_trace_execute": (C.c_int, [vp, C.POINTER(TraceDesc), vp]),
     "strelka_trace_host": (C.c_int, [vp, C.POINTER(TraceDesc), vp, vp, vp]),
+    "strelka_trace_execute_noalloc": (C.c_int, [C.POINTER(TraceDesc), vp, vp]),
     "strelka_bvh_build": (C.c_int, [C.POINTER(BVHInputPosition), C.c_uint32, C.POINTER(C.POINTER(BVHNode)),
                                     C.POINTER(C.c_uint32)]),
     "strelka_host_free": (None, [vp]),
