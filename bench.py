@@ -271,9 +271,9 @@ def main():
         pt_count.execute(ds.desc(hs.param(frameNumber=rank * 100000 + args.warmup + k), sb), total, 1, 0, stream)
     cnt = pt_count.counters(stream)
     pt_count.close()
-    # algorithmic bytes of the closest-hit traversal: 32 B per inner node,
-    # 32 + 48 B per leaf (node + triangle), 32 B ray in, 20 B hit out
-    bytes_alg = 32 * cnt["extend_inner"] + 80 * cnt["extend_leaf"] + 52 * cnt["extend_rays"]
+    # algorithmic bytes of the closest-hit traversal: 64 B per node-pair
+    # record processed, 48 B per triangle test, 32 B ray in, 20 B hit out
+    bytes_alg = 64 * cnt["extend_inner"] + 48 * cnt["extend_leaf"] + 52 * cnt["extend_rays"]
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         peak = json.load(open(peaks_path))["hbm_gbs"]

@@ -132,7 +132,7 @@ def trace(view: SceneView, rays: np.ndarray, any_hit: bool = False, prune: bool 
     found = np.zeros(n, np.uint8)
     counters = np.zeros(2, np.uint64)
     lib.oracle_trace(C.byref(view.scene), _ptr(rays), n, _ptr(hits), _ptr(found), 1 if any_hit else 0,
-                     1 if prune else 0, _ptr(counters), threads)
+                     int(prune), _ptr(counters), threads)
     return hits, found.astype(bool), counters
 
 

@@ -471,6 +471,254 @@ static int any_hit(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, unsig
     return 0;
 }
 
+/* ------------------------------------------------------------------------- */
+/* The GPU's node-pair traversal, replayed for visit counts and for its exact
+ * closest-hit tie order (not a reference algorithm).  For an inner node n the
+ * children are L = n+1 and R = escape(L) (the implicit tree of the depth-first
+ * layout); one "record" step tests both: a leaf child by Moller-Trumbore, an
+ * inner child by its box.  Closest hit descends into the nearer child first
+ * with a 32-entry stack and the 2^-12 pruning rule; any hit keeps the
+ * depth-first order.  A full stack falls back to the stackless loops. */
+#define PAIR_STACK 32
+static int node_is_leaf(const OracleScene* s, uint32_t c) { return (uint32_t)s->nodes[c].instId != INVALID_INDEX; }
+
+static void pair_children(const OracleScene* s, uint32_t n, uint32_t* L, uint32_t* R)
+{
+    *L = n + 1 < s->numNodes ? n + 1 : INVALID_INDEX;
+    *R = INVALID_INDEX;
+    if (*L != INVALID_INDEX) {
+        uint32_t r = (uint32_t)s->nodes[*L].nodeOffset;
+        *R = r < s->numNodes ? r : INVALID_INDEX;
+    }
+}
+
+static int leaf_test(const OracleScene* s, uint32_t leaf, v3 o, v3 d, float* t, float* bu, float* bv, uint32_t* inst,
+                     uint32_t* prim)
+{
+    const BVHNode* n = &s->nodes[leaf];
+    *inst = (uint32_t)n->instId;
+    *prim = asuint_f(n->minBounds[0]);
+    Tri tri = get_triangle(s, *inst, *prim);
+    *t = 1e9f;
+    if (!tri.ok) {
+        *t = NAN;
+        return 0;
+    }
+    return ray_triangle(o, d, tri.v0, tri.e0, tri.e1, t, bu, bv);
+}
+
+static void stackless_closest_from(const OracleScene* s, v3 o, float tmax, v3 d, const float inv[3], uint32_t node, float* minHit,
+                                   Hit* hit, int* found, unsigned long long* nI, unsigned long long* nL)
+{
+    float oo[3] = {o.x, o.y, o.z};
+    uint64_t cap = 2ull * s->numNodes + 2, visits = 0;
+    while (node != INVALID_INDEX) {
+        if (node >= s->numNodes || ++visits > cap) break;
+        const BVHNode* n = &s->nodes[node];
+        if ((uint32_t)n->instId != INVALID_INDEX) {
+            (*nL)++;
+            float t, bu = 0, bv = 0;
+            uint32_t iid, pid;
+            if (leaf_test(s, node, o, d, &t, &bu, &bv, &iid, &pid) && t < tmax && t < *minHit) {
+                *minHit = t;
+                hit->t = t; hit->bary[0] = bu; hit->bary[1] = bv; hit->instId = iid; hit->primId = pid;
+                *found = 1;
+            }
+            node = (uint32_t)n->nodeOffset;
+            continue;
+        }
+        (*nI)++;
+        float boxT;
+        if (oracle_intersect_ray_box(oo, inv, n->minBounds, n->maxBounds, &boxT) && !(boxT > tmax) &&
+            !(boxT > *minHit * PRUNE_SCALE)) {
+            ++node;
+            continue;
+        }
+        node = (uint32_t)n->nodeOffset;
+    }
+}
+
+static int pair_closest(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, unsigned long long* nI, unsigned long long* nL)
+{
+    float inv[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    float oo[3] = {o.x, o.y, o.z};
+    float minHit = 1e9f;
+    int found = 0;
+    if (s->numNodes == 0) return 0;
+    uint32_t stackN[PAIR_STACK];
+    float stackT[PAIR_STACK];
+    int sp = 0;
+    uint32_t cur = 0, steps = 0;
+    for (;;) {
+        if (cur != INVALID_INDEX) {
+            if (cur >= s->numNodes || ++steps > s->numNodes + 1u) break;
+            if (cur == 0 && node_is_leaf(s, 0)) {
+                (*nL)++;
+                float t, bu = 0, bv = 0;
+                uint32_t iid, pid;
+                if (leaf_test(s, 0, o, d, &t, &bu, &bv, &iid, &pid) && t < tmax && t < minHit) {
+                    minHit = t;
+                    hit->t = t; hit->bary[0] = bu; hit->bary[1] = bv; hit->instId = iid; hit->primId = pid;
+                    found = 1;
+                }
+                cur = INVALID_INDEX;
+            } else {
+                (*nI)++;
+                uint32_t L, R;
+                pair_children(s, cur, &L, &R);
+                int goL = 0, goR = 0;
+                float tL = 0.0f, tR = 0.0f;
+                for (int k = 0; k < 2; ++k) {
+                    uint32_t c = k == 0 ? L : R;
+                    if (c == INVALID_INDEX) continue;
+                    if (node_is_leaf(s, c)) {
+                        (*nL)++;
+                        float t, bu = 0, bv = 0;
+                        uint32_t iid, pid;
+                        if (leaf_test(s, c, o, d, &t, &bu, &bv, &iid, &pid) && t < tmax && t < minHit) {
+                            minHit = t;
+                            hit->t = t; hit->bary[0] = bu; hit->bary[1] = bv; hit->instId = iid; hit->primId = pid;
+                            found = 1;
+                        }
+                    } else {
+                        float bt;
+                        int h = oracle_intersect_ray_box(oo, inv, s->nodes[c].minBounds, s->nodes[c].maxBounds, &bt);
+                        if (k == 0) { goL = h; tL = bt; } else { goR = h; tR = bt; }
+                    }
+                }
+                float lim = minHit * PRUNE_SCALE;
+                goL = goL && !(tL > tmax) && !(tL > lim);
+                goR = goR && !(tR > tmax) && !(tR > lim);
+                if (goL && goR) {
+                    int leftNear = tL <= tR;
+                    uint32_t nearC = leftNear ? L : R, farC = leftNear ? R : L;
+                    float farT = leftNear ? tR : tL;
+                    if (sp < PAIR_STACK) {
+                        stackN[sp] = farC;
+                        stackT[sp] = farT;
+                        ++sp;
+                        cur = nearC;
+                    } else {
+                        stackless_closest_from(s, o, tmax, d, inv, 0, &minHit, hit, &found, nI, nL);
+                        return found;
+                    }
+                } else if (goL) {
+                    cur = L;
+                } else if (goR) {
+                    cur = R;
+                } else {
+                    cur = INVALID_INDEX;
+                }
+            }
+        }
+        if (cur == INVALID_INDEX) {
+            float lim = minHit * PRUNE_SCALE;
+            while (sp > 0) {
+                --sp;
+                if (!(stackT[sp] > lim)) {
+                    cur = stackN[sp];
+                    break;
+                }
+            }
+            if (cur == INVALID_INDEX) break;
+        }
+    }
+    return found;
+}
+
+static int pair_any(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, unsigned long long* nI, unsigned long long* nL)
+{
+    float inv[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    float oo[3] = {o.x, o.y, o.z};
+    if (s->numNodes == 0) return 0;
+    uint32_t stackN[PAIR_STACK];
+    int sp = 0;
+    uint32_t cur = 0, steps = 0;
+    for (;;) {
+        if (cur != INVALID_INDEX) {
+            if (cur >= s->numNodes || ++steps > s->numNodes + 1u) return 0;
+            if (cur == 0 && node_is_leaf(s, 0)) {
+                (*nL)++;
+                float t, bu, bv;
+                uint32_t iid, pid;
+                int is = leaf_test(s, 0, o, d, &t, &bu, &bv, &iid, &pid);
+                hit->t = t;
+                if (is && t < tmax) {
+                    hit->instId = iid;
+                    hit->primId = pid;
+                    return 1;
+                }
+                cur = INVALID_INDEX;
+            } else {
+                (*nI)++;
+                uint32_t L, R;
+                pair_children(s, cur, &L, &R);
+                int goL = 0;
+                if (L != INVALID_INDEX) {
+                    if (node_is_leaf(s, L)) {
+                        (*nL)++;
+                        float t, bu, bv;
+                        uint32_t iid, pid;
+                        int is = leaf_test(s, L, o, d, &t, &bu, &bv, &iid, &pid);
+                        hit->t = t;
+                        if (is && t < tmax) {
+                            hit->instId = iid;
+                            hit->primId = pid;
+                            return 1;
+                        }
+                    } else {
+                        float bt;
+                        goL = oracle_intersect_ray_box(oo, inv, s->nodes[L].minBounds, s->nodes[L].maxBounds, &bt) &&
+                              !(bt > tmax);
+                    }
+                }
+                int rPending = 0;
+                if (R != INVALID_INDEX) {
+                    if (node_is_leaf(s, R)) {
+                        rPending = 1;
+                    } else {
+                        float bt;
+                        rPending = oracle_intersect_ray_box(oo, inv, s->nodes[R].minBounds, s->nodes[R].maxBounds, &bt) &&
+                                   !(bt > tmax);
+                    }
+                }
+                if (goL) {
+                    if (rPending) {
+                        if (sp < PAIR_STACK) {
+                            stackN[sp++] = R;
+                        } else {
+                            return any_hit(s, o, tmax, d, hit, nI, nL); /* unreachable with trees of depth <= 32 */
+                        }
+                    }
+                    cur = L;
+                } else if (rPending) {
+                    cur = R;
+                } else {
+                    cur = INVALID_INDEX;
+                }
+            }
+        }
+        for (;;) {
+            if (cur == INVALID_INDEX) {
+                if (sp == 0) return 0;
+                cur = stackN[--sp];
+            }
+            if (!node_is_leaf(s, cur)) break;
+            (*nL)++;
+            float t, bu, bv;
+            uint32_t iid, pid;
+            int is = leaf_test(s, cur, o, d, &t, &bu, &bv, &iid, &pid);
+            hit->t = t;
+            if (is && t < tmax) {
+                hit->instId = iid;
+                hit->primId = pid;
+                return 1;
+            }
+            cur = INVALID_INDEX;
+        }
+    }
+}
+
 int oracle_trace(const OracleScene* s, const Ray* rays, uint32_t n, Hit* hits, uint8_t* found, int mode,
                  int prune, unsigned long long* counters, int nthreads)
 {
@@ -487,7 +735,9 @@ int oracle_trace(const OracleScene* s, const Ray* rays, uint32_t n, Hit* hits, u
         h.instId = INVALID_INDEX;
         h.primId = INVALID_INDEX;
         unsigned long long ni = 0, nl = 0;
-        int f = mode == 1 ? any_hit(s, o, r->o.w, d, &h, &ni, &nl) : closest_hit(s, o, r->o.w, d, &h, prune, &ni, &nl);
+        int f;
+        if (prune == 2) f = mode == 1 ? pair_any(s, o, r->o.w, d, &h, &ni, &nl) : pair_closest(s, o, r->o.w, d, &h, &ni, &nl);
+        else f = mode == 1 ? any_hit(s, o, r->o.w, d, &h, &ni, &nl) : closest_hit(s, o, r->o.w, d, &h, prune, &ni, &nl);
         if (!f) {
             h.instId = INVALID_INDEX;
             h.primId = INVALID_INDEX;

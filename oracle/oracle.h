@@ -83,8 +83,11 @@ int oracle_ray_triangle(const float o[3], const float d[3], const float v0[3], c
                         const float e1[3], float* t, float* u, float* v);
 
 /* raytracing.h:198-286 over n rays.  mode 0 closest, 1 any.  found[i] = 0/1.
- * prune != 0 replays the GPU's closest-hit pruning rule (for visit counts).
- * counters (may be NULL) gets {inner visits, leaf visits} summed. */
+ * prune = 0: the reference's stackless depth-first loop; 1: the same with
+ * the GPU's closest-hit pruning rule; 2: the GPU's node-pair traversal (its
+ * visit counts and its closest-hit tie order).  counters (may be NULL) gets
+ * {inner visits, leaf visits} summed (for prune = 2: inner records
+ * processed, triangle tests). */
 int oracle_trace(const OracleScene* s, const Ray* rays, uint32_t n, Hit* hits, uint8_t* found,
                  int mode, int prune, unsigned long long* counters, int nthreads);
 

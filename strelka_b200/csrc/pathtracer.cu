@@ -31,30 +31,59 @@ enum KernelClass { KC_GENERATE = 0, KC_EXTEND, KC_SHADE, KC_SHADOW, KC_FINALIZE,
 const char* kKernelNames[KC_COUNT] = {"generate", "extend", "shade", "shadow", "finalize", "megakernel", "prep"};
 
 // ---------------------------------------------------------------------------
-// Scene preparation: leaf triangle table, raytracing.h:134-153 per leaf node.
-__global__ void k_prep_tris(const float4* __restrict__ nodes, uint32_t numNodes, const InstanceConstants* __restrict__ inst,
-                            uint32_t numInstances, const uint32_t* __restrict__ ib, uint32_t numIndices,
-                            const Vertex* __restrict__ vb, uint32_t numVertices, float4* __restrict__ tris,
-                            uint32_t* status)
+// Scene preparation: the record table of traverse.cuh, per node slot.
+// Leaf: the triangle exactly as getTriangle computes it (raytracing.h:134-153).
+// Inner: both children of the implicit tree (L = n+1, R = escape(n+1)) with
+// the boxes of inner children copied from their nodes.
+__global__ void k_prep_rec(const float4* __restrict__ nodes, uint32_t numNodes, const InstanceConstants* __restrict__ inst,
+                           uint32_t numInstances, const uint32_t* __restrict__ ib, uint32_t numIndices,
+                           const Vertex* __restrict__ vb, uint32_t numVertices, float4* __restrict__ rec, uint32_t* status)
 {
+    const float qnan = __int_as_float(0x7fc00000);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x) {
         const float4 lo = nodes[2 * (size_t)i];
         const float4 hi = nodes[2 * (size_t)i + 1];
         const uint32_t instId = __float_as_uint(lo.w);
-        float4* out = &tris[3 * (size_t)i];
+        float4* out = &rec[4 * (size_t)i];
+        const uint32_t esc = __float_as_uint(hi.w);
+        if (esc != SB_INVALID && esc >= numNodes) atomicOr(status, STRELKA_DEV_NODE_OOB);
         if (instId == SB_INVALID) {
-            // inner node: the slot is never read; record the bounds sanity only
-            uint32_t esc = __float_as_uint(hi.w);
-            if (esc != SB_INVALID && esc >= numNodes) atomicOr(status, STRELKA_DEV_NODE_OOB);
+            uint32_t ref[2] = {SB_INVALID, SB_INVALID};
+            float4 box[4] = {make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0),
+                             make_float4(0, 0, 0, 0)};
+            const uint32_t L = i + 1;
+            uint32_t R = SB_INVALID;
+            if (L < numNodes) R = __float_as_uint(nodes[2 * (size_t)L + 1].w);
+            else atomicOr(status, STRELKA_DEV_NODE_OOB);
+            if (R != SB_INVALID && R >= numNodes) {
+                atomicOr(status, STRELKA_DEV_NODE_OOB);
+                R = SB_INVALID;
+            }
+            const uint32_t child[2] = {L < numNodes ? L : SB_INVALID, R};
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const uint32_t c = child[k];
+                if (c == SB_INVALID) continue;
+                const float4 clo = nodes[2 * (size_t)c];
+                const float4 chi = nodes[2 * (size_t)c + 1];
+                if (__float_as_uint(clo.w) != SB_INVALID) {
+                    ref[k] = c | SB_LEAF_BIT;
+                } else {
+                    ref[k] = c;
+                    box[2 * k] = make_float4(clo.x, clo.y, clo.z, 0.0f);
+                    box[2 * k + 1] = make_float4(chi.x, chi.y, chi.z, 0.0f);
+                }
+            }
+            out[0] = make_float4(box[0].x, box[0].y, box[0].z, __uint_as_float(ref[0]));
+            out[1] = make_float4(box[1].x, box[1].y, box[1].z, __uint_as_float(ref[1]));
+            out[2] = box[2];
+            out[3] = box[3];
             continue;
         }
-        const float qnan = __int_as_float(0x7fc00000);
-        float4 bad = make_float4(qnan, qnan, qnan, 0.0f);
-        uint32_t esc = __float_as_uint(hi.w);
-        if (esc != SB_INVALID && esc >= numNodes) atomicOr(status, STRELKA_DEV_NODE_OOB);
+        const float4 bad = make_float4(qnan, qnan, qnan, 0.0f);
         if (instId >= numInstances) {
             atomicOr(status, STRELKA_DEV_INSTANCE_OOB);
-            out[0] = bad; out[1] = bad; out[2] = bad;
+            out[0] = bad; out[1] = bad; out[2] = bad; out[3] = bad;
             continue;
         }
         const InstanceConstants* ic = &inst[instId];
@@ -62,13 +91,13 @@ __global__ void k_prep_tris(const float4* __restrict__ nodes, uint32_t numNodes,
         const uint32_t base = (uint32_t)ic->indexOffset + prim * 3u;
         if ((uint64_t)base + 2 >= numIndices) {
             atomicOr(status, STRELKA_DEV_INDEX_OOB);
-            out[0] = bad; out[1] = bad; out[2] = bad;
+            out[0] = bad; out[1] = bad; out[2] = bad; out[3] = bad;
             continue;
         }
         const uint32_t i0 = ib[base], i1 = ib[base + 1], i2 = ib[base + 2];
         if (i0 >= numVertices || i1 >= numVertices || i2 >= numVertices) {
             atomicOr(status, STRELKA_DEV_INDEX_OOB);
-            out[0] = bad; out[1] = bad; out[2] = bad;
+            out[0] = bad; out[1] = bad; out[2] = bad; out[3] = bad;
             continue;
         }
         const float* m = ic->objectToWorld.m;
@@ -78,6 +107,7 @@ __global__ void k_prep_tris(const float4* __restrict__ nodes, uint32_t numNodes,
         out[0] = f4(v0, __uint_as_float(instId));
         out[1] = f4(e0, __uint_as_float(prim));
         out[2] = f4(e1, 0.0f);
+        out[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
 }
 
@@ -95,7 +125,7 @@ __global__ void __launch_bounds__(kExtendBlock) k_megakernel(DevScene s, PathTra
     while (ps.depth < maxDepth) {
         HitRec h;
         uint32_t a = 0, b = 0;
-        bool found = s.numNodes != 0 && trace_closest<false>(s, ps.ro, ps.tmax, ps.rd, h, a, b);
+        bool found = s.numNodes != 0 && trace_closest_rec<false>(s, ps.ro, ps.tmax, ps.rd, h, a, b);
         ShadowReq sr;
         bool cont = shade(s, ubo, ps, found, h, sr);
         if (sr.kind != 0 && shadow_visible(s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
@@ -149,28 +179,46 @@ __global__ void __launch_bounds__(kSmallBlock) k_generate(PathTracerParam ubo, W
     }
 }
 
-// extend: closest-hit query for every queued path.
+// extend: closest-hit query for every queued path.  Each lane takes its next
+// path as soon as its current query ends (the warp keeps stepping while any
+// lane has work), so a warp does not wait for its longest ray.
 template <bool COUNT>
 __global__ void __launch_bounds__(kExtendBlock) k_extend(DevScene s, Wave w, int qin, unsigned long long* visitCounters)
 {
-    uint32_t nR = 0;
     const uint32_t count = w.counters[qin];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         w.counters[qin ^ 1] = 0;  // consumed by shade(k-1); refilled by shade(k)
         w.counters[2] = 0;        // consumed by shadow(k-1); refilled by shade(k)
     }
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
-    uint32_t nI = 0, nL = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const uint32_t slot = q[i];
-        const float4 o = w.ray_o[slot];
-        const float4 d = w.ray_d[slot];
-        HitRec h;
-        bool found = s.numNodes != 0 && trace_closest<COUNT>(s, xyz(o), o.w, xyz(d), h, nI, nL);
-        w.hit[slot] = found ? make_float4(h.u, h.v, h.t, __uint_as_float(h.instId))
-                            : make_float4(0.0f, 0.0f, 1e9f, __uint_as_float(SB_INVALID));
-        w.hitPrim[slot] = found ? h.primId : SB_INVALID;
+    uint32_t stackN[SB_STACK];
+    float stackT[SB_STACK];
+    uint32_t nI = 0, nL = 0, nR = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t slot = 0;
+    Trav T;
+    bool have = i < count;
+    if (have) {
+        slot = q[i];
+        const float4 o = w.ray_o[slot], d = w.ray_d[slot];
+        trav_init(s, T, xyz(o), o.w, xyz(d), false);
+    }
+    while (__any_sync(0xffffffffu, have)) {
+        if (!have) continue;
+        const bool done = T.cur == SB_INVALID || closest_step<COUNT>(s, T, stackN, stackT, nI, nL);
+        if (!done) continue;
+        w.hit[slot] = T.found ? make_float4(T.hit.u, T.hit.v, T.hit.t, __uint_as_float(T.hit.instId))
+                              : make_float4(0.0f, 0.0f, 1e9f, __uint_as_float(SB_INVALID));
+        w.hitPrim[slot] = T.found ? T.hit.primId : SB_INVALID;
         if (COUNT) ++nR;
+        i += stride;
+        have = i < count;
+        if (have) {
+            slot = q[i];
+            const float4 o = w.ray_o[slot], d = w.ray_d[slot];
+            trav_init(s, T, xyz(o), o.w, xyz(d), false);
+        }
     }
     if (COUNT) {
         atomicAdd(&visitCounters[0], (unsigned long long)nI);
@@ -258,33 +306,43 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerPar
     }
 }
 
-// shadow: any-hit query for every next-event request; adds visible ones.
+// shadow: any-hit query for every next-event request (reference depth-first
+// order); adds the visible ones.  Lanes take new requests as theirs finish.
 template <bool COUNT>
 __global__ void __launch_bounds__(kExtendBlock) k_shadow(DevScene s, Wave w, unsigned long long* visitCounters)
 {
     const uint32_t count = w.counters[2];
+    uint32_t stackN[SB_STACK];
     uint32_t nI = 0, nL = 0, nR = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const float4 o = w.sh_o[i];
-        const float4 d = w.sh_d[i];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    Trav T;
+    bool have = i < count;
+    if (have) {
+        const float4 o = w.sh_o[i], d = w.sh_d[i];
+        trav_init(s, T, xyz(o), o.w, xyz(d), true);
+    }
+    while (__any_sync(0xffffffffu, have)) {
+        if (!have) continue;
+        const bool done = T.cur == SB_INVALID || any_step<COUNT>(s, T, stackN, nI, nL);
+        if (!done) continue;
         const float4 cd = w.sh_cd[i];
         const int kind = (int)__float_as_uint(cd.w);
-        bool visible;
-        if (COUNT) {
-            ++nR;
-            HitRec h;
-            h.instId = SB_INVALID;
-            bool occl = trace_any<true>(s, xyz(o), o.w, xyz(d), h, nI, nL);
-            visible = !occl || (kind == 1 && h.instId < s.numInstances && __ldg(&s.inst[h.instId].lightId) != -1);
-        } else {
-            visible = shadow_visible(s, kind, xyz(o), o.w, xyz(d));
-        }
+        const bool visible = !T.found || (kind == 1 && T.hit.instId < s.numInstances &&
+                                          __ldg(&s.inst[T.hit.instId].lightId) != -1);
         if (visible) {
-            const uint32_t slot = __float_as_uint(d.w);
+            const uint32_t slot = __float_as_uint(w.sh_d[i].w);
             const float4 cg = w.sh_cg[i];
             v3 c = xyz(w.col[slot]);
             apply_shadow(c, xyz(cd), xyz(cg));
             w.col[slot] = f4(c, 0.0f);
+        }
+        if (COUNT) ++nR;
+        i += stride;
+        have = i < count;
+        if (have) {
+            const float4 o = w.sh_o[i], d = w.sh_d[i];
+            trav_init(s, T, xyz(o), o.w, xyz(d), true);
         }
     }
     if (COUNT) {
@@ -311,22 +369,28 @@ template <bool ANY, bool COUNT, bool REFINE>
 __global__ void __launch_bounds__(kExtendBlock) k_trace(DevScene s, const float4* __restrict__ rays, Hit* __restrict__ hits,
                                                         uint32_t n, unsigned long long* counters)
 {
+    uint32_t stackN[SB_STACK];
+    float stackT[SB_STACK];
     uint32_t nI = 0, nL = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 o = __ldg(&rays[2 * (size_t)i]);
-        const float4 d = __ldg(&rays[2 * (size_t)i + 1]);
-        HitRec h;
-        h.u = 0.0f;
-        h.v = 0.0f;
-        h.t = ANY ? 0.0f : 1e9f;
-        h.instId = SB_INVALID;
-        h.primId = SB_INVALID;
-        bool found = false;
-        if (s.numNodes != 0)
-            found = ANY ? trace_any<COUNT>(s, xyz(o), o.w, xyz(d), h, nI, nL)
-                        : trace_closest<COUNT>(s, xyz(o), o.w, xyz(d), h, nI, nL);
-        if (REFINE && found) refine_hit(s, xyz(o), xyz(d), h.instId, h.primId, h.t, h.u, h.v);
-        if (!found) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    Trav T;
+    bool have = i < n;
+    if (have) {
+        const float4 o = __ldg(&rays[2 * (size_t)i]), d = __ldg(&rays[2 * (size_t)i + 1]);
+        trav_init(s, T, xyz(o), o.w, xyz(d), ANY);
+    }
+    while (__any_sync(0xffffffffu, have)) {
+        if (!have) continue;
+        const bool done = T.cur == SB_INVALID || (ANY ? any_step<COUNT>(s, T, stackN, nI, nL)
+                                                      : closest_step<COUNT>(s, T, stackN, stackT, nI, nL));
+        if (!done) continue;
+        HitRec h = T.hit;
+        if (REFINE && T.found) {
+            const float4 o = __ldg(&rays[2 * (size_t)i]), d = __ldg(&rays[2 * (size_t)i + 1]);
+            refine_hit(s, xyz(o), xyz(d), h.instId, h.primId, h.t, h.u, h.v);
+        }
+        if (!T.found) {
             h.instId = SB_INVALID;
             h.primId = SB_INVALID;
             if (!ANY) {
@@ -341,6 +405,12 @@ __global__ void __launch_bounds__(kExtendBlock) k_trace(DevScene s, const float4
         out[2] = __float_as_uint(h.t);
         out[3] = h.instId;
         out[4] = h.primId;
+        i += stride;
+        have = i < n;
+        if (have) {
+            const float4 o = __ldg(&rays[2 * (size_t)i]), d = __ldg(&rays[2 * (size_t)i + 1]);
+            trav_init(s, T, xyz(o), o.w, xyz(d), ANY);
+        }
     }
     if (COUNT) {
         atomicAdd(&counters[0], (unsigned long long)nI);
@@ -363,8 +433,8 @@ struct StrelkaPathTracer {
     const void* keyIb = nullptr;
     const void* keyInst = nullptr;
     uint32_t keyNumNodes = 0;
-    float4* tris = nullptr;
-    size_t trisCap = 0;  // nodes
+    float4* rec = nullptr;  // 4 float4 per node (traverse.cuh record table)
+    size_t recCap = 0;      // nodes
     float* srgbLut = nullptr;
     uint32_t* status = nullptr;
     // wavefront
@@ -479,20 +549,20 @@ int ensure_scene(StrelkaPathTracer* pt, const BVHNode* nodes, uint32_t numNodes,
                  uint64_t version, cudaStream_t st)
 {
     if (pt->sceneVersion == version && pt->keyNodes == nodes && pt->keyVb == vb && pt->keyIb == ib && pt->keyInst == inst &&
-        pt->keyNumNodes == numNodes && pt->tris)
+        pt->keyNumNodes == numNodes && pt->rec)
         return STRELKA_OK;
-    if (numNodes > pt->trisCap || !pt->tris) {
-        if (pt->tris) cudaFree(pt->tris);
-        pt->tris = nullptr;
+    if (numNodes > pt->recCap || !pt->rec) {
+        if (pt->rec) cudaFree(pt->rec);
+        pt->rec = nullptr;
         size_t cap = std::max<size_t>(numNodes, 1);
-        SB_CUDA_TRY(cudaMalloc(&pt->tris, cap * 3 * sizeof(float4)));
-        pt->trisCap = cap;
+        SB_CUDA_TRY(cudaMalloc(&pt->rec, cap * 4 * sizeof(float4)));
+        pt->recCap = cap;
     }
     if (numNodes) {
         Timer t(pt, KC_PREP, st);
         int grid = std::min<int>((numNodes + 255) / 256, pt->numSMs * 16);
-        k_prep_tris<<<grid, 256, 0, st>>>(reinterpret_cast<const float4*>(nodes), numNodes, inst, numInstances, ib, numIndices,
-                                          vb, numVertices, pt->tris, pt->status);
+        k_prep_rec<<<grid, 256, 0, st>>>(reinterpret_cast<const float4*>(nodes), numNodes, inst, numInstances, ib, numIndices,
+                                         vb, numVertices, pt->rec, pt->status);
         SB_CUDA_TRY(cudaGetLastError());
     }
     pt->sceneVersion = version;
@@ -508,7 +578,8 @@ DevScene make_scene(StrelkaPathTracer* pt, const PathTracerDesc* d)
 {
     DevScene s{};
     s.nodes = reinterpret_cast<const float4*>(d->bvhNodes);
-    s.tris = pt->tris;
+    s.tris = nullptr;
+    s.rec = pt->rec;
     s.numNodes = d->numNodes;
     s.numVertices = d->numVertices;
     s.vb = d->vb;
@@ -581,7 +652,7 @@ extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
 {
     if (!pt) return STRELKA_OK;
     free_wave(pt);
-    if (pt->tris) cudaFree(pt->tris);
+    if (pt->rec) cudaFree(pt->rec);
     if (pt->srgbLut) cudaFree(pt->srgbLut);
     if (pt->status) cudaFree(pt->status);
     if (pt->visitCounters) cudaFree(pt->visitCounters);

@@ -652,7 +652,7 @@ __device__ __forceinline__ bool shadow_visible(const DevScene& s, int kind, v3 o
     HitRec h;
     h.instId = SB_INVALID;
     uint32_t a = 0, b = 0;
-    bool occl = trace_any<false>(s, o, tmax, d, h, a, b);
+    bool occl = trace_any_rec<false>(s, o, tmax, d, h, a, b);
     if (!occl) return true;
     if (kind == 1 && h.instId < s.numInstances && __ldg(&s.inst[h.instId].lightId) != -1) return true;
     return false;

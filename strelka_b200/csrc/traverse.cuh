@@ -23,6 +23,7 @@ namespace sb {
 struct DevScene {
     const float4* nodes;  // 2 float4 per BVHNode
     const float4* tris;   // 3 float4 per node (leaf slots only)
+    const float4* rec;    // 4 float4 per node: node-pair records / leaf triangles
     uint32_t numNodes;
     uint32_t numVertices;
     const Vertex* vb;
@@ -181,6 +182,439 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, v3 o, float tmax, v
         node = __float_as_uint(hi.w);
     }
     return false;
+}
+
+}  // namespace sb
+
+// ===========================================================================
+// Node-pair traversal.
+//
+// A derived table of 4 float4 per node slot is built once per scene version:
+//   inner node n (children L = n+1 and R = escape(n+1), the implicit tree of
+//   the reference's depth-first layout, bvh.cpp:182-220):
+//     [0] = L box min | L ref   [1] = L box max | R ref
+//     [2] = R box min | 0       [3] = R box max | 0
+//   leaf node n:  [0] = v0 | instId  [1] = e0 | primId  [2] = e1 | 0
+// where a child ref is its node index, with bit 31 set for a leaf child and
+// 0xFFFFFFFF for a missing one.  Processing one inner record tests both
+// children with one 64-byte fetch: an inner child's box exactly as the
+// reference tests it when it visits that node, a leaf child's triangle
+// exactly as the reference tests it when it reaches that leaf.  So the set of
+// triangles a query can test is the reference's; only the order differs.
+//
+// Closest hit visits the nearer child first, keeps the farther on a
+// per-thread stack with its entry distance, and drops any subtree whose entry
+// exceeds the best hit by more than a relative 2^-12; the closest t is the
+// reference's, and on exact ties in t the winning primitive may differ.
+// Any hit keeps the reference's depth-first order exactly: the right child
+// (an inner node whose box was hit, or a leaf) is pushed until the left
+// subtree is done.  A full stack falls back to the stackless reference loop
+// (closest: restart from the root with the best hit so far; any: continue
+// from the child being entered, which visits the rest of the tree in the
+// same depth-first order).
+// ===========================================================================
+
+namespace sb {
+
+#define SB_STACK 32
+#define SB_LEAF_BIT 0x80000000u
+
+struct RayQ {
+    v3 o, d, inv;
+    float tmax;
+};
+
+__device__ __forceinline__ RayQ make_ray(v3 o, float tmax, v3 d)
+{
+    RayQ r;
+    r.o = o;
+    r.d = d;
+    r.tmax = tmax;
+    r.inv = V(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    return r;
+}
+
+// leaf triangle of node `leaf` in the record table
+__device__ __forceinline__ bool rec_triangle(const DevScene& s, const RayQ& r, uint32_t leaf, float& t, float& bu, float& bv,
+                                             uint32_t& instId, uint32_t& primId)
+{
+    const float4* tp = &s.rec[4 * (size_t)leaf];
+    const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+    instId = __float_as_uint(a.w);
+    primId = __float_as_uint(b.w);
+    return ray_triangle(r.o, r.d, xyz(a), xyz(b), xyz(c), t, bu, bv);
+}
+
+// Result of a stackless fallback (returned by value so that the caller's
+// traversal state can stay in registers).
+struct Fallback {
+    HitRec hit;
+    float minHit;
+    uint32_t nInner, nLeaf;
+    bool found;
+};
+
+// The reference's stackless closest-hit loop over the node array, reading
+// leaf triangles from the record table; runs from the root with the best hit
+// so far (used when the stack overflows).
+template <bool COUNT>
+__device__ __noinline__ Fallback closest_stackless_rec(const DevScene s, const RayQ r, float minHit, HitRec hit, bool found)
+{
+    Fallback f;
+    f.nInner = 0;
+    f.nLeaf = 0;
+    uint32_t node = 0;
+    const uint32_t cap = 2u * s.numNodes + 2u;
+    uint32_t visits = 0;
+    while (node != SB_INVALID) {
+        if (node >= s.numNodes) { raise_status(s, STRELKA_DEV_NODE_OOB); break; }
+        if (++visits > cap) { raise_status(s, STRELKA_DEV_TRAVERSAL_CAP); break; }
+        const float4 lo = __ldg(&s.nodes[2 * (size_t)node]);
+        const float4 hi = __ldg(&s.nodes[2 * (size_t)node + 1]);
+        if (__float_as_uint(lo.w) != SB_INVALID) {
+            if (COUNT) ++f.nLeaf;
+            float t, bu, bv;
+            uint32_t iid, pid;
+            if (rec_triangle(s, r, node, t, bu, bv, iid, pid) && (t < r.tmax) && (t < minHit)) {
+                minHit = t;
+                hit.t = t;
+                hit.u = bu;
+                hit.v = bv;
+                hit.instId = iid;
+                hit.primId = pid;
+                found = true;
+            }
+            node = __float_as_uint(hi.w);
+            continue;
+        }
+        if (COUNT) ++f.nInner;
+        float boxT;
+        if (ray_box(r.o, r.inv, lo, hi, boxT) && !(boxT > r.tmax) && !(boxT > minHit * SB_PRUNE_SCALE)) {
+            ++node;
+            continue;
+        }
+        node = __float_as_uint(hi.w);
+    }
+    f.hit = hit;
+    f.minHit = minHit;
+    f.found = found;
+    return f;
+}
+
+// The reference's stackless any-hit loop from `node` (raytracing.h:249-286).
+template <bool COUNT>
+__device__ __noinline__ Fallback any_stackless_rec(const DevScene s, const RayQ r, uint32_t node, HitRec hit)
+{
+    Fallback f;
+    f.nInner = 0;
+    f.nLeaf = 0;
+    f.found = false;
+    f.minHit = 0.0f;
+    const uint32_t cap = 2u * s.numNodes + 2u;
+    uint32_t visits = 0;
+    while (node != SB_INVALID) {
+        if (node >= s.numNodes) { raise_status(s, STRELKA_DEV_NODE_OOB); break; }
+        if (++visits > cap) { raise_status(s, STRELKA_DEV_TRAVERSAL_CAP); break; }
+        const float4 lo = __ldg(&s.nodes[2 * (size_t)node]);
+        const float4 hi = __ldg(&s.nodes[2 * (size_t)node + 1]);
+        if (__float_as_uint(lo.w) != SB_INVALID) {
+            if (COUNT) ++f.nLeaf;
+            float t, bu, bv;
+            uint32_t iid, pid;
+            bool isect = rec_triangle(s, r, node, t, bu, bv, iid, pid);
+            hit.t = t;
+            if (isect && (t < r.tmax)) {
+                hit.instId = iid;
+                hit.primId = pid;
+                f.found = true;
+                break;
+            }
+        } else {
+            if (COUNT) ++f.nInner;
+            float boxT;
+            if (ray_box(r.o, r.inv, lo, hi, boxT)) {
+                if (boxT > r.tmax) {
+                    node = __float_as_uint(hi.w);
+                    continue;
+                }
+                ++node;
+                continue;
+            }
+        }
+        node = __float_as_uint(hi.w);
+    }
+    f.hit = hit;
+    return f;
+}
+
+// Per-query traversal state for the step functions.
+struct Trav {
+    RayQ r;
+    float minHit;
+    uint32_t cur;  // record to process next; SB_INVALID = pop
+    int sp;
+    uint32_t steps;
+    bool found;
+    HitRec hit;
+};
+
+__device__ __forceinline__ void trav_init(const DevScene& s, Trav& T, v3 o, float tmax, v3 d, bool any)
+{
+    T.r = make_ray(o, tmax, d);
+    T.minHit = 1e9f;
+    T.sp = 0;
+    T.steps = 0;
+    T.found = false;
+    T.hit.u = 0.0f;
+    T.hit.v = 0.0f;
+    T.hit.t = any ? 0.0f : 1e9f;
+    T.hit.instId = SB_INVALID;
+    T.hit.primId = SB_INVALID;
+    T.cur = s.numNodes ? 0u : SB_INVALID;
+}
+
+// One closest-hit step: processes the record T.cur (or the root leaf), then
+// pops until a record to process is found.  Returns true when finished.
+template <bool COUNT>
+__device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, uint32_t* stackN, float* stackT, uint32_t& nInner,
+                                             uint32_t& nLeaf)
+{
+    const uint32_t cur = T.cur;
+    if (cur != SB_INVALID) {
+        if (cur >= s.numNodes || ++T.steps > s.numNodes + 1u) {
+            raise_status(s, cur >= s.numNodes ? STRELKA_DEV_NODE_OOB : STRELKA_DEV_TRAVERSAL_CAP);
+            return true;
+        }
+        const float4* rp = &s.rec[4 * (size_t)cur];
+        const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+        const uint32_t L = __float_as_uint(r0.w);
+        if (cur == 0 && __float_as_uint(__ldg(&s.nodes[0]).w) != SB_INVALID) {
+            // the root itself is a leaf
+            if (COUNT) ++nLeaf;
+            float t, bu, bv;
+            uint32_t iid, pid;
+            if (rec_triangle(s, T.r, 0, t, bu, bv, iid, pid) && (t < T.r.tmax) && (t < T.minHit)) {
+                T.minHit = t;
+                T.hit.t = t;
+                T.hit.u = bu;
+                T.hit.v = bv;
+                T.hit.instId = iid;
+                T.hit.primId = pid;
+                T.found = true;
+            }
+            T.cur = SB_INVALID;
+        } else {
+            if (COUNT) ++nInner;
+            const float4 r2 = __ldg(rp + 2), r3 = __ldg(rp + 3);
+            const uint32_t R = __float_as_uint(r1.w);
+            bool goL = false, goR = false;
+            float tL = 0.0f, tR = 0.0f;
+            // children in the reference's order: left, then right
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const uint32_t c = k == 0 ? L : R;
+                if (c == SB_INVALID) continue;
+                if (c & SB_LEAF_BIT) {
+                    if (COUNT) ++nLeaf;
+                    float t, bu, bv;
+                    uint32_t iid, pid;
+                    if (rec_triangle(s, T.r, c & ~SB_LEAF_BIT, t, bu, bv, iid, pid) && (t < T.r.tmax) && (t < T.minHit)) {
+                        T.minHit = t;
+                        T.hit.t = t;
+                        T.hit.u = bu;
+                        T.hit.v = bv;
+                        T.hit.instId = iid;
+                        T.hit.primId = pid;
+                        T.found = true;
+                    }
+                } else {
+                    float bt;
+                    const bool h = k == 0 ? ray_box(T.r.o, T.r.inv, r0, r1, bt) : ray_box(T.r.o, T.r.inv, r2, r3, bt);
+                    if (k == 0) { goL = h; tL = bt; } else { goR = h; tR = bt; }
+                }
+            }
+            const float lim = T.minHit * SB_PRUNE_SCALE;
+            goL = goL && !(tL > T.r.tmax) && !(tL > lim);
+            goR = goR && !(tR > T.r.tmax) && !(tR > lim);
+            if (goL && goR) {
+                const bool leftNear = tL <= tR;
+                const uint32_t nearC = leftNear ? L : R, farC = leftNear ? R : L;
+                const float farT = leftNear ? tR : tL;
+                if (T.sp < SB_STACK) {
+                    stackN[T.sp] = farC;
+                    stackT[T.sp] = farT;
+                    ++T.sp;
+                    T.cur = nearC;
+                } else {
+                    // stack full: finish with the stackless loop from the root
+                    const Fallback f = closest_stackless_rec<COUNT>(s, T.r, T.minHit, T.hit, T.found);
+                    T.hit = f.hit;
+                    T.minHit = f.minHit;
+                    T.found = f.found;
+                    if (COUNT) {
+                        nInner += f.nInner;
+                        nLeaf += f.nLeaf;
+                    }
+                    T.cur = SB_INVALID;
+                    T.sp = 0;
+                    return true;
+                }
+            } else if (goL) {
+                T.cur = L;
+            } else if (goR) {
+                T.cur = R;
+            } else {
+                T.cur = SB_INVALID;
+            }
+        }
+    }
+    if (T.cur == SB_INVALID) {
+        const float lim = T.minHit * SB_PRUNE_SCALE;
+        while (T.sp > 0) {
+            --T.sp;
+            if (!(stackT[T.sp] > lim)) {
+                T.cur = stackN[T.sp];
+                break;
+            }
+        }
+        if (T.cur == SB_INVALID) return true;
+    }
+    return false;
+}
+
+// One any-hit step (depth-first order).  Returns true when finished; T.found
+// tells whether a hit with t < tmax was found.
+template <bool COUNT>
+__device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, uint32_t* stackN, uint32_t& nInner, uint32_t& nLeaf)
+{
+    uint32_t cur = T.cur;
+    if (cur != SB_INVALID) {
+        if (cur >= s.numNodes || ++T.steps > s.numNodes + 1u) {
+            raise_status(s, cur >= s.numNodes ? STRELKA_DEV_NODE_OOB : STRELKA_DEV_TRAVERSAL_CAP);
+            return true;
+        }
+        if (cur == 0 && __float_as_uint(__ldg(&s.nodes[0]).w) != SB_INVALID) {
+            if (COUNT) ++nLeaf;
+            float t, bu, bv;
+            uint32_t iid, pid;
+            bool isect = rec_triangle(s, T.r, 0, t, bu, bv, iid, pid);
+            T.hit.t = t;
+            if (isect && (t < T.r.tmax)) {
+                T.hit.instId = iid;
+                T.hit.primId = pid;
+                T.found = true;
+                return true;
+            }
+            T.cur = SB_INVALID;
+        } else {
+            if (COUNT) ++nInner;
+            const float4* rp = &s.rec[4 * (size_t)cur];
+            const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1), r2 = __ldg(rp + 2), r3 = __ldg(rp + 3);
+            const uint32_t L = __float_as_uint(r0.w), R = __float_as_uint(r1.w);
+            bool goL = false;
+            if (L != SB_INVALID) {
+                if (L & SB_LEAF_BIT) {
+                    if (COUNT) ++nLeaf;
+                    float t, bu, bv;
+                    uint32_t iid, pid;
+                    bool isect = rec_triangle(s, T.r, L & ~SB_LEAF_BIT, t, bu, bv, iid, pid);
+                    T.hit.t = t;
+                    if (isect && (t < T.r.tmax)) {
+                        T.hit.instId = iid;
+                        T.hit.primId = pid;
+                        T.found = true;
+                        return true;
+                    }
+                } else {
+                    float bt;
+                    goL = ray_box(T.r.o, T.r.inv, r0, r1, bt) && !(bt > T.r.tmax);
+                }
+            }
+            bool rPending = false;  // R still to visit after L's subtree
+            if (R != SB_INVALID) {
+                if (R & SB_LEAF_BIT) {
+                    rPending = true;
+                } else {
+                    float bt;
+                    rPending = ray_box(T.r.o, T.r.inv, r2, r3, bt) && !(bt > T.r.tmax);
+                }
+            }
+            if (goL) {
+                if (rPending) {
+                    if (T.sp < SB_STACK) {
+                        stackN[T.sp++] = R;
+                    } else {
+                        // stack full: the stackless loop from L visits the
+                        // rest of the tree in the same order
+                        const Fallback f = any_stackless_rec<COUNT>(s, T.r, L, T.hit);
+                        T.hit = f.hit;
+                        T.found = f.found;
+                        if (COUNT) {
+                            nInner += f.nInner;
+                            nLeaf += f.nLeaf;
+                        }
+                        T.cur = SB_INVALID;
+                        T.sp = 0;
+                        return true;
+                    }
+                }
+                T.cur = L;
+            } else if (rPending) {
+                T.cur = R;
+            } else {
+                T.cur = SB_INVALID;
+            }
+        }
+    }
+    // a leaf reached as the next node (a pending right child or a popped one)
+    for (;;) {
+        if (T.cur == SB_INVALID) {
+            if (T.sp == 0) return true;
+            T.cur = stackN[--T.sp];
+        }
+        if (!(T.cur & SB_LEAF_BIT)) return false;
+        if (COUNT) ++nLeaf;
+        float t, bu, bv;
+        uint32_t iid, pid;
+        bool isect = rec_triangle(s, T.r, T.cur & ~SB_LEAF_BIT, t, bu, bv, iid, pid);
+        T.hit.t = t;
+        if (isect && (t < T.r.tmax)) {
+            T.hit.instId = iid;
+            T.hit.primId = pid;
+            T.found = true;
+            return true;
+        }
+        T.cur = SB_INVALID;
+    }
+}
+
+template <bool COUNT>
+__device__ __forceinline__ bool trace_closest_rec(const DevScene& s, v3 o, float tmax, v3 d, HitRec& hit, uint32_t& nInner,
+                                                  uint32_t& nLeaf)
+{
+    uint32_t stackN[SB_STACK];
+    float stackT[SB_STACK];
+    Trav T;
+    trav_init(s, T, o, tmax, d, false);
+    if (T.cur != SB_INVALID)
+        while (!closest_step<COUNT>(s, T, stackN, stackT, nInner, nLeaf)) {
+        }
+    hit = T.hit;
+    return T.found;
+}
+
+template <bool COUNT>
+__device__ __forceinline__ bool trace_any_rec(const DevScene& s, v3 o, float tmax, v3 d, HitRec& hit, uint32_t& nInner,
+                                              uint32_t& nLeaf)
+{
+    uint32_t stackN[SB_STACK];
+    Trav T;
+    trav_init(s, T, o, tmax, d, true);
+    if (T.cur != SB_INVALID)
+        while (!any_step<COUNT>(s, T, stackN, nInner, nLeaf)) {
+        }
+    hit = T.hit;
+    return T.found;
 }
 
 }  // namespace sb

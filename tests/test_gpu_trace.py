@@ -69,16 +69,21 @@ def test_any_hit_exact(cuda, soup_setup, shadow):
     assert np.array_equal(g, o)
 
 
-def test_visit_counters(cuda, soup_setup):
-    s, view, ds, pt = soup_setup
-    rays = scenes.rays_soup(50_000, 4)
-    _, cg = run_trace(cuda, pt, ds, rays, abi.TRACE_CLOSEST | abi.TRACE_COUNT)
-    _, _, co = oracle.trace(view, rays, prune=True)
+@pytest.mark.parametrize("setup", ["soup_setup", "cornell_setup"])
+def test_visit_counters(cuda, setup, request):
+    # the kernels count node-pair records and triangle tests; the oracle
+    # replays the same traversal rule (prune=2) and must count the same
+    s, view, ds, pt = request.getfixturevalue(setup)
+    rays = scenes.rays_soup(50_000, 4) if setup == "soup_setup" else interior_rays(50_000, 4)
+    g, cg = run_trace(cuda, pt, ds, rays, abi.TRACE_CLOSEST | abi.TRACE_COUNT)
+    o, _, co = oracle.trace(view, rays, prune=2)
     assert np.array_equal(cg, co)
-    rays = scenes.rays_soup(50_000, 5, shadow=True)
-    _, cg = run_trace(cuda, pt, ds, rays, abi.TRACE_ANY | abi.TRACE_COUNT)
-    _, _, co = oracle.trace(view, rays, any_hit=True)
+    assert np.array_equal(g, o)  # same traversal order: identical records, ties included
+    shadow = scenes.rays_soup(50_000, 5, shadow=True) if setup == "soup_setup" else interior_rays(50_000, 5, tmax=0.4)
+    g, cg = run_trace(cuda, pt, ds, shadow, abi.TRACE_ANY | abi.TRACE_COUNT)
+    o, _, co = oracle.trace(view, shadow, any_hit=True, prune=2)
     assert np.array_equal(cg, co)
+    assert np.array_equal(g, o)
 
 
 def test_refine_within_2ulp_of_fp64(cuda, cornell_setup):
