@@ -164,6 +164,57 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_traversal(args):
+    """--workload traversal: the ray-query microbenchmark (1M-triangle soup,
+    4M rays, closest hit and any hit with tmax uniform in [0.1, 2])."""
+    import torch
+
+    from strelka_b200 import abi, scenes
+    from strelka_b200.render import DeviceScene, PathTracer, to_device
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    hs = scenes.soup(args.tris, 0)
+    ds = DeviceScene(hs)
+    n = args.rays
+    res = {}
+    stream = torch.cuda.current_stream()
+    peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    for name, shadow, flags in (("closest", False, abi.TRACE_CLOSEST), ("any", True, abi.TRACE_ANY)):
+        rays = to_device(scenes.rays_soup(n, 1 if not shadow else 2, shadow=shadow))
+        hits = torch.empty(n * 20, dtype=torch.uint8, device="cuda")
+        pt = PathTracer()
+        desc = ds.trace_desc(rays, hits, flags)
+        for _ in range(args.warmup):
+            pt.trace(desc, stream)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            pt.trace(desc, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
+        pt.trace(ds.trace_desc(rays, hits, flags | abi.TRACE_COUNT, cnt), stream)
+        c = cnt.cpu().numpy()
+        out_bytes = 20
+        bytes_alg = 64 * int(c[0]) + 48 * int(c[1]) + (32 + out_bytes) * n
+        res[name] = {"mrays_s": n / (ms * 1e-3) / 1e6, "ms": ms, "records_per_ray": c[0] / n,
+                     "tests_per_ray": c[1] / n, "achieved_gbs": bytes_alg / (ms * 1e-3) / 1e9,
+                     "frac": bytes_alg / (ms * 1e-3) / 1e9 / peak}
+        pt.close()
+    line = {"metric": "Mrays/s (traversal microbenchmark)", "value": res["closest"]["mrays_s"], "unit": "Mrays/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"traversal microbenchmark: {args.tris} soup triangles (log-normal size, mu=ln 0.003, "
+                                   f"sigma=0.5), {n} rays, closest + any hit", "l2": "inputs larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": res["closest"]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": res["closest"]["frac"], "traffic": None},
+            "detail": res}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -181,7 +232,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-step-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="large", choices=["large", "traversal"])
+    ap.add_argument("--tris", type=int, default=1_000_000)
+    ap.add_argument("--rays", type=int, default=4_000_000)
     args = ap.parse_args()
+    if args.workload == "traversal":
+        run_traversal(args)
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "strelka" else args.warmup
 
     if args.impl == "reference":
@@ -190,7 +247,7 @@ def main():
 
     import torch
 
-    from strelka_b200 import abi
+    from strelka_b200 import abi, multigpu
     from strelka_b200.render import DeviceScene, PathTracer, accumulation_param, resolve, tonemap_param
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -220,7 +277,7 @@ def main():
 
     def frame(it):
         # PtRender::drawFrame (src/render/ptrender.cpp:735-862) for one view
-        p = hs.param(frameNumber=rank * 100000 + it, iteration=it)
+        p = hs.param(frameNumber=multigpu.frame_number(rank, it), iteration=it)
         pt.execute(ds.desc(p, sb), total, 1, it, stream)
         ap_ = accumulation_param(W, H, it)
         resolve(p, sb, tp, ap_ if it > 0 else None, hist if it > 0 else None, acc, None, rgba8, stream)
@@ -255,10 +312,7 @@ def main():
     el_ms = e0.elapsed_time(e1)
     # per-kernel CUDA-event times summed over every launch of the timed region
     times = pt.kernel_times(stream)
-    if dist:
-        t = torch.tensor([el_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el_ms = float(t.item())
+    el_ms = multigpu.max_over_ranks(el_ms, dist, device="cuda")
 
     value = world * total * args.steps / (el_ms * 1e-3) / 1e6
 
@@ -268,7 +322,8 @@ def main():
     launches = sum(c for _, c in times.values()) + args.steps  # + one resolve per frame
     pt_count = PathTracer(mode=mode, chunk_paths=args.chunk, count=True)
     for k in range(args.steps):
-        pt_count.execute(ds.desc(hs.param(frameNumber=rank * 100000 + args.warmup + k), sb), total, 1, 0, stream)
+        pt_count.execute(ds.desc(hs.param(frameNumber=multigpu.frame_number(rank, args.warmup + k)), sb), total, 1, 0,
+                         stream)
     cnt = pt_count.counters(stream)
     pt_count.close()
     # algorithmic bytes of the closest-hit traversal: 64 B per node-pair
@@ -295,11 +350,7 @@ def main():
         host_img.copy_(rgba8, non_blocking=True)
     f1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = multigpu.max_over_ranks(f0.elapsed_time(f1), dist, device="cuda")
     e2e = world * total * args.steps / (e2e_ms * 1e-3) / 1e6
     img = host_img.numpy()
     if not (img[3::4] == 255).all():
