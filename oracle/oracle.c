@@ -653,41 +653,52 @@ static int pair_any(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, unsi
                 (*nI)++;
                 uint32_t L, R;
                 pair_children(s, cur, &L, &R);
-                int goL = 0;
+                int goL = 0, rPending = 0;
                 if (L != INVALID_INDEX) {
-                    if (node_is_leaf(s, L)) {
-                        (*nL)++;
-                        float t, bu, bv;
-                        uint32_t iid, pid;
-                        int is = leaf_test(s, L, o, d, &t, &bu, &bv, &iid, &pid);
-                        hit->t = t;
-                        if (is && t < tmax) {
-                            hit->instId = iid;
-                            hit->primId = pid;
-                            return 1;
-                        }
-                    } else {
-                        float bt;
-                        goL = oracle_intersect_ray_box(oo, inv, s->nodes[L].minBounds, s->nodes[L].maxBounds, &bt) &&
-                              !(bt > tmax);
-                    }
+                    float bt;
+                    goL = node_is_leaf(s, L) ||
+                          (oracle_intersect_ray_box(oo, inv, s->nodes[L].minBounds, s->nodes[L].maxBounds, &bt) &&
+                           !(bt > tmax));
                 }
-                int rPending = 0;
                 if (R != INVALID_INDEX) {
-                    if (node_is_leaf(s, R)) {
-                        rPending = 1;
-                    } else {
-                        float bt;
-                        rPending = oracle_intersect_ray_box(oo, inv, s->nodes[R].minBounds, s->nodes[R].maxBounds, &bt) &&
-                                   !(bt > tmax);
-                    }
+                    float bt;
+                    rPending = node_is_leaf(s, R) ||
+                               (oracle_intersect_ray_box(oo, inv, s->nodes[R].minBounds, s->nodes[R].maxBounds, &bt) &&
+                                !(bt > tmax));
                 }
                 if (goL) {
                     if (rPending) {
                         if (sp < PAIR_STACK) {
                             stackN[sp++] = R;
                         } else {
-                            return any_hit(s, o, tmax, d, hit, nI, nL); /* unreachable with trees of depth <= 32 */
+                            /* stackless loop from L: the rest of the tree in the same order */
+                            uint32_t node = L;
+                            uint64_t cap = 2ull * s->numNodes + 2, visits = 0;
+                            while (node != INVALID_INDEX) {
+                                if (node >= s->numNodes || ++visits > cap) break;
+                                const BVHNode* n = &s->nodes[node];
+                                if ((uint32_t)n->instId != INVALID_INDEX) {
+                                    (*nL)++;
+                                    float t, bu, bv;
+                                    uint32_t iid, pid;
+                                    int is = leaf_test(s, node, o, d, &t, &bu, &bv, &iid, &pid);
+                                    hit->t = t;
+                                    if (is && t < tmax) {
+                                        hit->instId = iid;
+                                        hit->primId = pid;
+                                        return 1;
+                                    }
+                                } else {
+                                    (*nI)++;
+                                    float bt;
+                                    if (oracle_intersect_ray_box(oo, inv, n->minBounds, n->maxBounds, &bt) && !(bt > tmax)) {
+                                        ++node;
+                                        continue;
+                                    }
+                                }
+                                node = (uint32_t)n->nodeOffset;
+                            }
+                            return 0;
                         }
                     }
                     cur = L;

@@ -12,7 +12,8 @@ import ctypes as C
 import os
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libstrelka_b200.so")
+# STRELKA_B200_LIB selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("STRELKA_B200_LIB", os.path.join(_PKG, "libstrelka_b200.so"))
 
 # status codes
 OK = 0

@@ -27,6 +27,14 @@ constexpr int kExtendBlock = 128;
 constexpr int kShadeBlock = 128;
 constexpr int kSmallBlock = 256;
 
+// Minimum resident blocks per SM requested for the any-hit (shadow) kernel:
+// 10 blocks of 128 threads fit its registers without spills and measured
+// faster than the compiler's default; the closest-hit kernels keep the
+// default (a cap makes them spill).
+#ifndef SB_SHADOW_MINBLOCKS
+#define SB_SHADOW_MINBLOCKS 10
+#endif
+
 enum KernelClass { KC_GENERATE = 0, KC_EXTEND, KC_SHADE, KC_SHADOW, KC_FINALIZE, KC_MEGAKERNEL, KC_PREP, KC_COUNT };
 const char* kKernelNames[KC_COUNT] = {"generate", "extend", "shade", "shadow", "finalize", "megakernel", "prep"};
 
@@ -309,7 +317,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerPar
 // shadow: any-hit query for every next-event request (reference depth-first
 // order); adds the visible ones.  Lanes take new requests as theirs finish.
 template <bool COUNT>
-__global__ void __launch_bounds__(kExtendBlock) k_shadow(DevScene s, Wave w, unsigned long long* visitCounters)
+__global__ void __launch_bounds__(kExtendBlock, SB_SHADOW_MINBLOCKS) k_shadow(DevScene s, Wave w, unsigned long long* visitCounters)
 {
     const uint32_t count = w.counters[2];
     uint32_t stackN[SB_STACK];

@@ -511,33 +511,16 @@ __device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, uint32_t* s
             const float4* rp = &s.rec[4 * (size_t)cur];
             const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1), r2 = __ldg(rp + 2), r3 = __ldg(rp + 3);
             const uint32_t L = __float_as_uint(r0.w), R = __float_as_uint(r1.w);
-            bool goL = false;
+            // a leaf child is always visited; an inner child when its box is
+            // hit within tmax (raytracing.h:249-286 reaches the same nodes)
+            bool goL = false, rPending = false;
             if (L != SB_INVALID) {
-                if (L & SB_LEAF_BIT) {
-                    if (COUNT) ++nLeaf;
-                    float t, bu, bv;
-                    uint32_t iid, pid;
-                    bool isect = rec_triangle(s, T.r, L & ~SB_LEAF_BIT, t, bu, bv, iid, pid);
-                    T.hit.t = t;
-                    if (isect && (t < T.r.tmax)) {
-                        T.hit.instId = iid;
-                        T.hit.primId = pid;
-                        T.found = true;
-                        return true;
-                    }
-                } else {
-                    float bt;
-                    goL = ray_box(T.r.o, T.r.inv, r0, r1, bt) && !(bt > T.r.tmax);
-                }
+                float bt;
+                goL = (L & SB_LEAF_BIT) || (ray_box(T.r.o, T.r.inv, r0, r1, bt) && !(bt > T.r.tmax));
             }
-            bool rPending = false;  // R still to visit after L's subtree
             if (R != SB_INVALID) {
-                if (R & SB_LEAF_BIT) {
-                    rPending = true;
-                } else {
-                    float bt;
-                    rPending = ray_box(T.r.o, T.r.inv, r2, r3, bt) && !(bt > T.r.tmax);
-                }
+                float bt;
+                rPending = (R & SB_LEAF_BIT) || (ray_box(T.r.o, T.r.inv, r2, r3, bt) && !(bt > T.r.tmax));
             }
             if (goL) {
                 if (rPending) {
@@ -546,7 +529,7 @@ __device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, uint32_t* s
                     } else {
                         // stack full: the stackless loop from L visits the
                         // rest of the tree in the same order
-                        const Fallback f = any_stackless_rec<COUNT>(s, T.r, L, T.hit);
+                        const Fallback f = any_stackless_rec<COUNT>(s, T.r, L & ~SB_LEAF_BIT, T.hit);
                         T.hit = f.hit;
                         T.found = f.found;
                         if (COUNT) {
