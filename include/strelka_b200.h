@@ -403,6 +403,51 @@ int strelka_trace_host(StrelkaPathTracer* pt, const TraceDesc* desc, const Ray* 
 int strelka_trace_execute_noalloc(const TraceDesc* desc, uint32_t* deviceStatus, void* stream);
 
 /* ------------------------------------------------------------------------- */
+/* Neural radiance cache (no counterpart in the reference): a multiresolution
+ * hash-grid encoding (16 levels x 2 FP16 features, 2^log2TableSize entries
+ * per level, growth 1.5) of the position, degree-4 spherical harmonics of the
+ * direction, the normal and the roughness, fed to a 64-wide MLP with 4 hidden
+ * ReLU layers and 3 linear outputs (FP16 weights and activations, FP32
+ * accumulation on tensor cores), trained online with Adam on the relative L2
+ * loss.  Pointers to records are device pointers. */
+typedef struct StrelkaNrcRecord {
+    float pos[3];
+    float dir[3];      /* outgoing direction (towards the previous vertex) */
+    float normal[3];
+    float roughness;
+    float target[3];   /* training: radiance target; path-tracer queries: throughput */
+    uint32_t slot;     /* path-tracer queries: wavefront slot */
+    uint32_t pad[2];
+} StrelkaNrcRecord;    /* 64 bytes */
+
+typedef struct StrelkaNrcConfig {
+    float sceneMin[3];
+    float sceneMax[3];
+    float learningRate;     /* Adam, 1e-2 */
+    uint32_t seed;
+    uint32_t log2TableSize; /* 19 */
+    uint32_t pad[3];
+} StrelkaNrcConfig;
+
+typedef struct StrelkaNrc StrelkaNrc;
+
+int strelka_nrc_create(const StrelkaNrcConfig* config, StrelkaNrc** out);
+int strelka_nrc_destroy(StrelkaNrc* nrc);
+/* outRGB[3*i + c] = network output for records[i] (device pointers). */
+int strelka_nrc_infer(StrelkaNrc* nrc, const StrelkaNrcRecord* records, uint32_t n, float* outRGB, void* stream);
+/* One Adam step on the batch; *lossOut (host, may be NULL) receives the mean loss. */
+int strelka_nrc_train(StrelkaNrc* nrc, const StrelkaNrcRecord* samples, uint32_t n, float* lossOut, void* stream);
+/* Gradients of sum_i sum_c loss without updating (host outputs, may be NULL):
+ * mlpGrad (numMlpParams floats), gridGrad (numGridParams floats), lossSum. */
+int strelka_nrc_gradients(StrelkaNrc* nrc, const StrelkaNrcRecord* samples, uint32_t n, float* mlpGrad,
+                          float* gridGrad, float* lossSum, void* stream);
+/* FP32 master parameters, host arrays (numMlpParams and numGridParams floats). */
+int strelka_nrc_get_params(StrelkaNrc* nrc, float* mlp, float* grid);
+int strelka_nrc_set_params(StrelkaNrc* nrc, const float* mlp, const float* grid);
+/* Sizes and the per-level grid resolution (negative when the level is hashed). */
+int strelka_nrc_info(StrelkaNrc* nrc, uint32_t* numMlpParams, uint64_t* numGridParams, int32_t* levelRes);
+
+/* ------------------------------------------------------------------------- */
 /* Host-side scene preparation (replaces BvhBuilder, include/render/bvh.h:38-46). */
 
 /* SAH BVH over world-space triangles (3 consecutive positions per triangle),
@@ -454,5 +499,6 @@ STRELKA_STATIC_ASSERT(sizeof(Hit) == 20, "Hit size");
 STRELKA_STATIC_ASSERT(sizeof(BVHInputPosition) == 20, "BVHInputPosition size");
 STRELKA_STATIC_ASSERT(sizeof(StrelkaMaterialArgs) == 48, "StrelkaMaterialArgs size");
 STRELKA_STATIC_ASSERT(sizeof(StrelkaTexture) == 24, "StrelkaTexture size");
+STRELKA_STATIC_ASSERT(sizeof(StrelkaNrcRecord) == 64, "StrelkaNrcRecord size");
 
 #endif /* STRELKA_B200_H */

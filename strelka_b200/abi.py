@@ -192,6 +192,16 @@ class TraceDesc(C.Structure):
     ]
 
 
+class StrelkaNrcRecord(C.Structure):
+    _fields_ = [("pos", C.c_float * 3), ("dir", C.c_float * 3), ("normal", C.c_float * 3), ("roughness", C.c_float),
+                ("target", C.c_float * 3), ("slot", C.c_uint32), ("pad", C.c_uint32 * 2)]
+
+
+class StrelkaNrcConfig(C.Structure):
+    _fields_ = [("sceneMin", C.c_float * 3), ("sceneMax", C.c_float * 3), ("learningRate", C.c_float),
+                ("seed", C.c_uint32), ("log2TableSize", C.c_uint32), ("pad", C.c_uint32 * 3)]
+
+
 class StrelkaHostScene(C.Structure):
     _fields_ = [
         ("vb", C.POINTER(Vertex)), ("numVertices", C.c_uint32),
@@ -245,6 +255,14 @@ SIGNATURES = {
     "strelka_trace_execute": (C.c_int, [vp, C.POINTER(TraceDesc), vp]),
     "strelka_trace_host": (C.c_int, [vp, C.POINTER(TraceDesc), vp, vp, vp]),
     "strelka_trace_execute_noalloc": (C.c_int, [C.POINTER(TraceDesc), vp, vp]),
+    "strelka_nrc_create": (C.c_int, [C.POINTER(StrelkaNrcConfig), C.POINTER(vp)]),
+    "strelka_nrc_destroy": (C.c_int, [vp]),
+    "strelka_nrc_infer": (C.c_int, [vp, vp, C.c_uint32, vp, vp]),
+    "strelka_nrc_train": (C.c_int, [vp, vp, C.c_uint32, C.POINTER(C.c_float), vp]),
+    "strelka_nrc_gradients": (C.c_int, [vp, vp, C.c_uint32, vp, vp, C.POINTER(C.c_float), vp]),
+    "strelka_nrc_get_params": (C.c_int, [vp, vp, vp]),
+    "strelka_nrc_set_params": (C.c_int, [vp, vp, vp]),
+    "strelka_nrc_info": (C.c_int, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), vp]),
     "strelka_bvh_build": (C.c_int, [C.POINTER(BVHInputPosition), C.c_uint32, C.POINTER(C.POINTER(BVHNode)),
                                     C.POINTER(C.c_uint32)]),
     "strelka_host_free": (None, [vp]),
@@ -262,7 +280,7 @@ SIGNATURES = {
 LAYOUT_CHECK = [PathTracerParam, AccumulationParam, Tonemapparam, BVHNode, Vertex, InstanceConstants, UniformLight,
                 MdlMaterial, Mdl_resource_info, Ray, Hit, BVHInputPosition, StrelkaMaterialArgs, StrelkaTexture,
                 StrelkaEnvMap, PathTracerDesc, ReductionDesc, AccumulationDesc, TonemapDesc, TraceDesc,
-                StrelkaPathTracerConfig]
+                StrelkaPathTracerConfig, StrelkaNrcRecord, StrelkaNrcConfig]
 
 _lib = None
 

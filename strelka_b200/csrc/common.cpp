@@ -51,6 +51,8 @@ extern "C" size_t strelka_sizeof(const char* name)
     SB_SZ(TonemapDesc)
     SB_SZ(TraceDesc)
     SB_SZ(StrelkaPathTracerConfig)
+    SB_SZ(StrelkaNrcRecord)
+    SB_SZ(StrelkaNrcConfig)
 #undef SB_SZ
     return 0;
 }
