@@ -215,6 +215,143 @@ def run_traversal(args):
     print(json.dumps(line), flush=True)
 
 
+def run_nrc(args):
+    """--workload nrc: wall time of the radiance-cache renderer to reach the
+    relMSE of one plain frame (the large render at --spp samples per pixel),
+    both measured against a --ref-spp reference of the plain renderer.
+
+    The cached renderer starts from an untrained cache; its --nrc-warmup
+    training-only frames (each frame's training paths and Adam steps, no
+    image) count toward its time, and then it accumulates frames of
+    --nrc-spp samples, training on every frame, until its relMSE reaches
+    the plain frame's.  Every frame
+    is timed with CUDA events on the launching stream; relMSE is computed
+    between frames, outside the timed intervals."""
+    import torch
+
+    from strelka_b200 import abi
+    from strelka_b200.render import DeviceScene, PathTracer, RadianceCache
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    hs = make_scene(args)
+    ds = DeviceScene(hs)
+    W, H, S = args.width, args.height, args.spp
+    npx = W * H
+    stream = torch.cuda.current_stream()
+    sb = torch.empty(npx * max(S, 16, args.nrc_spp) * 3, dtype=torch.float32, device="cuda")
+
+    def render(pt, fn, spp):
+        p = hs.param(spp=spp, frameNumber=fn)
+        pt.execute(ds.desc(p, sb), npx * spp, 1, 0, stream)
+        return sb[:npx * spp * 3].view(npx, spp, 3)
+
+    def timed(pt, fn, spp, acc):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        img = render(pt, fn, spp)
+        acc += img.sum(1, dtype=torch.float64)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    plain = PathTracer(mode=abi.MODE_WAVEFRONT)
+    # reference: --ref-spp samples per pixel of the plain renderer, in 16-spp frames
+    t0 = time.perf_counter()
+    ref = torch.zeros(npx, 3, dtype=torch.float64, device="cuda")
+    ref_frames = max(1, args.ref_spp // 16)
+    for k in range(ref_frames):
+        ref += render(plain, 1_000_000 + k, 16).sum(1, dtype=torch.float64)
+    ref /= ref_frames * 16
+    torch.cuda.synchronize()
+    ref_s = time.perf_counter() - t0
+    den = ref * ref + 1e-2
+
+    def relmse(acc, n):
+        return float((((acc / n) - ref) ** 2 / den).mean())
+
+    # plain: one frame of S spp, a few independent frames
+    for k in range(3):
+        render(plain, 10 + k, S)
+    plain_ms, plain_err = [], []
+    for k in range(max(args.steps, 8)):
+        acc = torch.zeros(npx, 3, dtype=torch.float64, device="cuda")
+        plain_ms.append(timed(plain, 2000 + k, S, acc))
+        plain_err.append(relmse(acc, S))
+    target = statistics.mean(plain_err)
+    t_plain = statistics.median(plain_ms)
+    st = plain.device_status()
+    plain.close()
+
+    lo, hi = hs.bounds()
+    trials = []
+    kernel_ms = None
+    for trial in range(max(args.nrc_trials, 1)):
+        cache = RadianceCache(lo, hi, learning_rate=args.nrc_lr, seed=1 + trial, log2_table_size=args.nrc_log2t)
+        pt = PathTracer(mode=abi.MODE_WAVEFRONT, profile=True)
+        pt.set_nrc(cache, train_paths=args.nrc_train_paths, train_steps=args.nrc_train_steps,
+                   diffuse_roughness=args.nrc_diffuse_roughness)
+        pt.kernel_times(stream)
+        base = 100_000 * (trial + 1)
+        t_nrc = 0.0
+        # warm-up: training only (training paths + Adam steps), no image
+        for k in range(args.nrc_warmup):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            pt.train_nrc(ds.desc(hs.param(spp=args.nrc_spp, frameNumber=base + k), sb), base + k, stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_nrc += e0.elapsed_time(e1)
+        t_warm = t_nrc
+        acc = torch.zeros(npx, 3, dtype=torch.float64, device="cuda")
+        curve = []
+        reached = None
+        frames_ms = []
+        for k in range(args.nrc_max_frames):
+            ms = timed(pt, base + 50_000 + k, args.nrc_spp, acc)
+            frames_ms.append(ms)
+            t_nrc += ms
+            e = relmse(acc, (k + 1) * args.nrc_spp)
+            curve.append([(k + 1) * args.nrc_spp, round(e, 6), round(t_nrc, 3)])
+            if e <= target:
+                reached = (k + 1) * args.nrc_spp
+                break
+        times = pt.kernel_times(stream)
+        if kernel_ms is None:
+            kernel_ms = {k: v[0] / max(len(frames_ms), 1) for k, v in times.items() if v[1]}
+        st |= pt.device_status()
+        pt.close()
+        cache.close()
+        trials.append({"reached_at_spp": reached, "ratio": (t_nrc / t_plain) if reached else None, "ms_total": t_nrc,
+                       "ms_warmup": t_warm, "ms_per_frame": statistics.median(frames_ms),
+                       "curve_spp_relmse_ms": curve})
+    if st != 0:
+        raise RuntimeError(f"device status {st:#x}")
+    ratios = sorted(t["ratio"] if t["ratio"] is not None else float("inf") for t in trials)
+    median_ratio = ratios[len(ratios) // 2]
+    line = {
+        "metric": "radiance-cache wall time to the plain 16-spp relMSE, relative to plain",
+        "value": median_ratio if median_ratio != float("inf") else None, "unit": "x plain wall time", "n_gpus": 1,
+        "steps": args.steps, "warmup": 3, "ms_per_step": t_plain, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 render, f16 network (f32 accumulation)", "data": "synthetic",
+        "config": {"workload": f"radiance cache on the large render ({W}x{H}, depth {args.depth}, "
+                               f"{args.instances} instances)",
+                   "reference_spp": ref_frames * 16, "plain_spp": S, "plain_frames": len(plain_err),
+                   "nrc_trials": len(trials), "nrc_spp_per_frame": args.nrc_spp,
+                   "nrc_warmup_frames": args.nrc_warmup, "train_paths_per_frame": args.nrc_train_paths,
+                   "train_steps_per_frame": args.nrc_train_steps, "log2_table_size": args.nrc_log2t,
+                   "diffuse_roughness": args.nrc_diffuse_roughness, "learning_rate": args.nrc_lr,
+                   "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)"},
+        "plain": {"relmse": target, "relmse_frames": plain_err, "ms": t_plain},
+        "nrc": {"median_ratio": median_ratio, "trials": trials, "kernel_ms_per_frame_first_trial": kernel_ms},
+        "reference_seconds": ref_s,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -232,12 +369,25 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-step-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="large", choices=["large", "traversal"])
+    ap.add_argument("--workload", default="large", choices=["large", "traversal", "nrc"])
     ap.add_argument("--tris", type=int, default=1_000_000)
     ap.add_argument("--rays", type=int, default=4_000_000)
+    ap.add_argument("--ref-spp", type=int, default=16384)
+    ap.add_argument("--nrc-spp", type=int, default=2)
+    ap.add_argument("--nrc-warmup", type=int, default=16)
+    ap.add_argument("--nrc-max-frames", type=int, default=64)
+    ap.add_argument("--nrc-train-paths", type=int, default=16384)
+    ap.add_argument("--nrc-train-steps", type=int, default=1)
+    ap.add_argument("--nrc-trials", type=int, default=5)
+    ap.add_argument("--nrc-log2t", type=int, default=19)
+    ap.add_argument("--nrc-lr", type=float, default=1e-2)
+    ap.add_argument("--nrc-diffuse-roughness", type=float, default=0.25)
     args = ap.parse_args()
     if args.workload == "traversal":
         run_traversal(args)
+        return
+    if args.workload == "nrc":
+        run_nrc(args)
         return
     args.warmup = max(args.warmup, 3) if args.impl == "strelka" else args.warmup
 

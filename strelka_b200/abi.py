@@ -48,7 +48,8 @@ TRACE_ANY = 1
 TRACE_COUNT = 1 << 4
 TRACE_REFINE = 1 << 5
 
-KERNEL_CLASSES = ["generate", "extend", "shade", "shadow", "finalize", "megakernel", "prep"]
+KERNEL_CLASSES = ["generate", "extend", "shade", "shadow", "finalize", "megakernel", "prep", "nrc_paths", "nrc_train",
+                  "nrc_infer"]
 
 vp = C.c_void_p
 u8p = C.POINTER(C.c_uint8)
@@ -202,6 +203,11 @@ class StrelkaNrcConfig(C.Structure):
                 ("seed", C.c_uint32), ("log2TableSize", C.c_uint32), ("pad", C.c_uint32 * 3)]
 
 
+class StrelkaNrcRenderConfig(C.Structure):
+    _fields_ = [("enable", C.c_uint32), ("trainPaths", C.c_uint32), ("trainSteps", C.c_uint32),
+                ("diffuseRoughness", C.c_float), ("pad", C.c_uint32 * 4)]
+
+
 class StrelkaHostScene(C.Structure):
     _fields_ = [
         ("vb", C.POINTER(Vertex)), ("numVertices", C.c_uint32),
@@ -247,6 +253,8 @@ SIGNATURES = {
     "strelka_pathtracer_get_device_status": (C.c_int, [vp, vp, C.POINTER(C.c_uint32)]),
     "strelka_pathtracer_get_kernel_times": (C.c_int, [vp, vp, C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_uint32]),
     "strelka_pathtracer_get_counters": (C.c_int, [vp, vp, C.POINTER(C.c_uint64), C.c_uint32]),
+    "strelka_pathtracer_set_nrc": (C.c_int, [vp, vp, C.POINTER(StrelkaNrcRenderConfig)]),
+    "strelka_pathtracer_train_nrc": (C.c_int, [vp, C.POINTER(PathTracerDesc), C.c_uint64, vp]),
     "strelka_reduction_execute": (C.c_int, [C.POINTER(ReductionDesc), C.c_uint32, C.c_uint32, C.c_uint64, vp]),
     "strelka_accumulation_execute": (C.c_int, [C.POINTER(AccumulationDesc), C.c_uint32, C.c_uint32, C.c_uint64, vp]),
     "strelka_tonemap_execute": (C.c_int, [C.POINTER(TonemapDesc), C.c_uint32, C.c_uint32, C.c_uint64, vp]),
@@ -280,7 +288,7 @@ SIGNATURES = {
 LAYOUT_CHECK = [PathTracerParam, AccumulationParam, Tonemapparam, BVHNode, Vertex, InstanceConstants, UniformLight,
                 MdlMaterial, Mdl_resource_info, Ray, Hit, BVHInputPosition, StrelkaMaterialArgs, StrelkaTexture,
                 StrelkaEnvMap, PathTracerDesc, ReductionDesc, AccumulationDesc, TonemapDesc, TraceDesc,
-                StrelkaPathTracerConfig, StrelkaNrcRecord, StrelkaNrcConfig]
+                StrelkaPathTracerConfig, StrelkaNrcRecord, StrelkaNrcConfig, StrelkaNrcRenderConfig]
 
 _lib = None
 

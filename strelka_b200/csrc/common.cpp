@@ -53,6 +53,7 @@ extern "C" size_t strelka_sizeof(const char* name)
     SB_SZ(StrelkaPathTracerConfig)
     SB_SZ(StrelkaNrcRecord)
     SB_SZ(StrelkaNrcConfig)
+    SB_SZ(StrelkaNrcRenderConfig)
 #undef SB_SZ
     return 0;
 }

@@ -497,8 +497,9 @@ __global__ void __launch_bounds__(256) k_nrc_train(const StrelkaNrcRecord* __res
 // Adam over a parameter array (FP32 master + FP16 copy).
 __global__ void k_nrc_adam(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v, const float* __restrict__ grad,
                            __half* __restrict__ ph, size_t n, float lr, float gscale, float b1, float b2, float eps,
-                           float c1, float c2, int interleaveHalf2)
+                           float c1, float c2, const uint32_t* countPtr)
 {
+    if (countPtr) gscale = 1.0f / (kGradScale * fmaxf((float)*countPtr, 1.0f) * 3.0f);
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float gr = grad[i] * gscale;
         const float mi = b1 * m[i] + (1.0f - b1) * gr;
@@ -508,7 +509,6 @@ __global__ void k_nrc_adam(float* __restrict__ p, float* __restrict__ m, float* 
         const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
         p[i] = pi;
         ph[i] = __float2half(pi);
-        (void)interleaveHalf2;
     }
 }
 
@@ -669,7 +669,9 @@ int nrc_gradients_device(StrelkaNrc* nrc, const StrelkaNrcRecord* recs, const ui
     return STRELKA_OK;
 }
 
-int nrc_adam_device(StrelkaNrc* nrc, float batch, cudaStream_t st)
+int nrc_adam_device(StrelkaNrc* nrc, float batch, cudaStream_t st) { return nrc_adam_device_count(nrc, batch, nullptr, st); }
+
+int nrc_adam_device_count(StrelkaNrc* nrc, float batch, const uint32_t* countPtr, cudaStream_t st)
 {
     const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
     nrc->step += 1;
@@ -679,10 +681,10 @@ int nrc_adam_device(StrelkaNrc* nrc, float batch, cudaStream_t st)
     const float gscale = 1.0f / (kGradScale * std::max(batch, 1.0f) * 3.0f);
     const float lr = nrc->cfg.learningRate;
     k_nrc_adam<<<64, 256, 0, st>>>(nrc->mlp, nrc->mlpM, nrc->mlpV, nrc->mlpGrad, nrc->mlpHalf, kParams, lr, gscale, b1,
-                                   b2, eps, c1, c2, 0);
+                                   b2, eps, c1, c2, countPtr);
     k_nrc_adam<<<grid_blocks(nrc, nrc->gridN, 256), 256, 0, st>>>(nrc->grid, nrc->gridM, nrc->gridV, nrc->gridGrad,
                                                                   nrc->gridHalf, nrc->gridN, lr, gscale, b1, b2, eps, c1,
-                                                                  c2, 0);
+                                                                  c2, countPtr);
     SB_CUDA_TRY(cudaGetLastError());
     return STRELKA_OK;
 }

@@ -12,5 +12,7 @@ int nrc_infer_device(StrelkaNrc* nrc, const StrelkaNrcRecord* recs, const uint32
 // Gradients of the batch [0, *count) into the cache's gradient buffers.
 int nrc_gradients_device(StrelkaNrc* nrc, const StrelkaNrcRecord* recs, const uint32_t* count, uint32_t maxN,
                          cudaStream_t st);
-// One Adam step with the gradients of a batch of `batch` records.
+// One Adam step with the gradients of a batch of `batch` records (or of
+// *count records when count is not NULL).
 int nrc_adam_device(StrelkaNrc* nrc, float batch, cudaStream_t st);
+int nrc_adam_device_count(StrelkaNrc* nrc, float batch, const uint32_t* count, cudaStream_t st);

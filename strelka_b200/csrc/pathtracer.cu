@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "common.h"
+#include "nrc.h"
 #include "refine.cuh"
 #include "shading.cuh"
 
@@ -35,8 +36,21 @@ constexpr int kSmallBlock = 256;
 #define SB_SHADOW_MINBLOCKS 10
 #endif
 
-enum KernelClass { KC_GENERATE = 0, KC_EXTEND, KC_SHADE, KC_SHADOW, KC_FINALIZE, KC_MEGAKERNEL, KC_PREP, KC_COUNT };
-const char* kKernelNames[KC_COUNT] = {"generate", "extend", "shade", "shadow", "finalize", "megakernel", "prep"};
+enum KernelClass {
+    KC_GENERATE = 0,
+    KC_EXTEND,
+    KC_SHADE,
+    KC_SHADOW,
+    KC_FINALIZE,
+    KC_MEGAKERNEL,
+    KC_PREP,
+    KC_NRC_PATHS,
+    KC_NRC_TRAIN,
+    KC_NRC_INFER,
+    KC_COUNT
+};
+const char* kKernelNames[KC_COUNT] = {"generate",  "extend",    "shade",     "shadow",   "finalize", "megakernel",
+                                      "prep",      "nrc_paths", "nrc_train", "nrc_infer"};
 
 // ---------------------------------------------------------------------------
 // Scene preparation: the record table of traverse.cuh, per node slot.
@@ -165,8 +179,18 @@ struct Wave {
 
 __device__ __forceinline__ uint32_t pack_flags(const PathState& ps)
 {
-    return (uint32_t)ps.depth | ((uint32_t)ps.specular << 16) | ((uint32_t)ps.inside << 17);
+    return (uint32_t)ps.depth | ((uint32_t)ps.specular << 16) | ((uint32_t)ps.inside << 17) |
+           ((uint32_t)ps.nrcReady << 18);
 }
+
+// Radiance-cache queries of the wavefront (paths that end at a cache lookup).
+struct NrcWave {
+    StrelkaNrcRecord* queries;
+    uint32_t* count;
+    uint32_t capacity;
+    int enabled;
+    float diffuseRoughness;
+};
 
 __global__ void __launch_bounds__(kSmallBlock) k_generate(PathTracerParam ubo, Wave w, uint64_t first, uint32_t n)
 {
@@ -250,7 +274,8 @@ __device__ __forceinline__ uint32_t warp_push(uint32_t* counter, bool pred)
 
 // shade: one bounce of shading for every queued path; pushes surviving
 // paths to the other queue and next-event requests to the shadow queue.
-__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerParam ubo, Wave w, int qin)
+template <bool NRC>
+__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerParam ubo, Wave w, int qin, NrcWave nw)
 {
     const uint32_t count = w.counters[qin];
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
@@ -264,6 +289,11 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerPar
         ShadowReq sr;
         sr.kind = 0;
         uint32_t slot = 0;
+        bool query = false;
+        NrcShade nq;
+        nq.has = false;
+        nq.terminate = false;
+        v3 qdir = V(0.0f, 0.0f, 0.0f), qthr = V(0.0f, 0.0f, 0.0f);
         if (valid) {
             slot = q[i];
             const float4 o = w.ray_o[slot];
@@ -280,6 +310,7 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerPar
             ps.depth = (int)(fl & 0xffffu);
             ps.specular = (fl >> 16) & 1u;
             ps.inside = (fl >> 17) & 1u;
+            ps.nrcReady = (fl >> 18) & 1u;
             ps.color = xyz(c4);
             ps.rng = w.rng[slot];
             const float4 h4 = w.hit[slot];
@@ -290,7 +321,20 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerPar
             h.instId = __float_as_uint(h4.w);
             h.primId = w.hitPrim[slot];
             const bool found = h.instId != SB_INVALID;
-            cont = shade(s, ubo, ps, found, h, sr);
+            if (NRC) {
+                nq.mode = 2;
+                nq.diffuseRoughness = nw.diffuseRoughness;
+                nq.has = false;
+                nq.terminate = false;
+                cont = shade(s, ubo, ps, found, h, sr, &nq);
+                if (nq.terminate) {
+                    query = true;
+                    qdir = vneg(ps.rd);
+                    qthr = ps.throughput;
+                }
+            } else {
+                cont = shade(s, ubo, ps, found, h, sr);
+            }
             if (cont) {
                 ++ps.depth;
                 cont = ps.depth < maxDepth;
@@ -303,6 +347,21 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerPar
         }
         const uint32_t qpos = warp_push(&w.counters[qin ^ 1], cont);
         if (cont) qout[qpos] = slot;
+        if (NRC) {
+            const uint32_t qpos2 = warp_push(nw.count, query);
+            if (query && qpos2 < nw.capacity) {
+                StrelkaNrcRecord r;
+                r.pos[0] = nq.pos.x; r.pos[1] = nq.pos.y; r.pos[2] = nq.pos.z;
+                r.dir[0] = qdir.x; r.dir[1] = qdir.y; r.dir[2] = qdir.z;
+                r.normal[0] = nq.normal.x; r.normal[1] = nq.normal.y; r.normal[2] = nq.normal.z;
+                r.roughness = nq.rough;
+                r.target[0] = qthr.x; r.target[1] = qthr.y; r.target[2] = qthr.z;
+                r.slot = slot;
+                r.pad[0] = 0;
+                r.pad[1] = 0;
+                nw.queries[qpos2] = r;
+            }
+        }
         const bool hasShadow = sr.kind != 0;
         const uint32_t spos = warp_push(&w.counters[2], hasShadow);
         if (hasShadow) {
@@ -368,6 +427,80 @@ __global__ void __launch_bounds__(kSmallBlock) k_finalize(Wave w, float* __restr
         o[0] = c.x;
         o[1] = c.y;
         o[2] = c.z;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Radiance-cache training paths: short plain paths from random samples of
+// the frame (a decorrelated RNG stream); every shading vertex k becomes a
+// training record with target (C_end - C_k) / T_k, where C_k and T_k are the
+// path's colour and throughput on arrival at k and C_end its final colour.
+constexpr int kNrcMaxVerts = 16;
+constexpr int kNrcPathBlock = 32;  // few, long paths: spread them over many SMs
+
+__global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, PathTracerParam ubo, uint32_t nPaths, float diffuseRoughness,
+                                                         StrelkaNrcRecord* __restrict__ out, uint32_t* count, uint32_t capacity)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nPaths) return;
+    const uint64_t total = (uint64_t)ubo.dimension[0] * (uint64_t)ubo.dimension[1] * (uint64_t)ubo.spp;
+    const uint32_t h = jenkins_hash(i * 0x9E3779B9u ^ jenkins_hash(ubo.frameNumber ^ 0x5bd1e995u));
+    const uint64_t idx = (uint64_t)h % total;
+    PathTracerParam u = ubo;
+    u.frameNumber = ubo.frameNumber ^ 0x3c6ef372u;
+    PathState ps;
+    init_path(u, idx, ps);
+    float vrec[kNrcMaxVerts][10];
+    v3 cIn[kNrcMaxVerts], tIn[kNrcMaxVerts];
+    int nv = 0;
+    const int maxDepth = (int)ubo.maxDepth;
+    while (ps.depth < maxDepth) {
+        HitRec hit;
+        uint32_t a = 0, b = 0;
+        bool found = s.numNodes != 0 && trace_closest_rec<false>(s, ps.ro, ps.tmax, ps.rd, hit, a, b);
+        const v3 c0 = ps.color, t0 = ps.throughput, dOut = vneg(ps.rd);
+        NrcShade nq;
+        nq.mode = 1;
+        nq.diffuseRoughness = diffuseRoughness;
+        nq.has = false;
+        nq.terminate = false;
+        ShadowReq sr;
+        bool cont = shade(s, u, ps, found, hit, sr, &nq);
+        if (sr.kind != 0 && shadow_visible(s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
+        if (nq.has && nv < kNrcMaxVerts) {
+            float* r = vrec[nv];
+            r[0] = nq.pos.x; r[1] = nq.pos.y; r[2] = nq.pos.z;
+            r[3] = dOut.x; r[4] = dOut.y; r[5] = dOut.z;
+            r[6] = nq.normal.x; r[7] = nq.normal.y; r[8] = nq.normal.z;
+            r[9] = nq.rough;
+            cIn[nv] = c0;
+            tIn[nv] = t0;
+            ++nv;
+        }
+        if (!cont) break;
+        ++ps.depth;
+    }
+    for (int k = 0; k < nv; ++k) {
+        const v3 t = tIn[k];
+        if (!(t.x > 0.0f && t.y > 0.0f && t.z > 0.0f)) continue;
+        const v3 L = V((ps.color.x - cIn[k].x) / t.x, (ps.color.y - cIn[k].y) / t.y, (ps.color.z - cIn[k].z) / t.z);
+        if (!all_finite(L)) continue;
+        const uint32_t pos = atomicAdd(count, 1u);
+        if (pos >= capacity) continue;
+        StrelkaNrcRecord r;
+        for (int c = 0; c < 3; ++c) {
+            r.pos[c] = vrec[k][c];
+            r.dir[c] = vrec[k][3 + c];
+            r.normal[c] = vrec[k][6 + c];
+        }
+        r.roughness = vrec[k][9];
+        r.target[0] = fmaxf(L.x, 0.0f);
+        r.target[1] = fmaxf(L.y, 0.0f);
+        r.target[2] = fmaxf(L.z, 0.0f);
+        r.slot = 0;
+        r.pad[0] = 0;
+        r.pad[1] = 0;
+        out[pos] = r;
     }
 }
 
@@ -456,8 +589,16 @@ struct StrelkaPathTracer {
     std::vector<Rec> recs;
     std::vector<cudaEvent_t> eventPool;
     size_t eventsUsed = 0;
-    int extendGrid = 0, shadeGrid = 0, smallGrid = 0;
+    int extendGrid = 0, shadeGrid = 0, shadeGridNrc = 0, smallGrid = 0;
     unsigned long long* visitCounters = nullptr;  // 6 entries (STRELKA_PT_COUNT)
+    // radiance cache
+    StrelkaNrc* nrc = nullptr;
+    StrelkaNrcRenderConfig nrcCfg{};
+    StrelkaNrcRecord* nrcTrain = nullptr;
+    size_t nrcTrainCap = 0;
+    StrelkaNrcRecord* nrcQueries = nullptr;
+    size_t nrcQueryCap = 0;
+    uint32_t* nrcCounts = nullptr;  // [0] training records, [1] queries
 };
 
 namespace {
@@ -650,7 +791,8 @@ extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, 
     }
     cudaMemset(pt->visitCounters, 0, 8 * sizeof(unsigned long long));
     pt->extendGrid = occupancy_grid((const void*)k_extend<false>, kExtendBlock, pt->numSMs);
-    pt->shadeGrid = occupancy_grid((const void*)k_shade, kShadeBlock, pt->numSMs);
+    pt->shadeGrid = occupancy_grid((const void*)k_shade<false>, kShadeBlock, pt->numSMs);
+    pt->shadeGridNrc = occupancy_grid((const void*)k_shade<true>, kShadeBlock, pt->numSMs);
     pt->smallGrid = pt->numSMs * 8;
     *out = pt;
     return STRELKA_OK;
@@ -664,8 +806,44 @@ extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
     if (pt->srgbLut) cudaFree(pt->srgbLut);
     if (pt->status) cudaFree(pt->status);
     if (pt->visitCounters) cudaFree(pt->visitCounters);
+    if (pt->nrcTrain) cudaFree(pt->nrcTrain);
+    if (pt->nrcQueries) cudaFree(pt->nrcQueries);
+    if (pt->nrcCounts) cudaFree(pt->nrcCounts);
     for (cudaEvent_t e : pt->eventPool) cudaEventDestroy(e);
     delete pt;
+    return STRELKA_OK;
+}
+
+// Radiance-cache training for one frame: trainPaths training paths, then
+// trainSteps gradient + Adam steps on their vertices (batch size read on the
+// device).
+static int nrc_train_frame(StrelkaPathTracer* pt, const DevScene& s, const PathTracerParam& ubo, cudaStream_t st)
+{
+    if (!pt->nrcCounts) SB_CUDA_TRY(cudaMalloc(&pt->nrcCounts, 2 * sizeof(uint32_t)));
+    const uint32_t nTrain = pt->nrcCfg.trainPaths;
+    if (nTrain == 0) return STRELKA_OK;
+    const size_t trainCap =
+        (size_t)nTrain * std::min<uint32_t>(std::max<uint32_t>(ubo.maxDepth, 1u), (uint32_t)kNrcMaxVerts);
+    if (trainCap > pt->nrcTrainCap) {
+        if (pt->nrcTrain) cudaFree(pt->nrcTrain);
+        pt->nrcTrain = nullptr;
+        SB_CUDA_TRY(cudaMalloc(&pt->nrcTrain, trainCap * sizeof(StrelkaNrcRecord)));
+        pt->nrcTrainCap = trainCap;
+    }
+    {
+        Timer t(pt, KC_NRC_PATHS, st);
+        SB_CUDA_TRY(cudaMemsetAsync(pt->nrcCounts, 0, sizeof(uint32_t), st));
+        k_nrc_train_paths<<<(nTrain + kNrcPathBlock - 1) / kNrcPathBlock, kNrcPathBlock, 0, st>>>(
+            s, ubo, nTrain, pt->nrcCfg.diffuseRoughness, pt->nrcTrain, pt->nrcCounts, (uint32_t)trainCap);
+        SB_CUDA_TRY(cudaGetLastError());
+    }
+    Timer t(pt, KC_NRC_TRAIN, st);
+    for (uint32_t k = 0; k < std::max<uint32_t>(pt->nrcCfg.trainSteps, 1u); ++k) {
+        int rc = nrc_gradients_device(pt->nrc, pt->nrcTrain, pt->nrcCounts, (uint32_t)trainCap, st);
+        if (rc) return rc;
+        rc = nrc_adam_device_count(pt->nrc, 1.0f, pt->nrcCounts, st);
+        if (rc) return rc;
+    }
     return STRELKA_OK;
 }
 
@@ -695,6 +873,9 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
     if (rc) return rc;
     DevScene s = make_scene(pt, desc);
 
+    const bool useNrc = pt->nrc && pt->nrcCfg.enable;
+    if (useNrc && pt->cfg.mode == STRELKA_MODE_MEGAKERNEL)
+        return fail(STRELKA_ERR_UNSUPPORTED, "the radiance cache runs with the wavefront mode");
     if (pt->cfg.mode == STRELKA_MODE_MEGAKERNEL) {
         Timer t(pt, KC_MEGAKERNEL, st);
         const uint64_t blocks = (total + kExtendBlock - 1) / kExtendBlock;
@@ -711,8 +892,26 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
     rc = ensure_wave(pt, chunk);
     if (rc) return rc;
     const int maxDepth = (int)ubo.maxDepth;
+    NrcWave nw{};
+    if (useNrc) {
+        if (chunk > pt->nrcQueryCap) {
+            if (pt->nrcQueries) cudaFree(pt->nrcQueries);
+            pt->nrcQueries = nullptr;
+            SB_CUDA_TRY(cudaMalloc(&pt->nrcQueries, chunk * sizeof(StrelkaNrcRecord)));
+            pt->nrcQueryCap = chunk;
+        }
+        // train the cache on this frame's training paths before rendering
+        rc = nrc_train_frame(pt, s, ubo, st);
+        if (rc) return rc;
+        nw.queries = pt->nrcQueries;
+        nw.count = pt->nrcCounts + 1;
+        nw.capacity = (uint32_t)chunk;
+        nw.enabled = 1;
+        nw.diffuseRoughness = pt->nrcCfg.diffuseRoughness;
+    }
     for (uint64_t first = 0; first < total; first += chunk) {
         const uint32_t n = (uint32_t)std::min<uint64_t>(chunk, total - first);
+        if (useNrc) SB_CUDA_TRY(cudaMemsetAsync(pt->nrcCounts + 1, 0, sizeof(uint32_t), st));
         {
             Timer t(pt, KC_GENERATE, st);
             int grid = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, pt->smallGrid);
@@ -721,7 +920,8 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
         for (int depth = 0; depth < maxDepth; ++depth) {
             const int qin = depth & 1;
             const int gridE = std::min<int>((n + kExtendBlock - 1) / kExtendBlock, pt->extendGrid);
-            const int gridS = std::min<int>((n + kShadeBlock - 1) / kShadeBlock, pt->shadeGrid);
+            const int gridS =
+                std::min<int>((n + kShadeBlock - 1) / kShadeBlock, useNrc ? pt->shadeGridNrc : pt->shadeGrid);
             const bool count = (pt->cfg.flags & STRELKA_PT_COUNT) != 0;
             {
                 Timer t(pt, KC_EXTEND, st);
@@ -730,13 +930,21 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             }
             {
                 Timer t(pt, KC_SHADE, st);
-                k_shade<<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->wave, qin);
+                if (useNrc)
+                    k_shade<true><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->wave, qin, nw);
+                else
+                    k_shade<false><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->wave, qin, nw);
             }
             {
                 Timer t(pt, KC_SHADOW, st);
                 if (count) k_shadow<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, pt->visitCounters);
                 else k_shadow<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, nullptr);
             }
+        }
+        if (useNrc) {
+            Timer t(pt, KC_NRC_INFER, st);
+            rc = nrc_infer_device(pt->nrc, pt->nrcQueries, pt->nrcCounts + 1, n, nullptr, pt->wave.col, st);
+            if (rc) return rc;
         }
         {
             Timer t(pt, KC_FINALIZE, st);
@@ -745,6 +953,40 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
         }
         SB_CUDA_TRY(cudaGetLastError());
     }
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_pathtracer_train_nrc(StrelkaPathTracer* pt, const PathTracerDesc* desc, uint64_t frameIndex,
+                                            void* stream)
+{
+    (void)frameIndex;
+    if (!pt) return fail(STRELKA_ERR_INVALID_ARGUMENT, "path tracer is NULL");
+    if (!pt->nrc || !pt->nrcCfg.enable) return fail(STRELKA_ERR_INVALID_ARGUMENT, "no radiance cache attached");
+    int rc = check_scene_desc(desc);
+    if (rc) return rc;
+    const PathTracerParam& ubo = desc->constants;
+    if (ubo.dimension[0] <= 0 || ubo.dimension[1] <= 0 || ubo.spp <= 0)
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "dimension and spp must be positive");
+    if (desc->envMap) {
+        const StrelkaEnvMap* e = desc->envMap;
+        if (!e->rgba32f || !e->marginal_cdf || !e->conditional_cdf || e->width == 0 || e->height == 0)
+            return fail(STRELKA_ERR_INVALID_ARGUMENT, "incomplete environment map");
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    rc = ensure_scene(pt, desc->bvhNodes, desc->numNodes, desc->vb, desc->numVertices, desc->ib, desc->numIndices,
+                      desc->instanceConst, desc->numInstances, desc->sceneVersion, st);
+    if (rc) return rc;
+    DevScene s = make_scene(pt, desc);
+    return nrc_train_frame(pt, s, ubo, st);
+}
+
+extern "C" int strelka_pathtracer_set_nrc(StrelkaPathTracer* pt, StrelkaNrc* nrc, const StrelkaNrcRenderConfig* cfg)
+{
+    if (!pt) return fail(STRELKA_ERR_INVALID_ARGUMENT, "path tracer is NULL");
+    pt->nrc = nrc;
+    if (cfg) pt->nrcCfg = *cfg;
+    else pt->nrcCfg = StrelkaNrcRenderConfig{};
+    if (nrc && !cfg) pt->nrcCfg.enable = 0;
     return STRELKA_OK;
 }
 

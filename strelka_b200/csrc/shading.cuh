@@ -612,6 +612,19 @@ struct PathState {
     int depth;
     int specular;
     int inside;
+    int nrcReady;  // radiance cache: the path has made a diffuse-ish bounce
+};
+
+// Radiance-cache hook of shade(): mode 1 records the shading vertex (training
+// paths), mode 2 also ends the path there with a cache query once the path
+// has made a diffuse-ish bounce (a Lambert sample, or roughness >= threshold).
+struct NrcShade {
+    int mode;
+    float diffuseRoughness;
+    bool has;
+    bool terminate;
+    v3 pos, normal;
+    float rough;
 };
 
 // Deferred next-event contribution (see file comment).
@@ -640,6 +653,7 @@ __device__ __forceinline__ void init_path(const PathTracerParam& ubo, uint64_t i
     ps.depth = 0;
     ps.specular = 0;
     ps.inside = 0;
+    ps.nrcReady = 0;
 }
 
 __device__ __forceinline__ bool all_finite(v3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
@@ -669,7 +683,7 @@ __device__ __forceinline__ void apply_shadow(v3& color, v3 cd, v3 cg)
 // (pathtracerMdl.hlsl:225-401).  Returns true when the path continues (the
 // caller then increments depth and tests depth < maxDepth).
 __device__ __forceinline__ bool shade(const DevScene& s, const PathTracerParam& ubo, PathState& ps, bool found,
-                                      const HitRec& hit, ShadowReq& sr)
+                                      const HitRec& hit, ShadowReq& sr, NrcShade* nq = nullptr)
 {
     sr.kind = 0;
     if (!found) {
@@ -738,6 +752,16 @@ __device__ __forceinline__ bool shade(const DevScene& s, const PathTracerParam& 
     if (!load_material(s, __ldg(&ic->materialId), st, m)) {
         raise_status(s, STRELKA_DEV_MATERIAL_OOB);
         return false;
+    }
+    if (nq) {
+        nq->has = true;
+        nq->pos = st.position;
+        nq->normal = st.normal;
+        nq->rough = m.fn == STRELKA_FN_LAMBERT ? 1.0f : m.roughness;
+        if (nq->mode == 2 && ps.nrcReady) {
+            nq->terminate = true;
+            return false;
+        }
     }
     const float ior1 = ps.inside ? -1.0f : 1.0f;  // BSDF_USE_MATERIAL_IOR = -1
     const float ior2 = ps.inside ? 1.0f : -1.0f;
@@ -855,6 +879,7 @@ __device__ __forceinline__ bool shade(const DevScene& s, const PathTracerParam& 
     const v3 rayOriginNext = offset_ray(st.position, vscale(st.geom_normal, ps.inside ? -1.0f : 1.0f));
     ps.throughput = vmul(ps.throughput, smp.bsdf_over_pdf);
     ps.lastPdf = smp.pdf;
+    if (nq && (m.fn == STRELKA_FN_LAMBERT || m.roughness >= nq->diffuseRoughness)) ps.nrcReady = 1;
     if (ps.depth > 3) {
         float p = fmaxf(ps.throughput.x, fmaxf(ps.throughput.y, ps.throughput.z));
         if (rand01(ps.rng) > p) return false;

@@ -170,9 +170,75 @@ class PathTracer:
         keys = ["extend_inner", "extend_leaf", "shadow_inner", "shadow_leaf", "extend_rays", "shadow_rays"]
         return {k: int(out[i]) for i, k in enumerate(keys)}
 
+    def set_nrc(self, cache: "RadianceCache | None", train_paths: int = 16384, train_steps: int = 1,
+                diffuse_roughness: float = 0.25) -> None:
+        """Renders with the radiance cache (wavefront mode), or without it when
+        `cache` is None.  The cache object must outlive its use here."""
+        cfg = abi.StrelkaNrcRenderConfig(1 if cache is not None else 0, train_paths, train_steps, diffuse_roughness)
+        abi.check(self.lib.strelka_pathtracer_set_nrc(self.handle, cache.handle if cache is not None else None,
+                                                      C.byref(cfg)))
+        self._cache = cache
+
+    def train_nrc(self, desc: abi.PathTracerDesc, frame_index: int = 0, stream=None) -> None:
+        """Trains the attached cache on the frame's training paths without rendering."""
+        abi.check(self.lib.strelka_pathtracer_train_nrc(self.handle, C.byref(desc), frame_index,
+                                                        _stream_handle(stream)))
+
     def close(self) -> None:
         if self.handle:
             self.lib.strelka_pathtracer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RadianceCache:
+    """Online-trained neural radiance cache: a multi-resolution hash grid and
+    a fully fused FP16 MLP (strelka_nrc_*).  Records are StrelkaNrcRecord
+    rows (16 float32: pos, dir, normal, roughness, target rgb, slot, pad) in
+    device memory."""
+
+    def __init__(self, scene_min, scene_max, learning_rate: float = 1e-2, seed: int = 1, log2_table_size: int = 19):
+        self.lib = abi.load()
+        cfg = abi.StrelkaNrcConfig((C.c_float * 3)(*[float(v) for v in scene_min]),
+                                   (C.c_float * 3)(*[float(v) for v in scene_max]), learning_rate, seed,
+                                   log2_table_size, (C.c_uint32 * 3)())
+        h = C.c_void_p()
+        abi.check(self.lib.strelka_nrc_create(C.byref(cfg), C.byref(h)))
+        self.handle = h
+        nm = C.c_uint32()
+        ng = C.c_uint64()
+        abi.check(self.lib.strelka_nrc_info(h, C.byref(nm), C.byref(ng), None))
+        self.num_mlp_params = nm.value
+        self.num_grid_params = ng.value
+
+    def train(self, records, n: int, stream=None) -> float:
+        loss = C.c_float()
+        abi.check(self.lib.strelka_nrc_train(self.handle, ptr(records), n, C.byref(loss), _stream_handle(stream)))
+        return loss.value
+
+    def infer(self, records, n: int, out, stream=None) -> None:
+        abi.check(self.lib.strelka_nrc_infer(self.handle, ptr(records), n, ptr(out), _stream_handle(stream)))
+
+    def params(self) -> tuple[np.ndarray, np.ndarray]:
+        mlp = np.zeros(self.num_mlp_params, np.float32)
+        grid = np.zeros(self.num_grid_params, np.float32)
+        abi.check(self.lib.strelka_nrc_get_params(self.handle, mlp.ctypes.data, grid.ctypes.data))
+        return mlp, grid
+
+    def set_params(self, mlp: np.ndarray | None, grid: np.ndarray | None) -> None:
+        m = None if mlp is None else np.ascontiguousarray(mlp, np.float32)
+        g = None if grid is None else np.ascontiguousarray(grid, np.float32)
+        abi.check(self.lib.strelka_nrc_set_params(self.handle, None if m is None else m.ctypes.data,
+                                                  None if g is None else g.ctypes.data))
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.strelka_nrc_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

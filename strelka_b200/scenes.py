@@ -59,6 +59,14 @@ class HostScene:
     def num_materials(self) -> int:
         return self.materials.size // 16
 
+    def bounds(self) -> tuple[np.ndarray, np.ndarray]:
+        """World-space box of the scene: the root node of the BVH (node 0 of
+        the depth-first layout)."""
+        if self.num_nodes == 0:
+            return np.zeros(3, np.float32), np.ones(3, np.float32)
+        root = self.nodes[:32].view(np.float32)
+        return root[0:3].copy(), root[4:7].copy()
+
     def param(self, **kw) -> abi.PathTracerParam:
         """A copy of the camera parameter block with fields overridden by `kw`."""
         p = abi.PathTracerParam()
