@@ -220,11 +220,11 @@ def run_nrc(args):
     relMSE of one plain frame (the large render at --spp samples per pixel),
     both measured against a --ref-spp reference of the plain renderer.
 
-    The cached renderer starts from an untrained cache; its --nrc-warmup
-    training-only frames (each frame's training paths and Adam steps, no
-    image) count toward its time, and then it accumulates frames of
-    --nrc-spp samples, training on every frame, until its relMSE reaches
-    the plain frame's.  Every frame
+    The cached renderer starts from an untrained cache; its warm-up of
+    --nrc-warmup training batches (training paths and Adam steps, no image)
+    counts toward its time, and then it accumulates frames of --nrc-spp
+    samples, training on every frame, until its relMSE reaches the plain
+    frame's.  Every frame
     is timed with CUDA events on the launching stream; relMSE is computed
     between frames, outside the timed intervals."""
     import torch
@@ -288,20 +288,33 @@ def run_nrc(args):
     lo, hi = hs.bounds()
     trials = []
     kernel_ms = None
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    # one renderer for every trial, its buffers allocated by an untimed frame
+    # with a throwaway cache (as the plain renderer had warm-up frames)
+    pt = PathTracer(mode=abi.MODE_WAVEFRONT, profile=True)
+    scratch_cache = RadianceCache(lo, hi, learning_rate=args.nrc_lr, seed=99, log2_table_size=args.nrc_log2t)
+    pt.set_nrc(scratch_cache, train_paths=args.nrc_train_paths, train_steps=args.nrc_train_steps,
+               diffuse_roughness=args.nrc_diffuse_roughness)
+    for k in range(2):
+        render(pt, 77 + k, args.nrc_spp)
+    torch.cuda.synchronize()
     for trial in range(max(args.nrc_trials, 1)):
         cache = RadianceCache(lo, hi, learning_rate=args.nrc_lr, seed=1 + trial, log2_table_size=args.nrc_log2t)
-        pt = PathTracer(mode=abi.MODE_WAVEFRONT, profile=True)
         pt.set_nrc(cache, train_paths=args.nrc_train_paths, train_steps=args.nrc_train_steps,
                    diffuse_roughness=args.nrc_diffuse_roughness)
+        torch.cuda.synchronize()
         pt.kernel_times(stream)
         base = 100_000 * (trial + 1)
         t_nrc = 0.0
-        # warm-up: training only (training paths + Adam steps), no image
-        for k in range(args.nrc_warmup):
+        # warm-up: training only (training paths + Adam steps), no image;
+        # --nrc-warmup batches, --nrc-warmup-group of them traced per launch
+        for k in range(0, args.nrc_warmup, args.nrc_warmup_group):
+            nb = min(args.nrc_warmup_group, args.nrc_warmup - k)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            pt.train_nrc(ds.desc(hs.param(spp=args.nrc_spp, frameNumber=base + k), sb), base + k, stream)
+            pt.train_nrc(ds.desc(hs.param(spp=args.nrc_spp, frameNumber=base + k), sb), base + k, nb, stream)
             e1.record(stream)
             torch.cuda.synchronize()
             t_nrc += e0.elapsed_time(e1)
@@ -323,11 +336,14 @@ def run_nrc(args):
         if kernel_ms is None:
             kernel_ms = {k: v[0] / max(len(frames_ms), 1) for k, v in times.items() if v[1]}
         st |= pt.device_status()
-        pt.close()
+        pt.set_nrc(None)
         cache.close()
         trials.append({"reached_at_spp": reached, "ratio": (t_nrc / t_plain) if reached else None, "ms_total": t_nrc,
                        "ms_warmup": t_warm, "ms_per_frame": statistics.median(frames_ms),
                        "curve_spp_relmse_ms": curve})
+    clk = clocks.stop()
+    pt.close()
+    scratch_cache.close()
     if st != 0:
         raise RuntimeError(f"device status {st:#x}")
     ratios = sorted(t["ratio"] if t["ratio"] is not None else float("inf") for t in trials)
@@ -341,13 +357,14 @@ def run_nrc(args):
                                f"{args.instances} instances)",
                    "reference_spp": ref_frames * 16, "plain_spp": S, "plain_frames": len(plain_err),
                    "nrc_trials": len(trials), "nrc_spp_per_frame": args.nrc_spp,
-                   "nrc_warmup_frames": args.nrc_warmup, "train_paths_per_frame": args.nrc_train_paths,
+                   "nrc_warmup_batches": args.nrc_warmup, "nrc_warmup_batches_per_launch": args.nrc_warmup_group, "train_paths_per_frame": args.nrc_train_paths,
                    "train_steps_per_frame": args.nrc_train_steps, "log2_table_size": args.nrc_log2t,
                    "diffuse_roughness": args.nrc_diffuse_roughness, "learning_rate": args.nrc_lr,
                    "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)"},
         "plain": {"relmse": target, "relmse_frames": plain_err, "ms": t_plain},
         "nrc": {"median_ratio": median_ratio, "trials": trials, "kernel_ms_per_frame_first_trial": kernel_ms},
         "reference_seconds": ref_s,
+        "clocks": clk,
     }
     print(json.dumps(line), flush=True)
 
@@ -375,6 +392,7 @@ def main():
     ap.add_argument("--ref-spp", type=int, default=16384)
     ap.add_argument("--nrc-spp", type=int, default=2)
     ap.add_argument("--nrc-warmup", type=int, default=16)
+    ap.add_argument("--nrc-warmup-group", type=int, default=8)
     ap.add_argument("--nrc-max-frames", type=int, default=64)
     ap.add_argument("--nrc-train-paths", type=int, default=16384)
     ap.add_argument("--nrc-train-steps", type=int, default=1)

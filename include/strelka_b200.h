@@ -318,26 +318,29 @@ int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTracerDesc* desc
                                uint32_t w, uint32_t h, uint64_t frameIndex, void* stream);
 
 /* Radiance-cache rendering (an extension; the reference has no cache).  With
- * enable != 0, each execute first traces trainPaths short plain paths from
- * random samples of the frame and takes trainSteps Adam steps on their
- * vertices, then renders with every path ending at its first shading vertex
- * after a diffuse-ish bounce (a Lambert sample or roughness >=
- * diffuseRoughness), where the cache's prediction times the path throughput
- * is added.  Wavefront mode only.  The cache object stays owned by the
- * caller; pass NULL to detach it. */
+ * enable != 0, each execute traces trainPaths short plain paths from random
+ * samples of the frame and takes trainSteps Adam steps on their vertices (on
+ * a stream of the pass's own, concurrently with the frame's paths), and
+ * renders with every path ending at its first shading vertex after a
+ * diffuse-ish bounce (a Lambert sample or roughness >= diffuseRoughness),
+ * where the cache's prediction, taken after this frame's training, times the
+ * path throughput is added.  Wavefront mode only.  The cache object stays
+ * owned by the caller; pass NULL to detach it. */
 typedef struct StrelkaNrcRenderConfig {
     uint32_t enable;
     uint32_t trainPaths;      /* e.g. 16384 (about 2^16 training vertices) */
-    uint32_t trainSteps;      /* Adam steps per frame, >= 1 */
+    uint32_t trainSteps;      /* Adam steps per batch, >= 1 */
     float diffuseRoughness;   /* 0.25 */
     uint32_t pad[4];
 } StrelkaNrcRenderConfig;
 
 int strelka_pathtracer_set_nrc(StrelkaPathTracer* pt, StrelkaNrc* nrc, const StrelkaNrcRenderConfig* cfg);
-/* Only the training half of an execute with the cache attached: the training
- * paths of the frame described by desc (sampleBuffer unused) and the Adam
- * steps.  Warms a fresh cache up without rendering images. */
-int strelka_pathtracer_train_nrc(StrelkaPathTracer* pt, const PathTracerDesc* desc, uint64_t frameIndex, void* stream);
+/* Training without rendering: `batches` batches of trainPaths training paths
+ * of the frame described by desc (sampleBuffer unused; each batch its own
+ * random samples), traced in one launch, then trainSteps Adam steps per
+ * batch in order, on `stream`.  Warms a fresh cache up cheaply. */
+int strelka_pathtracer_train_nrc(StrelkaPathTracer* pt, const PathTracerDesc* desc, uint64_t frameIndex,
+                                 uint32_t batches, void* stream);
 
 /* Reads and clears the device status word (STRELKA_DEV_* bits); synchronises
  * the stream first. */

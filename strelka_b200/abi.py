@@ -254,7 +254,7 @@ SIGNATURES = {
     "strelka_pathtracer_get_kernel_times": (C.c_int, [vp, vp, C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_uint32]),
     "strelka_pathtracer_get_counters": (C.c_int, [vp, vp, C.POINTER(C.c_uint64), C.c_uint32]),
     "strelka_pathtracer_set_nrc": (C.c_int, [vp, vp, C.POINTER(StrelkaNrcRenderConfig)]),
-    "strelka_pathtracer_train_nrc": (C.c_int, [vp, C.POINTER(PathTracerDesc), C.c_uint64, vp]),
+    "strelka_pathtracer_train_nrc": (C.c_int, [vp, C.POINTER(PathTracerDesc), C.c_uint64, C.c_uint32, vp]),
     "strelka_reduction_execute": (C.c_int, [C.POINTER(ReductionDesc), C.c_uint32, C.c_uint32, C.c_uint64, vp]),
     "strelka_accumulation_execute": (C.c_int, [C.POINTER(AccumulationDesc), C.c_uint32, C.c_uint32, C.c_uint64, vp]),
     "strelka_tonemap_execute": (C.c_int, [C.POINTER(TonemapDesc), C.c_uint32, C.c_uint32, C.c_uint64, vp]),

@@ -177,6 +177,14 @@ struct Wave {
     uint32_t* counters;  // [0],[1] queue sizes, [2] shadow queue size
 };
 
+constexpr int kNrcMaxVerts = 16;  // training vertices recorded per path
+
+struct WaveBuf {
+    Wave w{};
+    size_t cap = 0;
+    std::vector<void*> allocs;
+};
+
 __device__ __forceinline__ uint32_t pack_flags(const PathState& ps)
 {
     return (uint32_t)ps.depth | ((uint32_t)ps.specular << 16) | ((uint32_t)ps.inside << 17) |
@@ -431,26 +439,31 @@ __global__ void __launch_bounds__(kSmallBlock) k_finalize(Wave w, float* __restr
 }
 
 // ---------------------------------------------------------------------------
-// Radiance-cache training paths: short plain paths from random samples of
-// the frame (a decorrelated RNG stream); every shading vertex k becomes a
-// training record with target (C_end - C_k) / T_k, where C_k and T_k are the
-// path's colour and throughput on arrival at k and C_end its final colour.
-constexpr int kNrcMaxVerts = 16;
-constexpr int kNrcPathBlock = 32;  // few, long paths: spread them over many SMs
+// Radiance-cache training paths: plain paths from random samples of the frame
+// (a decorrelated RNG stream per batch), one thread per path; every shading
+// vertex k becomes a training record with target (C_end - C_k) / T_k, where
+// C_k and T_k are the path's colour and throughput on arrival at k and C_end
+// its final colour.  Path i belongs to batch i / pathsPerBatch, whose records
+// are appended at out + batch * capPerBatch through count[batch].  The paths
+// are few and long, so they run in small blocks spread over many SMs.
+constexpr int kNrcPathBlock = 32;
 
-__global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, PathTracerParam ubo, uint32_t nPaths, float diffuseRoughness,
-                                                         StrelkaNrcRecord* __restrict__ out, uint32_t* count, uint32_t capacity)
+__global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, PathTracerParam ubo, uint32_t pathsPerBatch,
+                                                                   uint32_t batches, float diffuseRoughness,
+                                                                   StrelkaNrcRecord* __restrict__ out, uint32_t* count,
+                                                                   uint32_t capPerBatch)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nPaths) return;
+    if (i >= pathsPerBatch * batches) return;
+    const uint32_t batch = i / pathsPerBatch;
     const uint64_t total = (uint64_t)ubo.dimension[0] * (uint64_t)ubo.dimension[1] * (uint64_t)ubo.spp;
-    const uint32_t h = jenkins_hash(i * 0x9E3779B9u ^ jenkins_hash(ubo.frameNumber ^ 0x5bd1e995u));
-    const uint64_t idx = (uint64_t)h % total;
+    const uint32_t fseed = jenkins_hash((ubo.frameNumber + batch * 0x2545F491u) ^ 0x5bd1e995u);
+    const uint32_t h = jenkins_hash(i * 0x9E3779B9u ^ fseed);
     PathTracerParam u = ubo;
-    u.frameNumber = ubo.frameNumber ^ 0x3c6ef372u;
+    u.frameNumber = (ubo.frameNumber + batch * 0x2545F491u) ^ 0x3c6ef372u;
     PathState ps;
-    init_path(u, idx, ps);
-    float vrec[kNrcMaxVerts][10];
+    init_path(u, (uint64_t)h % total, ps);
+    float4 vrec[kNrcMaxVerts][3];
     v3 cIn[kNrcMaxVerts], tIn[kNrcMaxVerts];
     int nv = 0;
     const int maxDepth = (int)ubo.maxDepth;
@@ -468,11 +481,9 @@ __global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, P
         bool cont = shade(s, u, ps, found, hit, sr, &nq);
         if (sr.kind != 0 && shadow_visible(s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
         if (nq.has && nv < kNrcMaxVerts) {
-            float* r = vrec[nv];
-            r[0] = nq.pos.x; r[1] = nq.pos.y; r[2] = nq.pos.z;
-            r[3] = dOut.x; r[4] = dOut.y; r[5] = dOut.z;
-            r[6] = nq.normal.x; r[7] = nq.normal.y; r[8] = nq.normal.z;
-            r[9] = nq.rough;
+            vrec[nv][0] = f4(nq.pos, nq.rough);
+            vrec[nv][1] = f4(dOut, nq.normal.x);
+            vrec[nv][2] = make_float4(nq.normal.y, nq.normal.z, 0.0f, 0.0f);
             cIn[nv] = c0;
             tIn[nv] = t0;
             ++nv;
@@ -480,27 +491,26 @@ __global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, P
         if (!cont) break;
         ++ps.depth;
     }
+    StrelkaNrcRecord* dst = out + (size_t)batch * capPerBatch;
     for (int k = 0; k < nv; ++k) {
         const v3 t = tIn[k];
         if (!(t.x > 0.0f && t.y > 0.0f && t.z > 0.0f)) continue;
         const v3 L = V((ps.color.x - cIn[k].x) / t.x, (ps.color.y - cIn[k].y) / t.y, (ps.color.z - cIn[k].z) / t.z);
         if (!all_finite(L)) continue;
-        const uint32_t pos = atomicAdd(count, 1u);
-        if (pos >= capacity) continue;
+        const uint32_t pos = atomicAdd(&count[batch], 1u);
+        if (pos >= capPerBatch) continue;
         StrelkaNrcRecord r;
-        for (int c = 0; c < 3; ++c) {
-            r.pos[c] = vrec[k][c];
-            r.dir[c] = vrec[k][3 + c];
-            r.normal[c] = vrec[k][6 + c];
-        }
-        r.roughness = vrec[k][9];
+        r.pos[0] = vrec[k][0].x; r.pos[1] = vrec[k][0].y; r.pos[2] = vrec[k][0].z;
+        r.dir[0] = vrec[k][1].x; r.dir[1] = vrec[k][1].y; r.dir[2] = vrec[k][1].z;
+        r.normal[0] = vrec[k][1].w; r.normal[1] = vrec[k][2].x; r.normal[2] = vrec[k][2].y;
+        r.roughness = vrec[k][0].w;
         r.target[0] = fmaxf(L.x, 0.0f);
         r.target[1] = fmaxf(L.y, 0.0f);
         r.target[2] = fmaxf(L.z, 0.0f);
         r.slot = 0;
         r.pad[0] = 0;
         r.pad[1] = 0;
-        out[pos] = r;
+        dst[pos] = r;
     }
 }
 
@@ -580,8 +590,7 @@ struct StrelkaPathTracer {
     uint32_t* status = nullptr;
     // wavefront
     Wave wave{};
-    size_t waveCap = 0;
-    std::vector<void*> waveAllocs;
+    WaveBuf main;  // the frame's paths
     // environment descriptor copy
     StrelkaEnvMap env{};
     // profiling
@@ -598,45 +607,48 @@ struct StrelkaPathTracer {
     size_t nrcTrainCap = 0;
     StrelkaNrcRecord* nrcQueries = nullptr;
     size_t nrcQueryCap = 0;
-    uint32_t* nrcCounts = nullptr;  // [0] training records, [1] queries
+    uint32_t* nrcCounts = nullptr;  // [0] queries, [1 + b] training records of batch b
+    uint32_t nrcCountCap = 0;       // training batches the counters hold
+    cudaStream_t side = nullptr;    // training runs here, beside the frame
+    cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
 };
 
 namespace {
 
-void free_wave(StrelkaPathTracer* pt)
+void free_wave(WaveBuf& b)
 {
-    for (void* p : pt->waveAllocs) cudaFree(p);
-    pt->waveAllocs.clear();
-    pt->wave = Wave{};
-    pt->waveCap = 0;
+    for (void* p : b.allocs) cudaFree(p);
+    b.allocs.clear();
+    b.w = Wave{};
+    b.cap = 0;
 }
 
 template <typename T>
-int walloc(StrelkaPathTracer* pt, T** p, size_t n)
+int walloc(WaveBuf& b, T** p, size_t n)
 {
     void* q = nullptr;
     cudaError_t e = cudaMalloc(&q, n * sizeof(T));
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(wavefront state)");
-    pt->waveAllocs.push_back(q);
+    b.allocs.push_back(q);
     *p = static_cast<T*>(q);
     return STRELKA_OK;
 }
 
-int ensure_wave(StrelkaPathTracer* pt, size_t cap)
+int ensure_wave(WaveBuf& b, size_t cap)
 {
-    if (pt->waveCap >= cap) return STRELKA_OK;
-    free_wave(pt);
-    Wave& w = pt->wave;
+    if (b.cap >= cap) return STRELKA_OK;
+    free_wave(b);
+    Wave& w = b.w;
     int rc;
-    if ((rc = walloc(pt, &w.ray_o, cap)) || (rc = walloc(pt, &w.ray_d, cap)) || (rc = walloc(pt, &w.thr, cap)) ||
-        (rc = walloc(pt, &w.col, cap)) || (rc = walloc(pt, &w.rng, cap)) || (rc = walloc(pt, &w.hit, cap)) ||
-        (rc = walloc(pt, &w.hitPrim, cap)) || (rc = walloc(pt, &w.queue[0], cap)) || (rc = walloc(pt, &w.queue[1], cap)) ||
-        (rc = walloc(pt, &w.sh_o, cap)) || (rc = walloc(pt, &w.sh_d, cap)) || (rc = walloc(pt, &w.sh_cd, cap)) ||
-        (rc = walloc(pt, &w.sh_cg, cap)) || (rc = walloc(pt, &w.counters, 4))) {
-        free_wave(pt);
+    if ((rc = walloc(b, &w.ray_o, cap)) || (rc = walloc(b, &w.ray_d, cap)) || (rc = walloc(b, &w.thr, cap)) ||
+        (rc = walloc(b, &w.col, cap)) || (rc = walloc(b, &w.rng, cap)) || (rc = walloc(b, &w.hit, cap)) ||
+        (rc = walloc(b, &w.hitPrim, cap)) || (rc = walloc(b, &w.queue[0], cap)) || (rc = walloc(b, &w.queue[1], cap)) ||
+        (rc = walloc(b, &w.sh_o, cap)) || (rc = walloc(b, &w.sh_d, cap)) || (rc = walloc(b, &w.sh_cd, cap)) ||
+        (rc = walloc(b, &w.sh_cg, cap)) || (rc = walloc(b, &w.counters, 4))) {
+        free_wave(b);
         return rc;
     }
-    pt->waveCap = cap;
+    b.cap = cap;
     return STRELKA_OK;
 }
 
@@ -801,7 +813,7 @@ extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, 
 extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
 {
     if (!pt) return STRELKA_OK;
-    free_wave(pt);
+    free_wave(pt->main);
     if (pt->rec) cudaFree(pt->rec);
     if (pt->srgbLut) cudaFree(pt->srgbLut);
     if (pt->status) cudaFree(pt->status);
@@ -809,40 +821,59 @@ extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
     if (pt->nrcTrain) cudaFree(pt->nrcTrain);
     if (pt->nrcQueries) cudaFree(pt->nrcQueries);
     if (pt->nrcCounts) cudaFree(pt->nrcCounts);
+    if (pt->forkEvent) cudaEventDestroy(pt->forkEvent);
+    if (pt->joinEvent) cudaEventDestroy(pt->joinEvent);
+    if (pt->side) cudaStreamDestroy(pt->side);
     for (cudaEvent_t e : pt->eventPool) cudaEventDestroy(e);
     delete pt;
     return STRELKA_OK;
 }
 
-// Radiance-cache training for one frame: trainPaths training paths, then
-// trainSteps gradient + Adam steps on their vertices (batch size read on the
-// device).
-static int nrc_train_frame(StrelkaPathTracer* pt, const DevScene& s, const PathTracerParam& ubo, cudaStream_t st)
+// Radiance-cache training: `batches` batches of trainPaths training paths,
+// traced in one launch, then per batch trainSteps gradient + Adam steps on
+// its vertices (batch sizes read on the device).
+static int nrc_train_frame(StrelkaPathTracer* pt, const DevScene& s, const PathTracerParam& ubo, uint32_t batches,
+                           cudaStream_t st)
 {
-    if (!pt->nrcCounts) SB_CUDA_TRY(cudaMalloc(&pt->nrcCounts, 2 * sizeof(uint32_t)));
     const uint32_t nTrain = pt->nrcCfg.trainPaths;
-    if (nTrain == 0) return STRELKA_OK;
-    const size_t trainCap =
+    if (nTrain == 0 || batches == 0) return STRELKA_OK;
+    if ((uint64_t)nTrain * batches > (1ull << 26))
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "trainPaths x batches exceeds 2^26");
+    if (batches + 1 > pt->nrcCountCap) {
+        if (pt->nrcCounts) cudaFree(pt->nrcCounts);
+        pt->nrcCounts = nullptr;
+        pt->nrcCountCap = 0;
+        SB_CUDA_TRY(cudaMalloc(&pt->nrcCounts, (size_t)(batches + 1) * sizeof(uint32_t)));
+        pt->nrcCountCap = batches + 1;
+    }
+    const size_t capPerBatch =
         (size_t)nTrain * std::min<uint32_t>(std::max<uint32_t>(ubo.maxDepth, 1u), (uint32_t)kNrcMaxVerts);
-    if (trainCap > pt->nrcTrainCap) {
+    if (capPerBatch * batches > pt->nrcTrainCap) {
         if (pt->nrcTrain) cudaFree(pt->nrcTrain);
         pt->nrcTrain = nullptr;
-        SB_CUDA_TRY(cudaMalloc(&pt->nrcTrain, trainCap * sizeof(StrelkaNrcRecord)));
-        pt->nrcTrainCap = trainCap;
+        pt->nrcTrainCap = 0;
+        SB_CUDA_TRY(cudaMalloc(&pt->nrcTrain, capPerBatch * batches * sizeof(StrelkaNrcRecord)));
+        pt->nrcTrainCap = capPerBatch * batches;
     }
     {
         Timer t(pt, KC_NRC_PATHS, st);
-        SB_CUDA_TRY(cudaMemsetAsync(pt->nrcCounts, 0, sizeof(uint32_t), st));
-        k_nrc_train_paths<<<(nTrain + kNrcPathBlock - 1) / kNrcPathBlock, kNrcPathBlock, 0, st>>>(
-            s, ubo, nTrain, pt->nrcCfg.diffuseRoughness, pt->nrcTrain, pt->nrcCounts, (uint32_t)trainCap);
+        SB_CUDA_TRY(cudaMemsetAsync(pt->nrcCounts + 1, 0, batches * sizeof(uint32_t), st));
+        const uint32_t n = nTrain * batches;
+        k_nrc_train_paths<<<(n + kNrcPathBlock - 1) / kNrcPathBlock, kNrcPathBlock, 0, st>>>(
+            s, ubo, nTrain, batches, pt->nrcCfg.diffuseRoughness, pt->nrcTrain, pt->nrcCounts + 1,
+            (uint32_t)capPerBatch);
         SB_CUDA_TRY(cudaGetLastError());
     }
     Timer t(pt, KC_NRC_TRAIN, st);
-    for (uint32_t k = 0; k < std::max<uint32_t>(pt->nrcCfg.trainSteps, 1u); ++k) {
-        int rc = nrc_gradients_device(pt->nrc, pt->nrcTrain, pt->nrcCounts, (uint32_t)trainCap, st);
-        if (rc) return rc;
-        rc = nrc_adam_device_count(pt->nrc, 1.0f, pt->nrcCounts, st);
-        if (rc) return rc;
+    for (uint32_t b = 0; b < batches; ++b) {
+        const StrelkaNrcRecord* recs = pt->nrcTrain + (size_t)b * capPerBatch;
+        const uint32_t* cnt = pt->nrcCounts + 1 + b;
+        for (uint32_t k = 0; k < std::max<uint32_t>(pt->nrcCfg.trainSteps, 1u); ++k) {
+            int rc = nrc_gradients_device(pt->nrc, recs, cnt, (uint32_t)capPerBatch, st);
+            if (rc) return rc;
+            rc = nrc_adam_device_count(pt->nrc, 1.0f, cnt, st);
+            if (rc) return rc;
+        }
     }
     return STRELKA_OK;
 }
@@ -889,7 +920,7 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
     // 1080p x 16 spp frame is 33.2M paths, 5.3 GB)
     size_t chunk = pt->cfg.chunkPaths ? pt->cfg.chunkPaths : (size_t)1 << 25;
     chunk = std::min<size_t>(chunk, total);
-    rc = ensure_wave(pt, chunk);
+    rc = ensure_wave(pt->main, chunk);
     if (rc) return rc;
     const int maxDepth = (int)ubo.maxDepth;
     NrcWave nw{};
@@ -900,22 +931,35 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             SB_CUDA_TRY(cudaMalloc(&pt->nrcQueries, chunk * sizeof(StrelkaNrcRecord)));
             pt->nrcQueryCap = chunk;
         }
-        // train the cache on this frame's training paths before rendering
-        rc = nrc_train_frame(pt, s, ubo, st);
+        if (!pt->nrcCounts) {
+            SB_CUDA_TRY(cudaMalloc(&pt->nrcCounts, 2 * sizeof(uint32_t)));
+            pt->nrcCountCap = 2;
+        }
+        if (!pt->side) {
+            SB_CUDA_TRY(cudaStreamCreateWithFlags(&pt->side, cudaStreamNonBlocking));
+            SB_CUDA_TRY(cudaEventCreateWithFlags(&pt->forkEvent, cudaEventDisableTiming));
+            SB_CUDA_TRY(cudaEventCreateWithFlags(&pt->joinEvent, cudaEventDisableTiming));
+        }
+        // this frame's training runs on the side stream while the frame's
+        // paths are traced; the frame waits for it before the cache inference
+        SB_CUDA_TRY(cudaEventRecord(pt->forkEvent, st));
+        SB_CUDA_TRY(cudaStreamWaitEvent(pt->side, pt->forkEvent, 0));
+        rc = nrc_train_frame(pt, s, ubo, 1, pt->side);
         if (rc) return rc;
+        SB_CUDA_TRY(cudaEventRecord(pt->joinEvent, pt->side));
         nw.queries = pt->nrcQueries;
-        nw.count = pt->nrcCounts + 1;
+        nw.count = pt->nrcCounts;
         nw.capacity = (uint32_t)chunk;
         nw.enabled = 1;
         nw.diffuseRoughness = pt->nrcCfg.diffuseRoughness;
     }
     for (uint64_t first = 0; first < total; first += chunk) {
         const uint32_t n = (uint32_t)std::min<uint64_t>(chunk, total - first);
-        if (useNrc) SB_CUDA_TRY(cudaMemsetAsync(pt->nrcCounts + 1, 0, sizeof(uint32_t), st));
+        if (useNrc) SB_CUDA_TRY(cudaMemsetAsync(pt->nrcCounts, 0, sizeof(uint32_t), st));
         {
             Timer t(pt, KC_GENERATE, st);
             int grid = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, pt->smallGrid);
-            k_generate<<<grid, kSmallBlock, 0, st>>>(ubo, pt->wave, first, n);
+            k_generate<<<grid, kSmallBlock, 0, st>>>(ubo, pt->main.w, first, n);
         }
         for (int depth = 0; depth < maxDepth; ++depth) {
             const int qin = depth & 1;
@@ -925,31 +969,32 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             const bool count = (pt->cfg.flags & STRELKA_PT_COUNT) != 0;
             {
                 Timer t(pt, KC_EXTEND, st);
-                if (count) k_extend<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, qin, pt->visitCounters);
-                else k_extend<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, qin, nullptr);
+                if (count) k_extend<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, pt->visitCounters);
+                else k_extend<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, nullptr);
             }
             {
                 Timer t(pt, KC_SHADE, st);
                 if (useNrc)
-                    k_shade<true><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->wave, qin, nw);
+                    k_shade<true><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->main.w, qin, nw);
                 else
-                    k_shade<false><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->wave, qin, nw);
+                    k_shade<false><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->main.w, qin, nw);
             }
             {
                 Timer t(pt, KC_SHADOW, st);
-                if (count) k_shadow<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, pt->visitCounters);
-                else k_shadow<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->wave, nullptr);
+                if (count) k_shadow<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, pt->visitCounters);
+                else k_shadow<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, nullptr);
             }
         }
         if (useNrc) {
+            if (first == 0) SB_CUDA_TRY(cudaStreamWaitEvent(st, pt->joinEvent, 0));
             Timer t(pt, KC_NRC_INFER, st);
-            rc = nrc_infer_device(pt->nrc, pt->nrcQueries, pt->nrcCounts + 1, n, nullptr, pt->wave.col, st);
+            rc = nrc_infer_device(pt->nrc, pt->nrcQueries, pt->nrcCounts, n, nullptr, pt->main.w.col, st);
             if (rc) return rc;
         }
         {
             Timer t(pt, KC_FINALIZE, st);
             int grid = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, pt->smallGrid);
-            k_finalize<<<grid, kSmallBlock, 0, st>>>(pt->wave, desc->sampleBuffer, first, n);
+            k_finalize<<<grid, kSmallBlock, 0, st>>>(pt->main.w, desc->sampleBuffer, first, n);
         }
         SB_CUDA_TRY(cudaGetLastError());
     }
@@ -957,7 +1002,7 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
 }
 
 extern "C" int strelka_pathtracer_train_nrc(StrelkaPathTracer* pt, const PathTracerDesc* desc, uint64_t frameIndex,
-                                            void* stream)
+                                            uint32_t batches, void* stream)
 {
     (void)frameIndex;
     if (!pt) return fail(STRELKA_ERR_INVALID_ARGUMENT, "path tracer is NULL");
@@ -977,7 +1022,7 @@ extern "C" int strelka_pathtracer_train_nrc(StrelkaPathTracer* pt, const PathTra
                       desc->instanceConst, desc->numInstances, desc->sceneVersion, st);
     if (rc) return rc;
     DevScene s = make_scene(pt, desc);
-    return nrc_train_frame(pt, s, ubo, st);
+    return nrc_train_frame(pt, s, ubo, batches, st);
 }
 
 extern "C" int strelka_pathtracer_set_nrc(StrelkaPathTracer* pt, StrelkaNrc* nrc, const StrelkaNrcRenderConfig* cfg)

@@ -179,9 +179,10 @@ class PathTracer:
                                                       C.byref(cfg)))
         self._cache = cache
 
-    def train_nrc(self, desc: abi.PathTracerDesc, frame_index: int = 0, stream=None) -> None:
-        """Trains the attached cache on the frame's training paths without rendering."""
-        abi.check(self.lib.strelka_pathtracer_train_nrc(self.handle, C.byref(desc), frame_index,
+    def train_nrc(self, desc: abi.PathTracerDesc, frame_index: int = 0, batches: int = 1, stream=None) -> None:
+        """Trains the attached cache on `batches` batches of the frame's
+        training paths (one Adam step group per batch) without rendering."""
+        abi.check(self.lib.strelka_pathtracer_train_nrc(self.handle, C.byref(desc), frame_index, batches,
                                                         _stream_handle(stream)))
 
     def close(self) -> None:
