@@ -215,6 +215,63 @@ def run_traversal(args):
     print(json.dumps(line), flush=True)
 
 
+def nrc_mlp_microbench(torch, RadianceCache, lo, hi, log2t, peak_tflops):
+    """Throughput of the cache's fused kernels on resident random records:
+    inference over 2^22 queries and one training step (forward + backward
+    + Adam) over 2^16 records.  Forward FLOPs per query: 2 x (4 x 64 x 64 +
+    16 x 64) = 34,816; a training record costs the forward pass plus about
+    twice that backward (input and weight gradients)."""
+    rng = np.random.default_rng(0)
+
+    def records(n):
+        r = np.zeros((n, 16), np.float32)
+        r[:, 0:3] = rng.uniform(lo, hi, (n, 3))
+        d = rng.normal(size=(n, 3))
+        r[:, 3:6] = d / np.linalg.norm(d, axis=1, keepdims=True)
+        nn = rng.normal(size=(n, 3))
+        r[:, 6:9] = nn / np.linalg.norm(nn, axis=1, keepdims=True)
+        r[:, 9] = rng.uniform(0.05, 1.0, n)
+        r[:, 10:13] = rng.gamma(1.0, 1.0, (n, 3))
+        return torch.from_numpy(r).cuda()
+
+    cache = RadianceCache(lo, hi, seed=5, log2_table_size=log2t)
+    out = {}
+    n = 1 << 22
+    recs = records(n)
+    y = torch.empty(n * 3, dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        cache.infer(recs, n, y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        cache.infer(recs, n, y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 10
+    fl = 34816.0 * n
+    out["infer"] = {"queries": n, "ms": ms, "gqueries_s": n / ms / 1e6, "tflops": fl / ms / 1e9,
+                    "frac_of_sustained_peak": fl / ms / 1e9 / peak_tflops}
+    n = 1 << 16
+    recs = records(n)
+    for _ in range(3):
+        cache.train(recs, n)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record()
+    for _ in range(20):
+        cache.train(recs, n)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 20
+    fl = 3 * 34816.0 * n
+    out["train_step"] = {"records": n, "ms": ms, "tflops_mlp": fl / ms / 1e9,
+                         "note": "includes the loss read-back to the host, the gradient clears and dense Adam "
+                                 "over all hash-grid parameters"}
+    cache.close()
+    return out
+
+
 def run_nrc(args):
     """--workload nrc: wall time of the radiance-cache renderer to reach the
     relMSE of one plain frame (the large render at --spp samples per pixel),
@@ -344,6 +401,9 @@ def run_nrc(args):
     clk = clocks.stop()
     pt.close()
     scratch_cache.close()
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak_tf = json.load(open(peaks_path)).get("bf16_tflops_sustained", 1400.0) if os.path.exists(peaks_path) else 1400.0
+    mlp = nrc_mlp_microbench(torch, RadianceCache, lo, hi, args.nrc_log2t, peak_tf)
     if st != 0:
         raise RuntimeError(f"device status {st:#x}")
     ratios = sorted(t["ratio"] if t["ratio"] is not None else float("inf") for t in trials)
@@ -365,6 +425,7 @@ def run_nrc(args):
         "nrc": {"median_ratio": median_ratio, "trials": trials, "kernel_ms_per_frame_first_trial": kernel_ms},
         "reference_seconds": ref_s,
         "clocks": clk,
+        "mlp_microbench": mlp,
     }
     print(json.dumps(line), flush=True)
 
