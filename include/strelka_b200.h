@@ -472,6 +472,67 @@ int strelka_nrc_set_params(StrelkaNrc* nrc, const float* mlp, const float* grid)
 int strelka_nrc_info(StrelkaNrc* nrc, uint32_t* numMlpParams, uint64_t* numGridParams, int32_t* levelRes);
 
 /* ------------------------------------------------------------------------- */
+/* Batched rendering (an extension; the reference renders one view per
+ * PathTracer::execute, src/render/pathtracer.cpp:50-59).  Many scene/camera
+ * jobs of uneven resolution, sample count, depth and triangle count are
+ * rendered by one launch sequence captured once into a CUDA graph.  Each job
+ * is a full PathTracerDesc with its own constants (dimension, spp, maxDepth,
+ * frameNumber, camera) and its own sampleBuffer of W*H*spp*3 floats; its
+ * samples are bit-identical to PathTracer::execute on the same descriptor. */
+#define STRELKA_BATCH_MAX_JOBS 64
+
+typedef struct StrelkaBatch StrelkaBatch;
+
+enum {
+    STRELKA_BATCH_PERSISTENT = 0, /* one persistent kernel tracing whole paths, fed by an atomic path queue */
+    STRELKA_BATCH_WAVEFRONT = 1   /* job-aware wavefront kernels fed by atomic queues */
+};
+
+typedef struct StrelkaBatchConfig {
+    uint32_t mode;          /* STRELKA_BATCH_* */
+    uint32_t blockSize;     /* 64, 128 or 256 threads */
+    uint32_t queueChunk;    /* queue items a warp takes at a time: a multiple of 32 in [32, 4096] */
+    uint32_t materialSort;  /* wavefront: sort each bounce's shade queue by (job, material) */
+    uint32_t useGraph;      /* 1: capture the launch sequence once and replay it with one cudaGraphLaunch */
+    uint32_t pad[3];
+} StrelkaBatchConfig;
+
+typedef struct StrelkaBatchTuneEntry {
+    StrelkaBatchConfig config;
+    float ms;               /* median batch time over the repeats (CUDA events) */
+    uint32_t pad[3];
+} StrelkaBatchTuneEntry;
+
+int strelka_batch_create(StrelkaBatch** out);
+int strelka_batch_destroy(StrelkaBatch* batch);
+/* Copies the job descriptors (at most STRELKA_BATCH_MAX_JOBS, at most 2^31
+ * paths in all) and prepares each distinct scene's traversal records on
+ * `stream`.  Device buffers stay owned by the caller.  Drops captured graphs
+ * and the tuned configuration. */
+int strelka_batch_set_jobs(StrelkaBatch* batch, const PathTracerDesc* jobs, uint32_t numJobs, void* stream);
+/* Sets every job's frameNumber to its descriptor's value + frameOffset
+ * (synchronises the stream; captured graphs stay valid). */
+int strelka_batch_set_frame(StrelkaBatch* batch, uint32_t frameOffset, void* stream);
+/* Renders every job once.  config NULL: the tuned configuration when
+ * strelka_batch_autotune has run, else wavefront / 128 / 256 / no sort /
+ * graph. */
+int strelka_batch_execute(StrelkaBatch* batch, const StrelkaBatchConfig* config, void* stream);
+/* Coordinate-descent search over mode, block size {64,128,256}, queue chunk
+ * {32..1024} and material sort, each candidate timed as the median of
+ * `repeats` executions after one warm-up; keeps the fastest as the default
+ * of strelka_batch_execute.  entries (may be NULL) receives every timed
+ * candidate, *numEntries their count. */
+int strelka_batch_autotune(StrelkaBatch* batch, uint32_t repeats, StrelkaBatchTuneEntry* entries, uint32_t capacity,
+                           uint32_t* numEntries, StrelkaBatchConfig* best, void* stream);
+/* Per-job latency of the last execution: ms from the batch's start to the
+ * job's last sample (device timer); synchronises the stream.  Returns the
+ * number of jobs. */
+int strelka_batch_job_latency(StrelkaBatch* batch, void* stream, float* ms, uint32_t capacity);
+/* Reads and clears the batch's device status word (STRELKA_DEV_* bits). */
+int strelka_batch_get_device_status(StrelkaBatch* batch, void* stream, uint32_t* status);
+int strelka_batch_info(StrelkaBatch* batch, uint64_t* totalPaths, uint32_t* numJobs, uint32_t* numSortKeys);
+
+/* ------------------------------------------------------------------------- */
 /* Host-side scene preparation (replaces BvhBuilder, include/render/bvh.h:38-46). */
 
 /* SAH BVH over world-space triangles (3 consecutive positions per triangle),

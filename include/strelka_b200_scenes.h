@@ -94,6 +94,13 @@ int strelka_envmap_build_cdf_host(const float* rgba32f, uint32_t width, uint32_t
 
 void strelka_scene_free(StrelkaHostScene* scene);
 
+/* Replaces the camera of a parameter block by a pinhole at `eye` looking at
+ * `target` (y up) with a vertical field of view of fovDeg, rendering
+ * width x height: the matrices Camera builds (src/scene/camera.cpp:61-131,
+ * reverse Z) and the dimension fields; every other field is kept. */
+int strelka_camera_lookat(PathTracerParam* param, uint32_t width, uint32_t height, const float eye[3],
+                          const float target[3], float fovDeg);
+
 #ifdef __cplusplus
 }
 #endif

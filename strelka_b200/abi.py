@@ -38,6 +38,9 @@ FN_LAMBERT = 0
 FN_GGX_CONDUCTOR = 1
 FN_GGX_DIELECTRIC = 2
 
+BATCH_PERSISTENT = 0
+BATCH_WAVEFRONT = 1
+BATCH_MAX_JOBS = 64
 MODE_WAVEFRONT = 0
 MODE_MEGAKERNEL = 1
 PT_PROFILE = 1
@@ -208,6 +211,15 @@ class StrelkaNrcRenderConfig(C.Structure):
                 ("diffuseRoughness", C.c_float), ("pad", C.c_uint32 * 4)]
 
 
+class StrelkaBatchConfig(C.Structure):
+    _fields_ = [("mode", C.c_uint32), ("blockSize", C.c_uint32), ("queueChunk", C.c_uint32),
+                ("materialSort", C.c_uint32), ("useGraph", C.c_uint32), ("pad", C.c_uint32 * 3)]
+
+
+class StrelkaBatchTuneEntry(C.Structure):
+    _fields_ = [("config", StrelkaBatchConfig), ("ms", C.c_float), ("pad", C.c_uint32 * 3)]
+
+
 class StrelkaHostScene(C.Structure):
     _fields_ = [
         ("vb", C.POINTER(Vertex)), ("numVertices", C.c_uint32),
@@ -271,6 +283,18 @@ SIGNATURES = {
     "strelka_nrc_get_params": (C.c_int, [vp, vp, vp]),
     "strelka_nrc_set_params": (C.c_int, [vp, vp, vp]),
     "strelka_nrc_info": (C.c_int, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), vp]),
+    "strelka_batch_create": (C.c_int, [C.POINTER(vp)]),
+    "strelka_batch_destroy": (C.c_int, [vp]),
+    "strelka_batch_set_jobs": (C.c_int, [vp, vp, C.c_uint32, vp]),
+    "strelka_batch_set_frame": (C.c_int, [vp, C.c_uint32, vp]),
+    "strelka_batch_execute": (C.c_int, [vp, C.POINTER(StrelkaBatchConfig), vp]),
+    "strelka_batch_autotune": (C.c_int, [vp, C.c_uint32, C.POINTER(StrelkaBatchTuneEntry), C.c_uint32,
+                                         C.POINTER(C.c_uint32), C.POINTER(StrelkaBatchConfig), vp]),
+    "strelka_batch_job_latency": (C.c_int, [vp, vp, C.POINTER(C.c_float), C.c_uint32]),
+    "strelka_batch_get_device_status": (C.c_int, [vp, vp, C.POINTER(C.c_uint32)]),
+    "strelka_batch_info": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "strelka_camera_lookat": (C.c_int, [C.POINTER(PathTracerParam), C.c_uint32, C.c_uint32, C.POINTER(C.c_float),
+                                        C.POINTER(C.c_float), C.c_float]),
     "strelka_bvh_build": (C.c_int, [C.POINTER(BVHInputPosition), C.c_uint32, C.POINTER(C.POINTER(BVHNode)),
                                     C.POINTER(C.c_uint32)]),
     "strelka_host_free": (None, [vp]),
@@ -288,7 +312,8 @@ SIGNATURES = {
 LAYOUT_CHECK = [PathTracerParam, AccumulationParam, Tonemapparam, BVHNode, Vertex, InstanceConstants, UniformLight,
                 MdlMaterial, Mdl_resource_info, Ray, Hit, BVHInputPosition, StrelkaMaterialArgs, StrelkaTexture,
                 StrelkaEnvMap, PathTracerDesc, ReductionDesc, AccumulationDesc, TonemapDesc, TraceDesc,
-                StrelkaPathTracerConfig, StrelkaNrcRecord, StrelkaNrcConfig, StrelkaNrcRenderConfig]
+                StrelkaPathTracerConfig, StrelkaNrcRecord, StrelkaNrcConfig, StrelkaNrcRenderConfig,
+                StrelkaBatchConfig, StrelkaBatchTuneEntry]
 
 _lib = None
 

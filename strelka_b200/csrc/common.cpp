@@ -54,6 +54,8 @@ extern "C" size_t strelka_sizeof(const char* name)
     SB_SZ(StrelkaNrcRecord)
     SB_SZ(StrelkaNrcConfig)
     SB_SZ(StrelkaNrcRenderConfig)
+    SB_SZ(StrelkaBatchConfig)
+    SB_SZ(StrelkaBatchTuneEntry)
 #undef SB_SZ
     return 0;
 }

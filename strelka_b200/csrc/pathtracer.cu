@@ -18,7 +18,9 @@
 #include "common.h"
 #include "nrc.h"
 #include "refine.cuh"
+#include "internal.h"
 #include "shading.cuh"
+#include "wave.cuh"
 
 using namespace sb;
 
@@ -159,24 +161,6 @@ __global__ void __launch_bounds__(kExtendBlock) k_megakernel(DevScene s, PathTra
     sampleBuffer[idx * 3 + 2] = ps.color.z;
 }
 
-// ---------------------------------------------------------------------------
-// Wavefront state (structure of arrays, one slot per path of the chunk).
-struct Wave {
-    float4* ray_o;   // origin, tmax
-    float4* ray_d;   // direction, last BSDF pdf
-    float4* thr;     // throughput, flags (depth | specular << 16 | inside << 17)
-    float4* col;     // color
-    uint32_t* rng;
-    float4* hit;     // u, v, t, instId (SB_INVALID = miss)
-    uint32_t* hitPrim;
-    uint32_t* queue[2];
-    float4* sh_o;    // origin, tmax
-    float4* sh_d;    // direction, slot
-    float4* sh_cd;   // diffuse contribution, kind
-    float4* sh_cg;   // glossy contribution
-    uint32_t* counters;  // [0],[1] queue sizes, [2] shadow queue size
-};
-
 constexpr int kNrcMaxVerts = 16;  // training vertices recorded per path
 
 struct WaveBuf {
@@ -184,12 +168,6 @@ struct WaveBuf {
     size_t cap = 0;
     std::vector<void*> allocs;
 };
-
-__device__ __forceinline__ uint32_t pack_flags(const PathState& ps)
-{
-    return (uint32_t)ps.depth | ((uint32_t)ps.specular << 16) | ((uint32_t)ps.inside << 17) |
-           ((uint32_t)ps.nrcReady << 18);
-}
 
 // Radiance-cache queries of the wavefront (paths that end at a cache lookup).
 struct NrcWave {
@@ -265,19 +243,6 @@ __global__ void __launch_bounds__(kExtendBlock) k_extend(DevScene s, Wave w, int
         atomicAdd(&visitCounters[1], (unsigned long long)nL);
         atomicAdd(&visitCounters[4], (unsigned long long)nR);
     }
-}
-
-__device__ __forceinline__ uint32_t warp_push(uint32_t* counter, bool pred)
-{
-    const unsigned mask = __ballot_sync(0xffffffffu, pred);
-    const int lane = threadIdx.x & 31;
-    uint32_t base = 0;
-    if (mask != 0) {
-        const int leader = __ffs(mask) - 1;
-        if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
-        base = __shfl_sync(0xffffffffu, base, leader);
-    }
-    return base + __popc(mask & ((1u << lane) - 1u));
 }
 
 // shade: one bounce of shading for every queued path; pushes surviving
@@ -686,14 +651,6 @@ struct Timer {
     }
 };
 
-void srgb_lut_host(float* lut)
-{
-    for (int i = 0; i < 256; ++i) {
-        float x = (float)i / 255.0f;
-        lut[i] = x <= 0.04045f ? x / 12.92f : powf((x + 0.055f) / 1.055f, 2.4f);
-    }
-}
-
 int check_scene_desc(const PathTracerDesc* d)
 {
     if (!d) return fail(STRELKA_ERR_INVALID_ARGUMENT, "desc is NULL");
@@ -721,10 +678,9 @@ int ensure_scene(StrelkaPathTracer* pt, const BVHNode* nodes, uint32_t numNodes,
     }
     if (numNodes) {
         Timer t(pt, KC_PREP, st);
-        int grid = std::min<int>((numNodes + 255) / 256, pt->numSMs * 16);
-        k_prep_rec<<<grid, 256, 0, st>>>(reinterpret_cast<const float4*>(nodes), numNodes, inst, numInstances, ib, numIndices,
-                                         vb, numVertices, pt->rec, pt->status);
-        SB_CUDA_TRY(cudaGetLastError());
+        int rc = launch_prep_records(nodes, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, pt->rec,
+                                     pt->status, pt->numSMs, st);
+        if (rc) return rc;
     }
     pt->sceneVersion = version;
     pt->keyNodes = nodes;
@@ -737,10 +693,48 @@ int ensure_scene(StrelkaPathTracer* pt, const BVHNode* nodes, uint32_t numNodes,
 
 DevScene make_scene(StrelkaPathTracer* pt, const PathTracerDesc* d)
 {
+    return scene_from_desc(d, pt->rec, pt->srgbLut, pt->status);
+}
+
+int occupancy_grid(const void* fn, int block, int numSMs)
+{
+    int perSM = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, block, 0) != cudaSuccess || perSM < 1) perSM = 1;
+    return perSM * numSMs;
+}
+
+}  // namespace
+
+namespace sb {
+
+void srgb_lut_host(float* lut)
+{
+    for (int i = 0; i < 256; ++i) {
+        float x = (float)i / 255.0f;
+        lut[i] = x <= 0.04045f ? x / 12.92f : powf((x + 0.055f) / 1.055f, 2.4f);
+    }
+}
+
+int validate_scene_desc(const PathTracerDesc* d) { return check_scene_desc(d); }
+
+int launch_prep_records(const BVHNode* nodes, uint32_t numNodes, const InstanceConstants* inst, uint32_t numInstances,
+                        const uint32_t* ib, uint32_t numIndices, const Vertex* vb, uint32_t numVertices, float4* rec,
+                        uint32_t* status, int numSMs, cudaStream_t st)
+{
+    if (!numNodes) return STRELKA_OK;
+    int grid = std::min<int>((numNodes + 255) / 256, numSMs * 16);
+    k_prep_rec<<<grid, 256, 0, st>>>(reinterpret_cast<const float4*>(nodes), numNodes, inst, numInstances, ib, numIndices,
+                                     vb, numVertices, rec, status);
+    SB_CUDA_TRY(cudaGetLastError());
+    return STRELKA_OK;
+}
+
+DevScene scene_from_desc(const PathTracerDesc* d, const float4* rec, const float* srgbLut, uint32_t* status)
+{
     DevScene s{};
     s.nodes = reinterpret_cast<const float4*>(d->bvhNodes);
     s.tris = nullptr;
-    s.rec = pt->rec;
+    s.rec = rec;
     s.numNodes = d->numNodes;
     s.numVertices = d->numVertices;
     s.vb = d->vb;
@@ -758,21 +752,14 @@ DevScene make_scene(StrelkaPathTracer* pt, const PathTracerDesc* d)
     s.numResInfos = d->mdl_resource_infos ? d->numResourceInfos : 0;
     s.numTextures = d->matTextures ? d->numTextures : 0;
     s.textures = d->matTextures;
-    s.srgbLut = pt->srgbLut;
+    s.srgbLut = srgbLut;
     s.hasEnv = d->envMap != nullptr;
     if (d->envMap) s.env = *d->envMap;
-    s.status = pt->status;
+    s.status = status;
     return s;
 }
 
-int occupancy_grid(const void* fn, int block, int numSMs)
-{
-    int perSM = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fn, block, 0) != cudaSuccess || perSM < 1) perSM = 1;
-    return perSM * numSMs;
-}
-
-}  // namespace
+}  // namespace sb
 
 extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, StrelkaPathTracer** out)
 {

@@ -865,6 +865,27 @@ extern "C" int strelka_scene_large(const StrelkaLargeConfig* cfg, StrelkaHostSce
     return STRELKA_OK;
 }
 
+extern "C" int strelka_camera_lookat(PathTracerParam* p, uint32_t width, uint32_t height, const float eye[3],
+                                     const float target[3], float fovDeg)
+{
+    if (!p || !eye || !target || width == 0 || height == 0 || !(fovDeg > 0.0f && fovDeg < 180.0f))
+        return sb::fail(STRELKA_ERR_INVALID_ARGUMENT, "invalid camera arguments");
+    const double e[3] = {eye[0], eye[1], eye[2]}, t[3] = {target[0], target[1], target[2]};
+    if (e[0] == t[0] && e[1] == t[1] && e[2] == t[2]) return sb::fail(STRELKA_ERR_INVALID_ARGUMENT, "eye == target");
+    PathTracerParam c;
+    set_camera(c, width, height, e, t, fovDeg);
+    p->viewToWorld = c.viewToWorld;
+    p->clipToView = c.clipToView;
+    p->viewToClip = c.viewToClip;
+    p->worldToView = c.worldToView;
+    p->camPos = c.camPos;
+    p->dimension[0] = c.dimension[0];
+    p->dimension[1] = c.dimension[1];
+    p->invDimension[0] = c.invDimension[0];
+    p->invDimension[1] = c.invDimension[1];
+    return STRELKA_OK;
+}
+
 extern "C" void strelka_scene_free(StrelkaHostScene* s)
 {
     if (!s) return;

@@ -249,6 +249,76 @@ class RadianceCache:
             pass
 
 
+def batch_config(mode: int = abi.BATCH_WAVEFRONT, block_size: int = 128, queue_chunk: int = 256,
+                 material_sort: bool = False, use_graph: bool = True) -> abi.StrelkaBatchConfig:
+    return abi.StrelkaBatchConfig(mode, block_size, queue_chunk, 1 if material_sort else 0, 1 if use_graph else 0)
+
+
+class Batch:
+    """Many scene/camera jobs rendered as one batch (strelka_batch_*).  Each
+    job is a PathTracerDesc with its own constants and sample buffer; the
+    scenes (DeviceScene objects) must outlive the batch's use of them."""
+
+    def __init__(self):
+        self.lib = abi.load()
+        h = C.c_void_p()
+        abi.check(self.lib.strelka_batch_create(C.byref(h)))
+        self.handle = h
+        self._descs = None
+
+    def set_jobs(self, descs, stream=None) -> None:
+        arr = (abi.PathTracerDesc * max(len(descs), 1))(*descs)
+        abi.check(self.lib.strelka_batch_set_jobs(self.handle, arr, len(descs), _stream_handle(stream)))
+        self._descs = (descs, arr)
+
+    def set_frame(self, frame_offset: int, stream=None) -> None:
+        abi.check(self.lib.strelka_batch_set_frame(self.handle, frame_offset, _stream_handle(stream)))
+
+    def execute(self, config: abi.StrelkaBatchConfig | None = None, stream=None) -> None:
+        abi.check(self.lib.strelka_batch_execute(self.handle, C.byref(config) if config is not None else None,
+                                                 _stream_handle(stream)))
+
+    def autotune(self, repeats: int = 3, stream=None):
+        """Returns (best config, [(config, ms), ...])."""
+        cap = 64
+        entries = (abi.StrelkaBatchTuneEntry * cap)()
+        n = C.c_uint32()
+        best = abi.StrelkaBatchConfig()
+        abi.check(self.lib.strelka_batch_autotune(self.handle, repeats, entries, cap, C.byref(n), C.byref(best),
+                                                  _stream_handle(stream)))
+        return best, [(entries[i].config, entries[i].ms) for i in range(min(n.value, cap))]
+
+    def job_latency(self, stream=None) -> list:
+        ms = (C.c_float * abi.BATCH_MAX_JOBS)()
+        n = self.lib.strelka_batch_job_latency(self.handle, _stream_handle(stream), ms, abi.BATCH_MAX_JOBS)
+        if n < 0:
+            abi.check(n)
+        return [ms[i] for i in range(n)]
+
+    def device_status(self, stream=None) -> int:
+        st = C.c_uint32(0)
+        abi.check(self.lib.strelka_batch_get_device_status(self.handle, _stream_handle(stream), C.byref(st)))
+        return st.value
+
+    def info(self) -> dict:
+        total = C.c_uint64()
+        jobs = C.c_uint32()
+        keys = C.c_uint32()
+        abi.check(self.lib.strelka_batch_info(self.handle, C.byref(total), C.byref(jobs), C.byref(keys)))
+        return {"total_paths": total.value, "jobs": jobs.value, "sort_keys": keys.value}
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.strelka_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class ReductionPass:
     """ReductionPass (shaders/reduction.hlsl:9-32)."""
 

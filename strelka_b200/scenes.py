@@ -67,6 +67,16 @@ class HostScene:
         root = self.nodes[:32].view(np.float32)
         return root[0:3].copy(), root[4:7].copy()
 
+    def look_at(self, width: int, height: int, eye, target, fov_deg: float = 40.0, **kw) -> abi.PathTracerParam:
+        """The parameter block with a pinhole camera at `eye` looking at
+        `target` (strelka_camera_lookat), rendering width x height, and
+        other fields overridden by `kw`."""
+        p = self.param(**kw)
+        e = (C.c_float * 3)(*[float(v) for v in eye])
+        t = (C.c_float * 3)(*[float(v) for v in target])
+        abi.check(abi.load().strelka_camera_lookat(C.byref(p), width, height, e, t, fov_deg))
+        return p
+
     def param(self, **kw) -> abi.PathTracerParam:
         """A copy of the camera parameter block with fields overridden by `kw`."""
         p = abi.PathTracerParam()
