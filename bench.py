@@ -430,6 +430,144 @@ def run_nrc(args):
     print(json.dumps(line), flush=True)
 
 
+def batch_jobs(args, rng):
+    """The batch workload: --batch-scenes scenes from the large-render
+    generator with triangle counts log-uniform in [50k, 10M], and
+    --batch-jobs jobs, each a scene with a camera on a random orbit,
+    resolution log-uniform from 256x256 to 1920x1080, spp uniform in
+    {1..16}, depth 6."""
+    from strelka_b200 import scenes
+
+    per_sphere_max = 20 * 89 * 89
+    scene_list = []
+    for k in range(args.batch_scenes):
+        tris = float(np.exp(rng.uniform(np.log(5e4), np.log(1e7))))
+        if tris < per_sphere_max:
+            inst, freq = 1, max(8, int(round(np.sqrt(tris / 20))))
+        else:
+            inst, freq = min(64, max(1, int(round(tris / per_sphere_max)))), 89
+        hs = scenes.large(width=256, height=256, instances=inst, frequency=freq, num_textures=8, tex_size=2048,
+                          env_width=1024, env_height=512, max_depth=6, spp=1, seed=100 + k)
+        scene_list.append(hs)
+    jobs = []
+    for j in range(args.batch_jobs):
+        si = int(rng.integers(len(scene_list)))
+        t = rng.uniform()
+        w = int(round(256 * (1920 / 256) ** t))
+        h = int(round(256 * (1080 / 256) ** t))
+        spp = int(rng.integers(1, 17))
+        a = rng.uniform(0, 2 * np.pi)
+        eye = (30 * np.sin(a), 4 + 8 * rng.uniform(), 30 * np.cos(a))
+        jobs.append((si, w, h, spp, eye, j))
+    return scene_list, jobs
+
+
+def run_batch(args):
+    """--workload batch: the jobs of batch_jobs rendered as one batch
+    (autotuned configuration, CUDA graph), timed over --steps executions
+    after --warmup, each with new sample seeds; against the same jobs
+    rendered one PathTracer::execute at a time (the reference's shape)."""
+    import torch
+
+    from strelka_b200 import abi
+    from strelka_b200.render import Batch, DeviceScene, PathTracer
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    rng = np.random.default_rng(args.batch_seed)
+    t0 = time.perf_counter()
+    scene_list, jobs = batch_jobs(args, rng)
+    gen_s = time.perf_counter() - t0
+    dss = [DeviceScene(hs) for hs in scene_list]
+    params, bufs, descs = [], [], []
+    for si, w, h, spp, eye, fn in jobs:
+        p = scene_list[si].look_at(w, h, eye, (0.0, 1.5, 0.0), 40.0, spp=spp, maxDepth=6, frameNumber=fn)
+        sb = torch.empty(w * h * spp * 3, dtype=torch.float32, device="cuda")
+        params.append(p)
+        bufs.append(sb)
+        descs.append(dss[si].desc(p, sb))
+    paths = [w * h * spp for _, w, h, spp, _, _ in jobs]
+    total = sum(paths)
+    stream = torch.cuda.current_stream()
+    b = Batch()
+    b.set_jobs(descs, stream)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    best, entries = b.autotune(repeats=args.batch_tune_repeats, stream=stream)
+    tune_s = time.perf_counter() - t1
+    for k in range(args.warmup):
+        b.set_frame(1000 + k, stream)
+        b.execute(None, stream)
+    torch.cuda.synchronize()
+    st = b.device_status(stream)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    times, lats = [], []
+    for k in range(args.steps):
+        b.set_frame(2000 + k, stream)  # synchronises; outside the timed interval
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.execute(None, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        lats.append(b.job_latency(stream))
+    clk = clocks.stop()
+    st |= b.device_status(stream)
+    ms = statistics.median(times)
+    lat = np.median(np.array(lats), axis=0)
+
+    # the same jobs one execute at a time (wavefront pass, whole-job chunks)
+    pt = PathTracer(mode=abi.MODE_WAVEFRONT)
+    for p, sb, (si, *_rest) in zip(params, bufs, jobs):
+        n = p.dimension[0] * p.dimension[1] * p.spp
+        pt.execute(dss[si].desc(p, sb), n, 1, 0, stream)
+    torch.cuda.synchronize()
+    seq = []
+    for k in range(max(1, min(args.steps, 3))):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for p, sb, (si, *_rest) in zip(params, bufs, jobs):
+            n = p.dimension[0] * p.dimension[1] * p.spp
+            pt.execute(dss[si].desc(p, sb), n, 1, 0, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        seq.append(e0.elapsed_time(e1))
+    st |= pt.device_status(stream)
+    pt.close()
+    b.close()
+    if st != 0:
+        raise RuntimeError(f"device status {st:#x}")
+    seq_ms = statistics.median(seq)
+    order = np.argsort(paths)
+    line = {
+        "metric": "batched Mpaths/s (32 jobs)", "value": total / (ms * 1e-3) / 1e6, "unit": "Mpaths/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{len(jobs)} jobs over {len(scene_list)} scenes of the large-render generator "
+                               "(50k-10M triangles), resolutions log-uniform 256^2..1920x1080, 1-16 spp, depth 6",
+                   "total_paths": total, "scene_triangles": [hs.num_triangles for hs in scene_list],
+                   "jobs": [{"scene": si, "w": w, "h": h, "spp": spp} for si, w, h, spp, _, _ in jobs],
+                   "l2": "inputs larger than L2", "seed": args.batch_seed},
+        "tuned": {"mode": ["persistent", "wavefront"][best.mode], "block": best.blockSize,
+                  "queue_chunk": best.queueChunk, "material_sort": bool(best.materialSort),
+                  "graph": bool(best.useGraph)},
+        "autotune": [{"mode": ["persistent", "wavefront"][c.mode], "block": c.blockSize, "chunk": c.queueChunk,
+                      "sort": bool(c.materialSort), "ms": round(t, 3)} for c, t in entries],
+        "job_latency_ms": {"p50": float(np.percentile(lat, 50)), "p95": float(np.percentile(lat, 95)),
+                           "max": float(lat.max()), "per_job": [round(float(v), 3) for v in lat],
+                           "smallest_job": round(float(lat[order[0]]), 3),
+                           "largest_job": round(float(lat[order[-1]]), 3)},
+        "sequential_single_job": {"ms": seq_ms, "mpaths_s": total / (seq_ms * 1e-3) / 1e6},
+        "gpu_launches": 1, "clocks": clk,
+        "setup_seconds": {"scene_generation": gen_s, "autotune": tune_s},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -447,7 +585,11 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-step-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="large", choices=["large", "traversal", "nrc"])
+    ap.add_argument("--workload", default="large", choices=["large", "traversal", "nrc", "batch"])
+    ap.add_argument("--batch-jobs", type=int, default=32)
+    ap.add_argument("--batch-scenes", type=int, default=6)
+    ap.add_argument("--batch-seed", type=int, default=0)
+    ap.add_argument("--batch-tune-repeats", type=int, default=3)
     ap.add_argument("--tris", type=int, default=1_000_000)
     ap.add_argument("--rays", type=int, default=4_000_000)
     ap.add_argument("--ref-spp", type=int, default=16384)
@@ -467,6 +609,9 @@ def main():
         return
     if args.workload == "nrc":
         run_nrc(args)
+        return
+    if args.workload == "batch":
+        run_batch(args)
         return
     args.warmup = max(args.warmup, 3) if args.impl == "strelka" else args.warmup
 
