@@ -298,11 +298,14 @@ typedef struct StrelkaPathTracerConfig {
     uint32_t chunkPaths;      /* wavefront: paths in flight per chunk (0 = auto) */
     uint32_t blockSize;       /* threads per block (0 = auto) */
     uint32_t flags;           /* STRELKA_PT_* */
+    uint32_t queueChunk;      /* wavefront: queue entries a warp takes at a time (0 = 32; a multiple of 32) */
+    uint32_t pad[3];
 } StrelkaPathTracerConfig;
 
 enum {
-    STRELKA_PT_PROFILE = 1u << 0, /* record per-kernel CUDA events (strelka_pathtracer_get_kernel_times) */
-    STRELKA_PT_COUNT = 1u << 1    /* count traversal visits (strelka_pathtracer_get_counters) */
+    STRELKA_PT_PROFILE = 1u << 0,       /* record per-kernel CUDA events (strelka_pathtracer_get_kernel_times) */
+    STRELKA_PT_COUNT = 1u << 1,         /* count traversal visits (strelka_pathtracer_get_counters) */
+    STRELKA_PT_NO_SHADE_SORT = 1u << 2  /* wavefront: shade paths in queue order, not sorted by material */
 };
 
 typedef struct StrelkaPathTracer StrelkaPathTracer;

@@ -45,6 +45,7 @@ MODE_WAVEFRONT = 0
 MODE_MEGAKERNEL = 1
 PT_PROFILE = 1
 PT_COUNT = 2
+PT_NO_SHADE_SORT = 4
 
 TRACE_CLOSEST = 0
 TRACE_ANY = 1
@@ -52,7 +53,7 @@ TRACE_COUNT = 1 << 4
 TRACE_REFINE = 1 << 5
 
 KERNEL_CLASSES = ["generate", "extend", "shade", "shadow", "finalize", "megakernel", "prep", "nrc_paths", "nrc_train",
-                  "nrc_infer"]
+                  "nrc_infer", "sort"]
 
 vp = C.c_void_p
 u8p = C.POINTER(C.c_uint8)
@@ -180,7 +181,8 @@ class TonemapDesc(C.Structure):
 
 
 class StrelkaPathTracerConfig(C.Structure):
-    _fields_ = [("mode", C.c_uint32), ("chunkPaths", C.c_uint32), ("blockSize", C.c_uint32), ("flags", C.c_uint32)]
+    _fields_ = [("mode", C.c_uint32), ("chunkPaths", C.c_uint32), ("blockSize", C.c_uint32), ("flags", C.c_uint32),
+                ("queueChunk", C.c_uint32), ("pad", C.c_uint32 * 3)]
 
 
 class TraceDesc(C.Structure):

@@ -96,43 +96,6 @@ __device__ __forceinline__ void job_done(BatchCtl* ctl, const BatchJobDev* jobs,
     }
 }
 
-// A warp's share of an atomic work queue: the warp takes `chunk` items at a
-// time and hands them to the lanes that ask.  Returns the item of a lane that
-// asked and got one, else SB_INVALID.  Warp-uniform state; called by the
-// whole warp.
-struct WarpPool {
-    uint32_t next, end;
-    int dry;
-};
-
-__device__ __forceinline__ uint32_t pool_take(WarpPool& p, uint32_t* counter, uint32_t total, uint32_t chunk, bool need)
-{
-    const int lane = threadIdx.x & 31;
-    unsigned mask = __ballot_sync(kFull, need);
-    uint32_t got = SB_INVALID;
-    while (mask) {
-        if (p.next >= p.end) {
-            if (p.dry) break;
-            uint32_t base = 0;
-            if (lane == 0) base = atomicAdd(counter, chunk);
-            base = __shfl_sync(kFull, base, 0);
-            if (base >= total) {
-                p.dry = 1;
-                break;
-            }
-            p.next = base;
-            p.end = (uint32_t)min((uint64_t)base + chunk, (uint64_t)total);
-        }
-        const uint32_t avail = p.end - p.next;
-        const uint32_t rank = (uint32_t)__popc(mask & ((1u << lane) - 1u));
-        const bool served = ((mask >> lane) & 1u) && rank < avail;
-        if (served) got = p.next + rank;
-        p.next += min((uint32_t)__popc(mask), avail);
-        mask &= ~__ballot_sync(kFull, served);
-    }
-    return got;
-}
-
 __global__ void k_batch_begin(BatchCtl* ctl, int numJobs)
 {
     for (int j = threadIdx.x; j < numJobs; j += blockDim.x) {
@@ -587,7 +550,7 @@ int ensure_wave(StrelkaBatch* b, size_t cap)
         (rc = balloc(b, &w.col, cap)) || (rc = balloc(b, &w.rng, cap)) || (rc = balloc(b, &w.hit, cap)) ||
         (rc = balloc(b, &w.hitPrim, cap)) || (rc = balloc(b, &w.queue[0], cap)) || (rc = balloc(b, &w.queue[1], cap)) ||
         (rc = balloc(b, &w.sh_o, cap)) || (rc = balloc(b, &w.sh_d, cap)) || (rc = balloc(b, &w.sh_cd, cap)) ||
-        (rc = balloc(b, &w.sh_cg, cap)) || (rc = balloc(b, &w.counters, 4)) || (rc = balloc(b, &b->sorted, cap))) {
+        (rc = balloc(b, &w.sh_cg, cap)) || (rc = balloc(b, &w.counters, kWaveCounters)) || (rc = balloc(b, &b->sorted, cap))) {
         free_wave(b);
         return rc;
     }
@@ -641,7 +604,7 @@ int launch_wavefront(StrelkaBatch* b, const JobTable& jt, const StrelkaBatchConf
     uint32_t f = 0;
     for (uint64_t first = 0; first < b->total; first += chunkPaths) {
         const uint32_t n = (uint32_t)std::min<uint64_t>(chunkPaths, b->total - first);
-        SB_CUDA_TRY(cudaMemsetAsync(b->w.counters, 0, 4 * sizeof(uint32_t), st));
+        SB_CUDA_TRY(cudaMemsetAsync(b->w.counters, 0, kWaveCounters * sizeof(uint32_t), st));
         const int gridG = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, b->numSMs * 8);
         k_batch_generate<<<gridG, kSmallBlock, 0, st>>>(jt, b->w, (uint32_t)first, n);
         for (int depth = 0; depth < b->maxDepth; ++depth) {

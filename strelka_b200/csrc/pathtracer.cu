@@ -29,13 +29,15 @@ namespace {
 constexpr int kExtendBlock = 128;
 constexpr int kShadeBlock = 128;
 constexpr int kSmallBlock = 256;
+constexpr uint32_t kMaxSortKeys = 4096;
+constexpr uint32_t kDefaultQueueChunk = 32;
 
 // Minimum resident blocks per SM requested for the any-hit (shadow) kernel:
-// 10 blocks of 128 threads fit its registers without spills and measured
+// 8 blocks of 128 threads fit its registers without spills and measured
 // faster than the compiler's default; the closest-hit kernels keep the
 // default (a cap makes them spill).
 #ifndef SB_SHADOW_MINBLOCKS
-#define SB_SHADOW_MINBLOCKS 10
+#define SB_SHADOW_MINBLOCKS 8
 #endif
 
 enum KernelClass {
@@ -49,10 +51,11 @@ enum KernelClass {
     KC_NRC_PATHS,
     KC_NRC_TRAIN,
     KC_NRC_INFER,
+    KC_SORT,
     KC_COUNT
 };
-const char* kKernelNames[KC_COUNT] = {"generate",  "extend",    "shade",     "shadow",   "finalize", "megakernel",
-                                      "prep",      "nrc_paths", "nrc_train", "nrc_infer"};
+const char* kKernelNames[KC_COUNT] = {"generate",  "extend",    "shade",     "shadow",    "finalize", "megakernel",
+                                      "prep",      "nrc_paths", "nrc_train", "nrc_infer", "sort"};
 
 // ---------------------------------------------------------------------------
 // Scene preparation: the record table of traverse.cuh, per node slot.
@@ -165,6 +168,7 @@ constexpr int kNrcMaxVerts = 16;  // training vertices recorded per path
 
 struct WaveBuf {
     Wave w{};
+    uint32_t* sorted = nullptr;  // the shade queue in material order
     size_t cap = 0;
     std::vector<void*> allocs;
 };
@@ -184,6 +188,7 @@ __global__ void __launch_bounds__(kSmallBlock) k_generate(PathTracerParam ubo, W
         w.counters[0] = n;
         w.counters[1] = 0;
         w.counters[2] = 0;
+        w.counters[3] = 0;  // extend's work-queue head
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         PathState ps;
@@ -197,32 +202,37 @@ __global__ void __launch_bounds__(kSmallBlock) k_generate(PathTracerParam ubo, W
     }
 }
 
-// extend: closest-hit query for every queued path.  Each lane takes its next
+// extend: closest-hit query for every queued path.  Warps take `chunk`
+// queue entries at a time from an atomic head, and a lane takes its next
 // path as soon as its current query ends (the warp keeps stepping while any
-// lane has work), so a warp does not wait for its longest ray.
+// lane has work), so neither a warp nor a CTA waits for its longest ray.
 template <bool COUNT>
-__global__ void __launch_bounds__(kExtendBlock) k_extend(DevScene s, Wave w, int qin, unsigned long long* visitCounters)
+__global__ void __launch_bounds__(kExtendBlock) k_extend(DevScene s, Wave w, int qin, uint32_t chunk,
+                                                         unsigned long long* visitCounters)
 {
     const uint32_t count = w.counters[qin];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         w.counters[qin ^ 1] = 0;  // consumed by shade(k-1); refilled by shade(k)
         w.counters[2] = 0;        // consumed by shadow(k-1); refilled by shade(k)
+        w.counters[4] = 0;        // shade's work-queue head
     }
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
     uint32_t stackN[SB_STACK];
     float stackT[SB_STACK];
     uint32_t nI = 0, nL = 0, nR = 0;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    WarpPool pool{0, 0, 0};
     uint32_t slot = 0;
     Trav T;
-    bool have = i < count;
-    if (have) {
-        slot = q[i];
-        const float4 o = w.ray_o[slot], d = w.ray_d[slot];
-        trav_init(s, T, xyz(o), o.w, xyz(d), false);
-    }
-    while (__any_sync(0xffffffffu, have)) {
+    bool have = false;
+    while (true) {
+        const uint32_t i = pool_take(pool, &w.counters[3], count, chunk, !have);
+        if (!have && i != SB_INVALID) {
+            slot = q[i];
+            const float4 o = w.ray_o[slot], d = w.ray_d[slot];
+            trav_init(s, T, xyz(o), o.w, xyz(d), false);
+            have = true;
+        }
+        if (!__any_sync(0xffffffffu, have)) break;
         if (!have) continue;
         const bool done = T.cur == SB_INVALID || closest_step<COUNT>(s, T, stackN, stackT, nI, nL);
         if (!done) continue;
@@ -230,13 +240,7 @@ __global__ void __launch_bounds__(kExtendBlock) k_extend(DevScene s, Wave w, int
                               : make_float4(0.0f, 0.0f, 1e9f, __uint_as_float(SB_INVALID));
         w.hitPrim[slot] = T.found ? T.hit.primId : SB_INVALID;
         if (COUNT) ++nR;
-        i += stride;
-        have = i < count;
-        if (have) {
-            slot = q[i];
-            const float4 o = w.ray_o[slot], d = w.ray_d[slot];
-            trav_init(s, T, xyz(o), o.w, xyz(d), false);
-        }
+        have = false;
     }
     if (COUNT) {
         atomicAdd(&visitCounters[0], (unsigned long long)nI);
@@ -245,19 +249,108 @@ __global__ void __launch_bounds__(kExtendBlock) k_extend(DevScene s, Wave w, int
     }
 }
 
-// shade: one bounce of shading for every queued path; pushes surviving
-// paths to the other queue and next-event requests to the shadow queue.
-template <bool NRC>
-__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerParam ubo, Wave w, int qin, NrcWave nw)
+// Shade-queue sort (a counting sort by the hit's material, so the warps of
+// k_shade see few BSDF kinds): key 0 = miss, 1 + material id, numMaterials
+// + 1 for light instances and out-of-range ids.
+__device__ __forceinline__ uint32_t shade_key(const DevScene& s, const Wave& w, uint32_t slot)
+{
+    const uint32_t inst = __float_as_uint(w.hit[slot].w);
+    if (inst == SB_INVALID) return 0;
+    const uint32_t nm = s.numMaterials;
+    if (inst >= s.numInstances) return 1 + nm;
+    const uint32_t m = (uint32_t)__ldg(&s.inst[inst].materialId);
+    return 1 + (m < nm ? m : nm);
+}
+
+__global__ void __launch_bounds__(kSmallBlock) k_sort_count(DevScene s, Wave w, int qin, uint32_t numKeys, uint32_t* hist)
+{
+    __shared__ uint32_t sh[kMaxSortKeys];
+    for (uint32_t k = threadIdx.x; k < numKeys; k += blockDim.x) sh[k] = 0;
+    __syncthreads();
+    const uint32_t count = w.counters[qin];
+    const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        atomicAdd(&sh[shade_key(s, w, q[i])], 1u);
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < numKeys; k += blockDim.x)
+        if (sh[k]) atomicAdd(&hist[k], sh[k]);
+}
+
+// Exclusive scan of the histogram into offsets (one block), clearing the
+// histogram for the next bounce.
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* hist, uint32_t numKeys, uint32_t* offsets)
+{
+    __shared__ uint32_t part[1024];
+    const uint32_t per = (numKeys + 1023) / 1024;
+    const uint32_t k0 = threadIdx.x * per;
+    uint32_t sum = 0;
+    for (uint32_t k = k0; k < min(k0 + per, numKeys); ++k) sum += hist[k];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[threadIdx.x] - sum;
+    for (uint32_t k = k0; k < min(k0 + per, numKeys); ++k) {
+        const uint32_t h = hist[k];
+        offsets[k] = run;
+        run += h;
+        hist[k] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(kSmallBlock) k_sort_scatter(DevScene s, Wave w, int qin, uint32_t* offsets,
+                                                              uint32_t* sorted)
 {
     const uint32_t count = w.counters[qin];
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
-    uint32_t* qout = qin ? w.queue[0] : w.queue[1];
-    const int maxDepth = (int)ubo.maxDepth;
+    const int lane = threadIdx.x & 31;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
-        const uint32_t i = base + (threadIdx.x & 31u);
+        const uint32_t i = base + lane;
         const bool valid = i < count;
+        uint32_t slot = 0, key = 0xFFFFFFFFu;
+        if (valid) {
+            slot = q[i];
+            key = shade_key(s, w, slot);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, valid ? key : 0xFFFFFFFFu);
+        const int leader = __ffs(peers) - 1;
+        uint32_t pos = 0;
+        if (valid && lane == leader) pos = atomicAdd(&offsets[key], (uint32_t)__popc(peers));
+        pos = __shfl_sync(0xffffffffu, pos, leader);
+        if (valid) sorted[pos + __popc(peers & ((1u << lane) - 1u))] = slot;
+    }
+}
+
+// shade: one bounce of shading for every queued path; pushes surviving
+// paths to the other queue and next-event requests to the shadow queue.
+template <bool NRC>
+__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerParam ubo, Wave w, int qin,
+                                                       const uint32_t* order, uint32_t chunk, NrcWave nw)
+{
+    const uint32_t count = w.counters[qin];
+    if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[5] = 0;  // shadow's work-queue head
+    const uint32_t* __restrict__ q = order ? order : (qin ? w.queue[1] : w.queue[0]);
+    uint32_t* qout = qin ? w.queue[0] : w.queue[1];
+    const int maxDepth = (int)ubo.maxDepth;
+    const int lane = threadIdx.x & 31;
+    uint32_t next = 0, end = 0;
+    while (true) {
+        if (next >= end) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&w.counters[4], chunk);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= count) break;
+            next = base;
+            end = (uint32_t)min((uint64_t)base + chunk, (uint64_t)count);
+        }
+        const uint32_t i = next + lane;
+        next = min(next + 32u, end);
+        const bool valid = i < end;
         bool cont = false;
         ShadowReq sr;
         sr.kind = 0;
@@ -347,43 +440,45 @@ __global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerPar
 }
 
 // shadow: any-hit query for every next-event request (reference depth-first
-// order); adds the visible ones.  Lanes take new requests as theirs finish.
+// order); adds the visible ones.  Work is taken from an atomic queue in
+// `chunk` units as in k_extend.
 template <bool COUNT>
-__global__ void __launch_bounds__(kExtendBlock, SB_SHADOW_MINBLOCKS) k_shadow(DevScene s, Wave w, unsigned long long* visitCounters)
+__global__ void __launch_bounds__(kExtendBlock, SB_SHADOW_MINBLOCKS) k_shadow(DevScene s, Wave w, uint32_t chunk,
+                                                                              unsigned long long* visitCounters)
 {
     const uint32_t count = w.counters[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[3] = 0;  // the next extend's work-queue head
     uint32_t stackN[SB_STACK];
     uint32_t nI = 0, nL = 0, nR = 0;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    WarpPool pool{0, 0, 0};
+    uint32_t item = 0;
     Trav T;
-    bool have = i < count;
-    if (have) {
-        const float4 o = w.sh_o[i], d = w.sh_d[i];
-        trav_init(s, T, xyz(o), o.w, xyz(d), true);
-    }
-    while (__any_sync(0xffffffffu, have)) {
+    bool have = false;
+    while (true) {
+        const uint32_t i = pool_take(pool, &w.counters[5], count, chunk, !have);
+        if (!have && i != SB_INVALID) {
+            item = i;
+            const float4 o = w.sh_o[i], d = w.sh_d[i];
+            trav_init(s, T, xyz(o), o.w, xyz(d), true);
+            have = true;
+        }
+        if (!__any_sync(0xffffffffu, have)) break;
         if (!have) continue;
         const bool done = T.cur == SB_INVALID || any_step<COUNT>(s, T, stackN, nI, nL);
         if (!done) continue;
-        const float4 cd = w.sh_cd[i];
+        const float4 cd = w.sh_cd[item];
         const int kind = (int)__float_as_uint(cd.w);
         const bool visible = !T.found || (kind == 1 && T.hit.instId < s.numInstances &&
                                           __ldg(&s.inst[T.hit.instId].lightId) != -1);
         if (visible) {
-            const uint32_t slot = __float_as_uint(w.sh_d[i].w);
-            const float4 cg = w.sh_cg[i];
+            const uint32_t slot = __float_as_uint(w.sh_d[item].w);
+            const float4 cg = w.sh_cg[item];
             v3 c = xyz(w.col[slot]);
             apply_shadow(c, xyz(cd), xyz(cg));
             w.col[slot] = f4(c, 0.0f);
         }
         if (COUNT) ++nR;
-        i += stride;
-        have = i < count;
-        if (have) {
-            const float4 o = w.sh_o[i], d = w.sh_d[i];
-            trav_init(s, T, xyz(o), o.w, xyz(d), true);
-        }
+        have = false;
     }
     if (COUNT) {
         atomicAdd(&visitCounters[2], (unsigned long long)nI);
@@ -483,20 +578,25 @@ __global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, P
 // Ray-query microbenchmark kernels.
 template <bool ANY, bool COUNT, bool REFINE>
 __global__ void __launch_bounds__(kExtendBlock) k_trace(DevScene s, const float4* __restrict__ rays, Hit* __restrict__ hits,
-                                                        uint32_t n, unsigned long long* counters)
+                                                        uint32_t n, uint32_t* head, uint32_t chunk,
+                                                        unsigned long long* counters)
 {
     uint32_t stackN[SB_STACK];
     float stackT[SB_STACK];
     uint32_t nI = 0, nL = 0;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    WarpPool pool{0, 0, 0};
+    uint32_t i = 0;
     Trav T;
-    bool have = i < n;
-    if (have) {
-        const float4 o = __ldg(&rays[2 * (size_t)i]), d = __ldg(&rays[2 * (size_t)i + 1]);
-        trav_init(s, T, xyz(o), o.w, xyz(d), ANY);
-    }
-    while (__any_sync(0xffffffffu, have)) {
+    bool have = false;
+    while (true) {
+        const uint32_t got = pool_take(pool, head, n, chunk, !have);
+        if (!have && got != SB_INVALID) {
+            i = got;
+            const float4 o = __ldg(&rays[2 * (size_t)i]), d = __ldg(&rays[2 * (size_t)i + 1]);
+            trav_init(s, T, xyz(o), o.w, xyz(d), ANY);
+            have = true;
+        }
+        if (!__any_sync(0xffffffffu, have)) break;
         if (!have) continue;
         const bool done = T.cur == SB_INVALID || (ANY ? any_step<COUNT>(s, T, stackN, nI, nL)
                                                       : closest_step<COUNT>(s, T, stackN, stackT, nI, nL));
@@ -521,12 +621,7 @@ __global__ void __launch_bounds__(kExtendBlock) k_trace(DevScene s, const float4
         out[2] = __float_as_uint(h.t);
         out[3] = h.instId;
         out[4] = h.primId;
-        i += stride;
-        have = i < n;
-        if (have) {
-            const float4 o = __ldg(&rays[2 * (size_t)i]), d = __ldg(&rays[2 * (size_t)i + 1]);
-            trav_init(s, T, xyz(o), o.w, xyz(d), ANY);
-        }
+        have = false;
     }
     if (COUNT) {
         atomicAdd(&counters[0], (unsigned long long)nI);
@@ -576,6 +671,9 @@ struct StrelkaPathTracer {
     uint32_t nrcCountCap = 0;       // training batches the counters hold
     cudaStream_t side = nullptr;    // training runs here, beside the frame
     cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
+    uint32_t* traceHead = nullptr;    // work-queue head of the ray-query kernel
+    uint32_t* sortHist = nullptr;     // shade-queue sort histogram (cleared by each scan)
+    uint32_t* sortOffsets = nullptr;
 };
 
 namespace {
@@ -585,6 +683,7 @@ void free_wave(WaveBuf& b)
     for (void* p : b.allocs) cudaFree(p);
     b.allocs.clear();
     b.w = Wave{};
+    b.sorted = nullptr;
     b.cap = 0;
 }
 
@@ -609,7 +708,8 @@ int ensure_wave(WaveBuf& b, size_t cap)
         (rc = walloc(b, &w.col, cap)) || (rc = walloc(b, &w.rng, cap)) || (rc = walloc(b, &w.hit, cap)) ||
         (rc = walloc(b, &w.hitPrim, cap)) || (rc = walloc(b, &w.queue[0], cap)) || (rc = walloc(b, &w.queue[1], cap)) ||
         (rc = walloc(b, &w.sh_o, cap)) || (rc = walloc(b, &w.sh_d, cap)) || (rc = walloc(b, &w.sh_cd, cap)) ||
-        (rc = walloc(b, &w.sh_cg, cap)) || (rc = walloc(b, &w.counters, 4))) {
+        (rc = walloc(b, &w.sh_cg, cap)) || (rc = walloc(b, &w.counters, kWaveCounters)) ||
+        (rc = walloc(b, &b.sorted, cap))) {
         free_wave(b);
         return rc;
     }
@@ -774,6 +874,10 @@ extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, 
         delete pt;
         return fail(STRELKA_ERR_INVALID_ARGUMENT, "unknown mode %u", config->mode);
     }
+    if (pt->cfg.queueChunk && (pt->cfg.queueChunk > 4096 || (pt->cfg.queueChunk & 31))) {
+        delete pt;
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "queueChunk must be 0 or a multiple of 32 up to 4096");
+    }
     pt->device = dev;
     cudaDeviceGetAttribute(&pt->numSMs, cudaDevAttrMultiProcessorCount, dev);
     float lut[256];
@@ -789,6 +893,10 @@ extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, 
         return fail(STRELKA_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
     }
     cudaMemset(pt->visitCounters, 0, 8 * sizeof(unsigned long long));
+    if (cudaMalloc(&pt->traceHead, sizeof(uint32_t)) != cudaSuccess) {
+        strelka_pathtracer_destroy(pt);
+        return fail(STRELKA_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
+    }
     pt->extendGrid = occupancy_grid((const void*)k_extend<false>, kExtendBlock, pt->numSMs);
     pt->shadeGrid = occupancy_grid((const void*)k_shade<false>, kShadeBlock, pt->numSMs);
     pt->shadeGridNrc = occupancy_grid((const void*)k_shade<true>, kShadeBlock, pt->numSMs);
@@ -808,6 +916,9 @@ extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
     if (pt->nrcTrain) cudaFree(pt->nrcTrain);
     if (pt->nrcQueries) cudaFree(pt->nrcQueries);
     if (pt->nrcCounts) cudaFree(pt->nrcCounts);
+    if (pt->traceHead) cudaFree(pt->traceHead);
+    if (pt->sortHist) cudaFree(pt->sortHist);
+    if (pt->sortOffsets) cudaFree(pt->sortOffsets);
     if (pt->forkEvent) cudaEventDestroy(pt->forkEvent);
     if (pt->joinEvent) cudaEventDestroy(pt->joinEvent);
     if (pt->side) cudaStreamDestroy(pt->side);
@@ -910,6 +1021,17 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
     rc = ensure_wave(pt->main, chunk);
     if (rc) return rc;
     const int maxDepth = (int)ubo.maxDepth;
+    const uint32_t qchunk = pt->cfg.queueChunk ? pt->cfg.queueChunk : kDefaultQueueChunk;
+    // shade-queue sort by material: one key per material + miss + light/invalid
+    uint32_t sortKeys = 0;
+    if (!(pt->cfg.flags & STRELKA_PT_NO_SHADE_SORT) && s.numMaterials + 2 <= kMaxSortKeys) {
+        sortKeys = s.numMaterials + 2;
+        if (!pt->sortHist) {
+            SB_CUDA_TRY(cudaMalloc(&pt->sortHist, kMaxSortKeys * sizeof(uint32_t)));
+            SB_CUDA_TRY(cudaMalloc(&pt->sortOffsets, kMaxSortKeys * sizeof(uint32_t)));
+            SB_CUDA_TRY(cudaMemsetAsync(pt->sortHist, 0, kMaxSortKeys * sizeof(uint32_t), st));
+        }
+    }
     NrcWave nw{};
     if (useNrc) {
         if (chunk > pt->nrcQueryCap) {
@@ -956,20 +1078,29 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             const bool count = (pt->cfg.flags & STRELKA_PT_COUNT) != 0;
             {
                 Timer t(pt, KC_EXTEND, st);
-                if (count) k_extend<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, pt->visitCounters);
-                else k_extend<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, nullptr);
+                if (count) k_extend<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, qchunk, pt->visitCounters);
+                else k_extend<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, qchunk, nullptr);
+            }
+            const uint32_t* order = nullptr;
+            if (sortKeys) {
+                Timer t(pt, KC_SORT, st);
+                const int gridK = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, pt->numSMs * 4);
+                k_sort_count<<<gridK, kSmallBlock, 0, st>>>(s, pt->main.w, qin, sortKeys, pt->sortHist);
+                k_sort_scan<<<1, 1024, 0, st>>>(pt->sortHist, sortKeys, pt->sortOffsets);
+                k_sort_scatter<<<gridK, kSmallBlock, 0, st>>>(s, pt->main.w, qin, pt->sortOffsets, pt->main.sorted);
+                order = pt->main.sorted;
             }
             {
                 Timer t(pt, KC_SHADE, st);
                 if (useNrc)
-                    k_shade<true><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->main.w, qin, nw);
+                    k_shade<true><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->main.w, qin, order, qchunk, nw);
                 else
-                    k_shade<false><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->main.w, qin, nw);
+                    k_shade<false><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->main.w, qin, order, qchunk, nw);
             }
             {
                 Timer t(pt, KC_SHADOW, st);
-                if (count) k_shadow<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, pt->visitCounters);
-                else k_shadow<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, nullptr);
+                if (count) k_shadow<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qchunk, pt->visitCounters);
+                else k_shadow<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qchunk, nullptr);
             }
         }
         if (useNrc) {
@@ -1103,13 +1234,17 @@ extern "C" int strelka_trace_execute(StrelkaPathTracer* pt, const TraceDesc* d, 
     const int grid = std::min<int>((d->numRays + kExtendBlock - 1) / kExtendBlock, pt->extendGrid);
     const float4* rays = reinterpret_cast<const float4*>(d->rays);
     Timer t(pt, KC_EXTEND, st);
-    if (any && cnt) k_trace<true, true, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, d->counters);
-    else if (any) k_trace<true, false, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, nullptr);
+    SB_CUDA_TRY(cudaMemsetAsync(pt->traceHead, 0, sizeof(uint32_t), st));
+    const uint32_t qc = pt->cfg.queueChunk ? pt->cfg.queueChunk : kDefaultQueueChunk;
+    uint32_t* hd = pt->traceHead;
+    const uint32_t nr = d->numRays;
+    if (any && cnt) k_trace<true, true, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, nr, hd, qc, d->counters);
+    else if (any) k_trace<true, false, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, nr, hd, qc, nullptr);
     else if (refine && cnt)
-        k_trace<false, true, true><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, d->counters);
-    else if (refine) k_trace<false, false, true><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, nullptr);
-    else if (cnt) k_trace<false, true, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, d->counters);
-    else k_trace<false, false, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, d->numRays, nullptr);
+        k_trace<false, true, true><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, nr, hd, qc, d->counters);
+    else if (refine) k_trace<false, false, true><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, nr, hd, qc, nullptr);
+    else if (cnt) k_trace<false, true, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, nr, hd, qc, d->counters);
+    else k_trace<false, false, false><<<grid, kExtendBlock, 0, st>>>(s, rays, d->hits, nr, hd, qc, nullptr);
     SB_CUDA_TRY(cudaGetLastError());
     return STRELKA_OK;
 }
