@@ -169,6 +169,7 @@ constexpr int kNrcMaxVerts = 16;  // training vertices recorded per path
 struct WaveBuf {
     Wave w{};
     uint32_t* sorted = nullptr;  // the shade queue in material order
+    uint16_t* keys = nullptr;    // sort key of each queue entry
     size_t cap = 0;
     std::vector<void*> allocs;
 };
@@ -262,15 +263,20 @@ __device__ __forceinline__ uint32_t shade_key(const DevScene& s, const Wave& w, 
     return 1 + (m < nm ? m : nm);
 }
 
-__global__ void __launch_bounds__(kSmallBlock) k_sort_count(DevScene s, Wave w, int qin, uint32_t numKeys, uint32_t* hist)
+// Keys of the queue in queue order (keys[i] for entry i) and their histogram.
+__global__ void __launch_bounds__(kSmallBlock) k_sort_count(DevScene s, Wave w, int qin, uint32_t numKeys, uint32_t* hist,
+                                                            uint16_t* keys)
 {
     __shared__ uint32_t sh[kMaxSortKeys];
     for (uint32_t k = threadIdx.x; k < numKeys; k += blockDim.x) sh[k] = 0;
     __syncthreads();
     const uint32_t count = w.counters[qin];
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
-        atomicAdd(&sh[shade_key(s, w, q[i])], 1u);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t key = shade_key(s, w, q[i]);
+        keys[i] = (uint16_t)key;
+        atomicAdd(&sh[key], 1u);
+    }
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < numKeys; k += blockDim.x)
         if (sh[k]) atomicAdd(&hist[k], sh[k]);
@@ -302,27 +308,45 @@ __global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* hist, uint32_t num
     }
 }
 
-__global__ void __launch_bounds__(kSmallBlock) k_sort_scatter(DevScene s, Wave w, int qin, uint32_t* offsets,
-                                                              uint32_t* sorted)
+// Scatter in tiles of kSortTile entries: ranks within the tile come from
+// shared-memory counters (one atomic per key per warp), and each tile
+// reserves its range of every key with one global atomic per key.
+constexpr int kSortPerThread = 8;
+constexpr int kSortTile = kSmallBlock * kSortPerThread;
+
+__global__ void __launch_bounds__(kSmallBlock) k_sort_scatter(Wave w, int qin, uint32_t numKeys, const uint16_t* __restrict__ keys,
+                                                              uint32_t* offsets, uint32_t* sorted)
 {
+    __shared__ uint32_t cnt[kMaxSortKeys];
     const uint32_t count = w.counters[qin];
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
     const int lane = threadIdx.x & 31;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
-        const uint32_t i = base + lane;
-        const bool valid = i < count;
-        uint32_t slot = 0, key = 0xFFFFFFFFu;
-        if (valid) {
-            slot = q[i];
-            key = shade_key(s, w, slot);
+    for (uint32_t tile = blockIdx.x * (uint32_t)kSortTile; tile < count; tile += gridDim.x * (uint32_t)kSortTile) {
+        for (uint32_t k = threadIdx.x; k < numKeys; k += blockDim.x) cnt[k] = 0;
+        __syncthreads();
+        uint32_t key[kSortPerThread], rank[kSortPerThread];
+#pragma unroll
+        for (int j = 0; j < kSortPerThread; ++j) {
+            const uint32_t i = tile + (uint32_t)j * kSmallBlock + threadIdx.x;
+            const bool valid = i < count;
+            key[j] = valid ? keys[i] : 0xFFFFu;
+            const unsigned peers = __match_any_sync(0xffffffffu, key[j]);
+            const int leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (valid && lane == leader) base = atomicAdd(&cnt[key[j]], (uint32_t)__popc(peers));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            rank[j] = base + __popc(peers & ((1u << lane) - 1u));
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, valid ? key : 0xFFFFFFFFu);
-        const int leader = __ffs(peers) - 1;
-        uint32_t pos = 0;
-        if (valid && lane == leader) pos = atomicAdd(&offsets[key], (uint32_t)__popc(peers));
-        pos = __shfl_sync(0xffffffffu, pos, leader);
-        if (valid) sorted[pos + __popc(peers & ((1u << lane) - 1u))] = slot;
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < numKeys; k += blockDim.x)
+            if (cnt[k]) cnt[k] = atomicAdd(&offsets[k], cnt[k]);
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kSortPerThread; ++j) {
+            const uint32_t i = tile + (uint32_t)j * kSmallBlock + threadIdx.x;
+            if (i < count) sorted[cnt[key[j]] + rank[j]] = q[i];
+        }
+        __syncthreads();
     }
 }
 
@@ -684,6 +708,7 @@ void free_wave(WaveBuf& b)
     b.allocs.clear();
     b.w = Wave{};
     b.sorted = nullptr;
+    b.keys = nullptr;
     b.cap = 0;
 }
 
@@ -709,7 +734,7 @@ int ensure_wave(WaveBuf& b, size_t cap)
         (rc = walloc(b, &w.hitPrim, cap)) || (rc = walloc(b, &w.queue[0], cap)) || (rc = walloc(b, &w.queue[1], cap)) ||
         (rc = walloc(b, &w.sh_o, cap)) || (rc = walloc(b, &w.sh_d, cap)) || (rc = walloc(b, &w.sh_cd, cap)) ||
         (rc = walloc(b, &w.sh_cg, cap)) || (rc = walloc(b, &w.counters, kWaveCounters)) ||
-        (rc = walloc(b, &b.sorted, cap))) {
+        (rc = walloc(b, &b.sorted, cap)) || (rc = walloc(b, &b.keys, cap))) {
         free_wave(b);
         return rc;
     }
@@ -1085,9 +1110,11 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             if (sortKeys) {
                 Timer t(pt, KC_SORT, st);
                 const int gridK = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, pt->numSMs * 4);
-                k_sort_count<<<gridK, kSmallBlock, 0, st>>>(s, pt->main.w, qin, sortKeys, pt->sortHist);
+                k_sort_count<<<gridK, kSmallBlock, 0, st>>>(s, pt->main.w, qin, sortKeys, pt->sortHist, pt->main.keys);
                 k_sort_scan<<<1, 1024, 0, st>>>(pt->sortHist, sortKeys, pt->sortOffsets);
-                k_sort_scatter<<<gridK, kSmallBlock, 0, st>>>(s, pt->main.w, qin, pt->sortOffsets, pt->main.sorted);
+                const int gridT = std::min<int>((n + kSortTile - 1) / kSortTile, pt->numSMs * 4);
+                k_sort_scatter<<<gridT, kSmallBlock, 0, st>>>(pt->main.w, qin, sortKeys, pt->main.keys, pt->sortOffsets,
+                                                             pt->main.sorted);
                 order = pt->main.sorted;
             }
             {
