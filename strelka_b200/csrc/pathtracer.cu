@@ -39,6 +39,11 @@ constexpr uint32_t kDefaultQueueChunk = 32;
 #ifndef SB_SHADOW_MINBLOCKS
 #define SB_SHADOW_MINBLOCKS 8
 #endif
+// The closest-hit kernel is latency-bound: 9 resident blocks (56 registers,
+// a few spilled) hide more of its dependent fetches than 8 without spills.
+#ifndef SB_EXTEND_MINBLOCKS
+#define SB_EXTEND_MINBLOCKS 9
+#endif
 
 enum KernelClass {
     KC_GENERATE = 0,
@@ -208,7 +213,7 @@ __global__ void __launch_bounds__(kSmallBlock) k_generate(PathTracerParam ubo, W
 // path as soon as its current query ends (the warp keeps stepping while any
 // lane has work), so neither a warp nor a CTA waits for its longest ray.
 template <bool COUNT>
-__global__ void __launch_bounds__(kExtendBlock) k_extend(DevScene s, Wave w, int qin, uint32_t chunk,
+__global__ void __launch_bounds__(kExtendBlock, SB_EXTEND_MINBLOCKS) k_extend(DevScene s, Wave w, int qin, uint32_t chunk,
                                                          unsigned long long* visitCounters)
 {
     const uint32_t count = w.counters[qin];
@@ -682,7 +687,7 @@ struct StrelkaPathTracer {
     std::vector<Rec> recs;
     std::vector<cudaEvent_t> eventPool;
     size_t eventsUsed = 0;
-    int extendGrid = 0, shadeGrid = 0, shadeGridNrc = 0, smallGrid = 0;
+    int extendGrid = 0, shadowGrid = 0, shadeGrid = 0, shadeGridNrc = 0, smallGrid = 0;
     unsigned long long* visitCounters = nullptr;  // 6 entries (STRELKA_PT_COUNT)
     // radiance cache
     StrelkaNrc* nrc = nullptr;
@@ -923,6 +928,7 @@ extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, 
         return fail(STRELKA_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
     }
     pt->extendGrid = occupancy_grid((const void*)k_extend<false>, kExtendBlock, pt->numSMs);
+    pt->shadowGrid = occupancy_grid((const void*)k_shadow<false>, kExtendBlock, pt->numSMs);
     pt->shadeGrid = occupancy_grid((const void*)k_shade<false>, kShadeBlock, pt->numSMs);
     pt->shadeGridNrc = occupancy_grid((const void*)k_shade<true>, kShadeBlock, pt->numSMs);
     pt->smallGrid = pt->numSMs * 8;
@@ -1098,6 +1104,7 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
         for (int depth = 0; depth < maxDepth; ++depth) {
             const int qin = depth & 1;
             const int gridE = std::min<int>((n + kExtendBlock - 1) / kExtendBlock, pt->extendGrid);
+            const int gridW = std::min<int>((n + kExtendBlock - 1) / kExtendBlock, pt->shadowGrid);
             const int gridS =
                 std::min<int>((n + kShadeBlock - 1) / kShadeBlock, useNrc ? pt->shadeGridNrc : pt->shadeGrid);
             const bool count = (pt->cfg.flags & STRELKA_PT_COUNT) != 0;
@@ -1126,8 +1133,8 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             }
             {
                 Timer t(pt, KC_SHADOW, st);
-                if (count) k_shadow<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qchunk, pt->visitCounters);
-                else k_shadow<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qchunk, nullptr);
+                if (count) k_shadow<true><<<gridW, kExtendBlock, 0, st>>>(s, pt->main.w, qchunk, pt->visitCounters);
+                else k_shadow<false><<<gridW, kExtendBlock, 0, st>>>(s, pt->main.w, qchunk, nullptr);
             }
         }
         if (useNrc) {

@@ -216,7 +216,9 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, v3 o, float tmax, v
 
 namespace sb {
 
+#ifndef SB_STACK
 #define SB_STACK 32
+#endif
 #define SB_LEAF_BIT 0x80000000u
 
 struct RayQ {
