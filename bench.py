@@ -41,6 +41,13 @@ if ROOT not in sys.path:
 METRIC = "Mpaths/s at 1080p"
 UNIT = "Mpaths/s"
 
+# DRAM bytes (read + write) per closest-hit query of the extend kernel on this
+# workload, from one ncu capture of a full frame's 8 extend launches
+# (dram__bytes_read.sum + dram__bytes_write.sum = 17.87 GB for 68.89M rays;
+# profiles/extend_large_1080p16_dram.md).  bench.py cannot run ncu itself, so
+# roofline.traffic is this figure times the rays of an average launch.
+EXTEND_DRAM_BYTES_PER_RAY = 259.4
+
 
 def workload_config(args):
     return {
@@ -754,7 +761,11 @@ def main():
         "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural scene, see config.workload)", "config": cfg,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": EXTEND_DRAM_BYTES_PER_RAY * cnt["extend_rays"] / max(ext_launches, 1)
+                     if args.width == 1920 and args.height == 1080 and args.spp == 16 else None,
+                     "traffic_source": "ncu DRAM bytes per ray of a full-frame capture x rays per launch",
+                     "bytes_alg_per_launch": bytes_alg / max(ext_launches, 1),
                      "kernel": "extend (closest-hit traversal)", "peak_source": peak_src,
                      "bytes_alg_timed_region": bytes_alg, "kernel_ms_timed_region": ext_ms,
                      "kernel_launches_timed_region": ext_launches, "visits": cnt},
