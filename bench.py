@@ -362,6 +362,7 @@ def run_nrc(args):
                diffuse_roughness=args.nrc_diffuse_roughness)
     for k in range(2):
         render(pt, 77 + k, args.nrc_spp)
+    pt.train_nrc(ds.desc(hs.param(spp=args.nrc_spp, frameNumber=79), sb), 79, args.nrc_warmup_group, stream)
     torch.cuda.synchronize()
     for trial in range(max(args.nrc_trials, 1)):
         cache = RadianceCache(lo, hi, learning_rate=args.nrc_lr, seed=1 + trial, log2_table_size=args.nrc_log2t)

@@ -192,8 +192,13 @@ __global__ void __launch_bounds__(kSmallBlock) k_batch_generate(JobTable jt, Wav
     }
 }
 
+// Resident threads per SM asked of the traversal kernels: 9 x 128 for
+// closest hit and 8 x 128 for any hit, as in the single-job pass.
+constexpr int kExtendThreadsPerSM = 9 * 128;
+constexpr int kShadowThreadsPerSM = 8 * 128;
+
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_batch_extend(JobTable jt, Wave w, int qin, uint32_t first, uint32_t chunk,
+__global__ void __launch_bounds__(BLOCK, kExtendThreadsPerSM / BLOCK) k_batch_extend(JobTable jt, Wave w, int qin, uint32_t first, uint32_t chunk,
                                                         uint32_t* fetch)
 {
     __shared__ uint32_t sp[kMaxJobs + 1];
@@ -247,8 +252,10 @@ __device__ __forceinline__ uint32_t shade_key(const JobTable& jt, const uint32_t
     return 1 + J.keyBase + (m < nm ? m : nm);
 }
 
+// Keys of the shade queue in queue order (keys[i] for entry i) and their
+// histogram.
 __global__ void __launch_bounds__(kSmallBlock) k_batch_sort_count(JobTable jt, Wave w, int qin, uint32_t first,
-                                                                  uint32_t numKeys, uint32_t* hist)
+                                                                  uint32_t numKeys, uint32_t* hist, uint16_t* keys)
 {
     __shared__ uint32_t sp[kMaxJobs + 1];
     __shared__ uint32_t sh[kMaxSortKeys];
@@ -256,8 +263,11 @@ __global__ void __launch_bounds__(kSmallBlock) k_batch_sort_count(JobTable jt, W
     load_prefix(jt, sp);
     const uint32_t count = w.counters[qin];
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
-        atomicAdd(&sh[shade_key(jt, sp, w, first, q[i])], 1u);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint32_t key = shade_key(jt, sp, w, first, q[i]);
+        keys[i] = (uint16_t)key;
+        atomicAdd(&sh[key], 1u);
+    }
     __syncthreads();
     for (uint32_t k = threadIdx.x; k < numKeys; k += blockDim.x)
         if (sh[k]) atomicAdd(&hist[k], sh[k]);
@@ -289,29 +299,46 @@ __global__ void __launch_bounds__(1024) k_batch_sort_scan(uint32_t* hist, uint32
     }
 }
 
-__global__ void __launch_bounds__(kSmallBlock) k_batch_sort_scatter(JobTable jt, Wave w, int qin, uint32_t first,
-                                                                    uint32_t* offsets, uint32_t* sorted)
+// Scatter in tiles of kSortTile entries: ranks within a tile come from
+// shared-memory counters (one atomic per key per warp), and each tile
+// reserves its range of every key with one global atomic per key.
+constexpr int kSortPerThread = 8;
+constexpr int kSortTile = kSmallBlock * kSortPerThread;
+
+__global__ void __launch_bounds__(kSmallBlock) k_batch_sort_scatter(Wave w, int qin, uint32_t numKeys,
+                                                                    const uint16_t* __restrict__ keys, uint32_t* offsets,
+                                                                    uint32_t* sorted)
 {
-    __shared__ uint32_t sp[kMaxJobs + 1];
-    load_prefix(jt, sp);
+    __shared__ uint32_t cnt[kMaxSortKeys];
     const uint32_t count = w.counters[qin];
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
     const int lane = threadIdx.x & 31;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
-        const uint32_t i = base + lane;
-        const bool valid = i < count;
-        uint32_t slot = 0, key = 0xFFFFFFFFu;
-        if (valid) {
-            slot = q[i];
-            key = shade_key(jt, sp, w, first, slot);
+    for (uint32_t tile = blockIdx.x * (uint32_t)kSortTile; tile < count; tile += gridDim.x * (uint32_t)kSortTile) {
+        for (uint32_t k = threadIdx.x; k < numKeys; k += blockDim.x) cnt[k] = 0;
+        __syncthreads();
+        uint32_t key[kSortPerThread], rank[kSortPerThread];
+#pragma unroll
+        for (int j = 0; j < kSortPerThread; ++j) {
+            const uint32_t i = tile + (uint32_t)j * kSmallBlock + threadIdx.x;
+            const bool valid = i < count;
+            key[j] = valid ? keys[i] : 0xFFFFu;
+            const unsigned peers = __match_any_sync(kFull, key[j]);
+            const int leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (valid && lane == leader) base = atomicAdd(&cnt[key[j]], (uint32_t)__popc(peers));
+            base = __shfl_sync(kFull, base, leader);
+            rank[j] = base + __popc(peers & ((1u << lane) - 1u));
         }
-        const unsigned peers = __match_any_sync(kFull, valid ? key : 0xFFFFFFFFu);
-        const int leader = __ffs(peers) - 1;
-        uint32_t pos = 0;
-        if (valid && lane == leader) pos = atomicAdd(&offsets[key], (uint32_t)__popc(peers));
-        pos = __shfl_sync(kFull, pos, leader);
-        if (valid) sorted[pos + __popc(peers & ((1u << lane) - 1u))] = slot;
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < numKeys; k += blockDim.x)
+            if (cnt[k]) cnt[k] = atomicAdd(&offsets[k], cnt[k]);
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kSortPerThread; ++j) {
+            const uint32_t i = tile + (uint32_t)j * kSmallBlock + threadIdx.x;
+            if (i < count) sorted[cnt[key[j]] + rank[j]] = q[i];
+        }
+        __syncthreads();
     }
 }
 
@@ -396,7 +423,7 @@ __global__ void __launch_bounds__(BLOCK) k_batch_shade(JobTable jt, Wave w, int 
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_batch_shadow(JobTable jt, Wave w, uint32_t first, uint32_t chunk,
+__global__ void __launch_bounds__(BLOCK, kShadowThreadsPerSM / BLOCK) k_batch_shadow(JobTable jt, Wave w, uint32_t first, uint32_t chunk,
                                                         uint32_t* fetch)
 {
     __shared__ uint32_t sp[kMaxJobs + 1];
@@ -498,6 +525,7 @@ struct StrelkaBatch {
     // wavefront state
     Wave w{};
     uint32_t* sorted = nullptr;
+    uint16_t* keys = nullptr;
     uint32_t* hist = nullptr;
     uint32_t* offsets = nullptr;
     size_t waveCap = 0;
@@ -525,6 +553,7 @@ void free_wave(StrelkaBatch* b)
     b->waveAllocs.clear();
     b->w = Wave{};
     b->sorted = nullptr;
+    b->keys = nullptr;
     b->waveCap = 0;
 }
 
@@ -550,7 +579,8 @@ int ensure_wave(StrelkaBatch* b, size_t cap)
         (rc = balloc(b, &w.col, cap)) || (rc = balloc(b, &w.rng, cap)) || (rc = balloc(b, &w.hit, cap)) ||
         (rc = balloc(b, &w.hitPrim, cap)) || (rc = balloc(b, &w.queue[0], cap)) || (rc = balloc(b, &w.queue[1], cap)) ||
         (rc = balloc(b, &w.sh_o, cap)) || (rc = balloc(b, &w.sh_d, cap)) || (rc = balloc(b, &w.sh_cd, cap)) ||
-        (rc = balloc(b, &w.sh_cg, cap)) || (rc = balloc(b, &w.counters, kWaveCounters)) || (rc = balloc(b, &b->sorted, cap))) {
+        (rc = balloc(b, &w.sh_cg, cap)) || (rc = balloc(b, &w.counters, kWaveCounters)) || (rc = balloc(b, &b->sorted, cap)) ||
+        (rc = balloc(b, &b->keys, cap))) {
         free_wave(b);
         return rc;
     }
@@ -612,10 +642,12 @@ int launch_wavefront(StrelkaBatch* b, const JobTable& jt, const StrelkaBatchConf
             k_batch_extend<BLOCK><<<gridE, BLOCK, 0, st>>>(jt, b->w, qin, (uint32_t)first, c.queueChunk, b->fetch + f++);
             const uint32_t* order = nullptr;
             if (c.materialSort) {
-                const int gridK = b->numSMs * 4;
-                k_batch_sort_count<<<gridK, kSmallBlock, 0, st>>>(jt, b->w, qin, (uint32_t)first, b->numKeys, b->hist);
+                const int gridK = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, b->numSMs * 4);
+                const int gridT = std::min<int>((n + kSortTile - 1) / kSortTile, b->numSMs * 4);
+                k_batch_sort_count<<<gridK, kSmallBlock, 0, st>>>(jt, b->w, qin, (uint32_t)first, b->numKeys, b->hist,
+                                                                  b->keys);
                 k_batch_sort_scan<<<1, 1024, 0, st>>>(b->hist, b->numKeys, b->offsets);
-                k_batch_sort_scatter<<<gridK, kSmallBlock, 0, st>>>(jt, b->w, qin, (uint32_t)first, b->offsets,
+                k_batch_sort_scatter<<<gridT, kSmallBlock, 0, st>>>(b->w, qin, b->numKeys, b->keys, b->offsets,
                                                                     b->sorted);
                 order = b->sorted;
             }
