@@ -281,6 +281,22 @@ typedef struct TonemapDesc {
     float* output;                /* RGBA32F */
 } TonemapDesc;
 
+/* shaders/upscalepassparam.h (16 bytes): the size of the OUTPUT image. */
+typedef struct Upscalepassparam {
+    int32_t dimension[2];
+    float invDimension[2];
+} Upscalepassparam;
+
+/* UpscaleDesc (include/render/upscalepass.h:9-14).  The input image's size
+ * is the render resolution, which the reference's Image handle carries. */
+typedef struct UpscaleDesc {
+    Upscalepassparam constants;
+    const float* input;           /* RGBA32F, inputWidth x inputHeight */
+    uint32_t inputWidth;
+    uint32_t inputHeight;
+    float* output;                /* RGBA32F, constants.dimension */
+} UpscaleDesc;
+
 /* ------------------------------------------------------------------------- */
 /* Path tracer pass object (replaces PathTracer : ComputePass<PathTracerParam>,
  * include/render/pathtracer.h:33-50, src/render/pathtracer.cpp:1-94).  The
@@ -373,6 +389,25 @@ int strelka_accumulation_execute(const AccumulationDesc* desc, uint32_t w, uint3
 /* Tonemap::execute (src/render/tonemap.cpp, shaders/tonemap.hlsl:66-88); w = W, h = H. */
 int strelka_tonemap_execute(const TonemapDesc* desc, uint32_t w, uint32_t h,
                             uint64_t frameIndex, void* stream);
+
+/* UpscalePass::execute (src/render/upscalepass.cpp:40-58, shaders/
+ * upscalepass.hlsl:9-21): output[p] = (bilinear sample of the input at
+ * uv = (p + 0.5) * invDimension, clamp to edge; rgb, 1), w x h = the output
+ * dimension.  The reference's sampler is linear with clamp-to-edge
+ * addressing (upscalepass.cpp:12-38); here the filter weights are exact FP32
+ * (a hardware sampler rounds them to its sub-texel precision). */
+int strelka_upscale_execute(const UpscaleDesc* desc, uint32_t w, uint32_t h, uint64_t frameIndex, void* stream);
+
+/* Tonemap followed by the upscale pass and the final blit
+ * (src/render/ptrender.cpp:850-896), fused: each output pixel tonemaps its
+ * four bilinear taps of the render-resolution input and blends them, so the
+ * tonemapped render-resolution image is never stored.  Bit-identical to
+ * strelka_tonemap_execute then strelka_upscale_execute.  outputRGBA8 (may be
+ * NULL) receives the same pixels quantised as the resolve pass does; output
+ * (may be NULL) receives RGBA32F.  tm->dimension is the input size,
+ * up->dimension the output size. */
+int strelka_tonemap_upscale_execute(const Tonemapparam* tm, const float* input, const Upscalepassparam* up,
+                                    float* output, uint8_t* outputRGBA8, void* stream);
 
 /* Fused reduce + accumulate + tonemap in one pass over the sample buffer.
  * Equivalent, bit for bit, to the three passes above run in sequence
@@ -574,6 +609,7 @@ STRELKA_STATIC_ASSERT(sizeof(AccumulationParam) == 416, "AccumulationParam size"
 STRELKA_STATIC_ASSERT(offsetof(AccumulationParam, dimension) == 384, "acc dimension offset");
 STRELKA_STATIC_ASSERT(offsetof(AccumulationParam, alpha) == 400, "acc alpha offset");
 STRELKA_STATIC_ASSERT(sizeof(Tonemapparam) == 16, "Tonemapparam size");
+STRELKA_STATIC_ASSERT(sizeof(Upscalepassparam) == 16, "Upscalepassparam size");
 STRELKA_STATIC_ASSERT(sizeof(BVHNode) == 32, "BVHNode size");
 STRELKA_STATIC_ASSERT(sizeof(Vertex) == 32, "Vertex size");
 STRELKA_STATIC_ASSERT(sizeof(InstanceConstants) == 208, "InstanceConstants size");

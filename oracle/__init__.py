@@ -83,6 +83,7 @@ def load(fast: bool = False) -> C.CDLL:
         "oracle_reduce": (C.c_int, [vp, vp, vp]),
         "oracle_accumulate": (C.c_int, [vp, vp, vp, vp]),
         "oracle_tonemap": (C.c_int, [vp, vp, vp]),
+        "oracle_upscale": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, vp]),
         "oracle_tex_lookup": (None, [vp, f32, f32, vp]),
     }
     for name, (res, args) in sigs.items():
@@ -173,6 +174,15 @@ def accumulate(param, inp: np.ndarray, hist: np.ndarray) -> np.ndarray:
     out = np.zeros_like(inp, dtype=np.float32)
     lib.oracle_accumulate(C.byref(param), _ptr(np.ascontiguousarray(inp, np.float32)),
                           _ptr(np.ascontiguousarray(hist, np.float32)), _ptr(out))
+    return out
+
+
+def upscale(param, inp: np.ndarray, in_w: int, in_h: int) -> np.ndarray:
+    """upscalepass.hlsl:9-21; inp is (in_h * in_w * 4) RGBA32F, param an
+    Upscalepassparam with the output size."""
+    lib = load()
+    out = np.zeros(param.dimension[0] * param.dimension[1] * 4, np.float32)
+    lib.oracle_upscale(C.byref(param), _ptr(np.ascontiguousarray(inp, np.float32)), in_w, in_h, _ptr(out))
     return out
 
 

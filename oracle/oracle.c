@@ -1717,3 +1717,36 @@ int oracle_tonemap(const Tonemapparam* p, const float* in, float* out)
     }
     return 0;
 }
+
+/* upscalepass.hlsl:9-21: uv = (pixel + 0.5) * invDimension; SampleLevel with
+ * a linear filter and clamp-to-edge addressing (upscalepass.cpp:12-38):
+ * texel-space position uv * size - 0.5, the four clamped neighbours and the
+ * fractional weights, blended in a fixed order; rgb kept, alpha 1. */
+int oracle_upscale(const Upscalepassparam* p, const float* in, uint32_t inW, uint32_t inH, float* out)
+{
+    const uint32_t W = (uint32_t)p->dimension[0], H = (uint32_t)p->dimension[1];
+    for (uint32_t py = 0; py < H; ++py)
+        for (uint32_t px = 0; px < W; ++px) {
+            const float u = ((float)px + 0.5f) * p->invDimension[0];
+            const float v = ((float)py + 0.5f) * p->invDimension[1];
+            const float fx = u * (float)inW - 0.5f;
+            const float fy = v * (float)inH - 0.5f;
+            const float flx = floorf(fx), fly = floorf(fy);
+            const float a = fx - flx, b = fy - fly;
+            int x0 = (int)flx, y0 = (int)fly, x1 = x0 + 1, y1 = y0 + 1;
+            const int mx = (int)inW - 1, my = (int)inH - 1;
+            x0 = x0 < 0 ? 0 : (x0 > mx ? mx : x0);
+            x1 = x1 < 0 ? 0 : (x1 > mx ? mx : x1);
+            y0 = y0 < 0 ? 0 : (y0 > my ? my : y0);
+            y1 = y1 < 0 ? 0 : (y1 > my ? my : y1);
+            const float w00 = (1.0f - a) * (1.0f - b), w10 = a * (1.0f - b), w01 = (1.0f - a) * b, w11 = a * b;
+            const float* c00 = in + 4 * ((size_t)y0 * inW + x0);
+            const float* c10 = in + 4 * ((size_t)y0 * inW + x1);
+            const float* c01 = in + 4 * ((size_t)y1 * inW + x0);
+            const float* c11 = in + 4 * ((size_t)y1 * inW + x1);
+            float* o = out + 4 * ((size_t)py * W + px);
+            for (int c = 0; c < 3; ++c) o[c] = ((c00[c] * w00 + c10[c] * w10) + c01[c] * w01) + c11[c] * w11;
+            o[3] = 1.0f;
+        }
+    return 0;
+}

@@ -111,6 +111,9 @@ int oracle_accumulate(const AccumulationParam* p, const float* input, const floa
                       float* output);
 /* tonemap.hlsl:9-88 */
 int oracle_tonemap(const Tonemapparam* p, const float* input, float* output);
+/* upscalepass.hlsl:9-21 with the pass's linear clamp-to-edge sampler
+ * (upscalepass.cpp:12-38); input RGBA32F inW x inH, output p->dimension. */
+int oracle_upscale(const Upscalepassparam* p, const float* input, uint32_t inW, uint32_t inH, float* output);
 
 /* texture lookup, mdl_runtime.hlsl:173-208 (REPEAT, no crop) */
 void oracle_tex_lookup(const OracleTexture* t, float u, float v, float out[4]);

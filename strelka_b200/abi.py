@@ -180,6 +180,15 @@ class TonemapDesc(C.Structure):
     _fields_ = [("constants", Tonemapparam), ("input", vp), ("output", vp)]
 
 
+class Upscalepassparam(C.Structure):
+    _fields_ = [("dimension", C.c_int32 * 2), ("invDimension", C.c_float * 2)]
+
+
+class UpscaleDesc(C.Structure):
+    _fields_ = [("constants", Upscalepassparam), ("input", vp), ("inputWidth", C.c_uint32), ("inputHeight", C.c_uint32),
+                ("output", vp)]
+
+
 class StrelkaPathTracerConfig(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("chunkPaths", C.c_uint32), ("blockSize", C.c_uint32), ("flags", C.c_uint32),
                 ("queueChunk", C.c_uint32), ("pad", C.c_uint32 * 3)]
@@ -272,6 +281,8 @@ SIGNATURES = {
     "strelka_reduction_execute": (C.c_int, [C.POINTER(ReductionDesc), C.c_uint32, C.c_uint32, C.c_uint64, vp]),
     "strelka_accumulation_execute": (C.c_int, [C.POINTER(AccumulationDesc), C.c_uint32, C.c_uint32, C.c_uint64, vp]),
     "strelka_tonemap_execute": (C.c_int, [C.POINTER(TonemapDesc), C.c_uint32, C.c_uint32, C.c_uint64, vp]),
+    "strelka_upscale_execute": (C.c_int, [C.POINTER(UpscaleDesc), C.c_uint32, C.c_uint32, C.c_uint64, vp]),
+    "strelka_tonemap_upscale_execute": (C.c_int, [C.POINTER(Tonemapparam), vp, C.POINTER(Upscalepassparam), vp, vp, vp]),
     "strelka_resolve_execute": (C.c_int, [C.POINTER(PathTracerParam), vp, C.c_int, C.POINTER(AccumulationParam), vp,
                                           vp, C.POINTER(Tonemapparam), vp, vp, vp]),
     "strelka_trace_execute": (C.c_int, [vp, C.POINTER(TraceDesc), vp]),
@@ -313,7 +324,8 @@ SIGNATURES = {
 
 LAYOUT_CHECK = [PathTracerParam, AccumulationParam, Tonemapparam, BVHNode, Vertex, InstanceConstants, UniformLight,
                 MdlMaterial, Mdl_resource_info, Ray, Hit, BVHInputPosition, StrelkaMaterialArgs, StrelkaTexture,
-                StrelkaEnvMap, PathTracerDesc, ReductionDesc, AccumulationDesc, TonemapDesc, TraceDesc,
+                StrelkaEnvMap, PathTracerDesc, ReductionDesc, AccumulationDesc, TonemapDesc, Upscalepassparam,
+                UpscaleDesc, TraceDesc,
                 StrelkaPathTracerConfig, StrelkaNrcRecord, StrelkaNrcConfig, StrelkaNrcRenderConfig,
                 StrelkaBatchConfig, StrelkaBatchTuneEntry]
 

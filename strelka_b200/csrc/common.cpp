@@ -49,6 +49,8 @@ extern "C" size_t strelka_sizeof(const char* name)
     SB_SZ(ReductionDesc)
     SB_SZ(AccumulationDesc)
     SB_SZ(TonemapDesc)
+    SB_SZ(Upscalepassparam)
+    SB_SZ(UpscaleDesc)
     SB_SZ(TraceDesc)
     SB_SZ(StrelkaPathTracerConfig)
     SB_SZ(StrelkaNrcRecord)

@@ -118,6 +118,73 @@ __global__ void k_resolve(const float* __restrict__ sb, int spp, uint32_t npix, 
     }
 }
 
+// Bilinear taps of the upscale pass (upscalepass.hlsl:17-19 with the
+// clamp-to-edge linear sampler of upscalepass.cpp:12-38): the output pixel's
+// uv in the input's texel space, the four clamped texel indices and the
+// fractional weights.
+struct Taps {
+    uint32_t i00, i10, i01, i11;
+    float w00, w10, w01, w11;
+};
+
+__device__ __forceinline__ Taps upscale_taps(uint32_t px, uint32_t py, float invW, float invH, int inW, int inH)
+{
+    const float u = ((float)px + 0.5f) * invW;
+    const float v = ((float)py + 0.5f) * invH;
+    const float fx = u * (float)inW - 0.5f;
+    const float fy = v * (float)inH - 0.5f;
+    const float flx = floorf(fx), fly = floorf(fy);
+    const float a = fx - flx, b = fy - fly;
+    const int x0 = min(max((int)flx, 0), inW - 1), x1 = min(max((int)flx + 1, 0), inW - 1);
+    const int y0 = min(max((int)fly, 0), inH - 1), y1 = min(max((int)fly + 1, 0), inH - 1);
+    Taps t;
+    t.i00 = (uint32_t)y0 * (uint32_t)inW + (uint32_t)x0;
+    t.i10 = (uint32_t)y0 * (uint32_t)inW + (uint32_t)x1;
+    t.i01 = (uint32_t)y1 * (uint32_t)inW + (uint32_t)x0;
+    t.i11 = (uint32_t)y1 * (uint32_t)inW + (uint32_t)x1;
+    t.w00 = (1.0f - a) * (1.0f - b);
+    t.w10 = a * (1.0f - b);
+    t.w01 = (1.0f - a) * b;
+    t.w11 = a * b;
+    return t;
+}
+
+__device__ __forceinline__ v3 blend(const Taps& t, v3 c00, v3 c10, v3 c01, v3 c11)
+{
+    return V(((c00.x * t.w00 + c10.x * t.w10) + c01.x * t.w01) + c11.x * t.w11,
+             ((c00.y * t.w00 + c10.y * t.w10) + c01.y * t.w01) + c11.y * t.w11,
+             ((c00.z * t.w00 + c10.z * t.w10) + c01.z * t.w01) + c11.z * t.w11);
+}
+
+__global__ void k_upscale(const float4* __restrict__ in, int inW, int inH, float4* __restrict__ out, uint32_t outW,
+                          uint32_t outH, float invW, float invH)
+{
+    const uint32_t n = outW * outH;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Taps t = upscale_taps(i % outW, i / outW, invW, invH, inW, inH);
+        const v3 c = blend(t, xyz(__ldg(&in[t.i00])), xyz(__ldg(&in[t.i10])), xyz(__ldg(&in[t.i01])), xyz(__ldg(&in[t.i11])));
+        out[i] = make_float4(c.x, c.y, c.z, 1.0f);
+    }
+}
+
+// Tonemap of each tap (as k_tonemap computes it) then the upscale blend.
+__global__ void k_tonemap_upscale(const float4* __restrict__ in, int inW, int inH, uint32_t tmType, float4* __restrict__ out,
+                                  uchar4* __restrict__ out8, uint32_t outW, uint32_t outH, float invW, float invH)
+{
+    const uint32_t n = outW * outH;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Taps t = upscale_taps(i % outW, i / outW, invW, invH, inW, inH);
+        v3 c00, c10, c01, c11;
+        tonemap_pixel(tmType, xyz(__ldg(&in[t.i00])), c00);
+        tonemap_pixel(tmType, xyz(__ldg(&in[t.i10])), c10);
+        tonemap_pixel(tmType, xyz(__ldg(&in[t.i01])), c01);
+        tonemap_pixel(tmType, xyz(__ldg(&in[t.i11])), c11);
+        const v3 c = blend(t, c00, c10, c01, c11);
+        if (out) out[i] = make_float4(c.x, c.y, c.z, 1.0f);
+        if (out8) out8[i] = make_uchar4(to_u8(c.x), to_u8(c.y), to_u8(c.z), 255);
+    }
+}
+
 int grid_for(uint32_t n)
 {
     int dev = 0, sms = 148;
@@ -211,6 +278,49 @@ extern "C" int strelka_resolve_execute(const PathTracerParam* pp, const float* s
                                               wH, wN, reinterpret_cast<float4*>(accOutput), tp->tonemapperType,
                                               reinterpret_cast<float4*>(tonemapOutput),
                                               reinterpret_cast<uchar4*>(tonemapRGBA8));
+    SB_CUDA_TRY(cudaGetLastError());
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_upscale_execute(const UpscaleDesc* d, uint32_t w, uint32_t h, uint64_t frameIndex, void* stream)
+{
+    (void)frameIndex;
+    if (!d || !d->input || !d->output) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    const Upscalepassparam& p = d->constants;
+    if (p.dimension[0] <= 0 || p.dimension[1] <= 0 || d->inputWidth == 0 || d->inputHeight == 0)
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "bad dimension");
+    if ((int64_t)w != p.dimension[0] || (int64_t)h != p.dimension[1])
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "w,h must equal the output dimension");
+    if ((uint64_t)p.dimension[0] * (uint64_t)p.dimension[1] > 0xFFFFFFFFull ||
+        (uint64_t)d->inputWidth * d->inputHeight > 0xFFFFFFFFull || d->inputWidth > 0x7FFFFFFFu || d->inputHeight > 0x7FFFFFFFu)
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "image too large");
+    if (!aligned16(d->input) || !aligned16(d->output)) return fail(STRELKA_ERR_INVALID_ARGUMENT, "images must be 16-byte aligned");
+    const uint32_t n = (uint32_t)p.dimension[0] * (uint32_t)p.dimension[1];
+    k_upscale<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const float4*>(d->input), (int)d->inputWidth, (int)d->inputHeight,
+        reinterpret_cast<float4*>(d->output), (uint32_t)p.dimension[0], (uint32_t)p.dimension[1], p.invDimension[0],
+        p.invDimension[1]);
+    SB_CUDA_TRY(cudaGetLastError());
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_tonemap_upscale_execute(const Tonemapparam* tm, const float* input, const Upscalepassparam* up,
+                                               float* output, uint8_t* outputRGBA8, void* stream)
+{
+    if (!tm || !input || !up || (!output && !outputRGBA8)) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (tm->dimension[0] <= 0 || tm->dimension[1] <= 0 || up->dimension[0] <= 0 || up->dimension[1] <= 0)
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "bad dimension");
+    if (tm->tonemapperType > 2) return fail(STRELKA_ERR_INVALID_ARGUMENT, "unknown tonemapper %u", tm->tonemapperType);
+    if ((uint64_t)up->dimension[0] * (uint64_t)up->dimension[1] > 0xFFFFFFFFull ||
+        (uint64_t)tm->dimension[0] * (uint64_t)tm->dimension[1] > 0xFFFFFFFFull)
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "image too large");
+    if (!aligned16(input) || (output && !aligned16(output)) || (outputRGBA8 && (reinterpret_cast<uintptr_t>(outputRGBA8) & 3)))
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "misaligned image");
+    const uint32_t n = (uint32_t)up->dimension[0] * (uint32_t)up->dimension[1];
+    k_tonemap_upscale<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const float4*>(input), tm->dimension[0], tm->dimension[1], tm->tonemapperType,
+        reinterpret_cast<float4*>(output), reinterpret_cast<uchar4*>(outputRGBA8), (uint32_t)up->dimension[0],
+        (uint32_t)up->dimension[1], up->invDimension[0], up->invDimension[1]);
     SB_CUDA_TRY(cudaGetLastError());
     return STRELKA_OK;
 }

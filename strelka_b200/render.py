@@ -7,6 +7,7 @@ h, frameIndex)`` (include/render/computepass.h:8-164):
 * ``ReductionPass``  include/render/reduction.h, src/render/reduction.cpp
 * ``Accumulation``   include/render/accumulation.h, src/render/accumulation.cpp
 * ``Tonemap``        include/render/tonemap.h, src/render/tonemap.cpp
+* ``UpscalePass``    include/render/upscalepass.h, src/render/upscalepass.cpp
 
 The classes below keep those names, descriptor contents and argument meaning;
 a CUDA stream (an int handle, 0 = the legacy default stream) stands in for
@@ -339,6 +340,25 @@ class Tonemap:
 
     def execute(self, desc: abi.TonemapDesc, w: int, h: int, frame_index: int = 0, stream=None) -> None:
         abi.check(abi.load().strelka_tonemap_execute(C.byref(desc), w, h, frame_index, _stream_handle(stream)))
+
+
+class UpscalePass:
+    """UpscalePass (shaders/upscalepass.hlsl:9-21): bilinear, clamp to edge."""
+
+    def execute(self, desc: abi.UpscaleDesc, w: int, h: int, frame_index: int = 0, stream=None) -> None:
+        abi.check(abi.load().strelka_upscale_execute(C.byref(desc), w, h, frame_index, _stream_handle(stream)))
+
+
+def upscale_param(width: int, height: int) -> abi.Upscalepassparam:
+    """The constants PtRender::drawFrame fills for the upscale pass
+    (src/render/ptrender.cpp:871-876): the output size and its inverse."""
+    return abi.Upscalepassparam((width, height), (1.0 / width, 1.0 / height))
+
+
+def tonemap_upscale(tm_param, inp, up_param, out=None, out_rgba8=None, stream=None) -> None:
+    """Tonemap + upscale (+ the final 8-bit blit) fused (strelka_tonemap_upscale_execute)."""
+    abi.check(abi.load().strelka_tonemap_upscale_execute(C.byref(tm_param), ptr(inp), C.byref(up_param), ptr(out),
+                                                         ptr(out_rgba8), _stream_handle(stream)))
 
 
 def resolve(pt_param, sample_buffer, tm_param, acc_param=None, history=None, acc_out=None, tonemap_out=None,

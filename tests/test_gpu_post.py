@@ -96,3 +96,57 @@ def test_bad_arguments(cuda, data):
     with pytest.raises(abi.StrelkaError) as e:
         ReductionPass().execute(d, W * H + 1, 1, 0)
     assert e.value.code == abi.ERR_INVALID_ARGUMENT
+
+
+# upscale pass (upscalepass.hlsl:9-21) and the fused tonemap + upscale + 8-bit blit
+UPSCALE_SIZES = [(37, 23, 74, 46), (37, 23, 1920 // 20, 1080 // 20), (64, 32, 64, 32), (40, 30, 17, 11)]
+
+
+@pytest.mark.parametrize("sizes", UPSCALE_SIZES)
+def test_upscale(cuda, sizes):
+    from strelka_b200.render import UpscalePass, upscale_param
+
+    iw, ih, ow, oh = sizes
+    rng = np.random.default_rng(iw * 7 + ow)
+    img = np.concatenate([rng.gamma(0.7, 1.0, (iw * ih, 3)), np.ones((iw * ih, 1))], 1).astype(np.float32).ravel()
+    src = dev(cuda, img)
+    out = cuda.full((ow * oh * 4,), -1.0, dtype=cuda.float32, device="cuda")
+    up = upscale_param(ow, oh)
+    UpscalePass().execute(abi.UpscaleDesc(up, ptr(src), iw, ih, ptr(out)), ow, oh, 0)
+    cuda.cuda.synchronize()
+    assert np.array_equal(host(out).view(np.uint32), oracle.upscale(up, img, iw, ih).view(np.uint32))
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+@pytest.mark.parametrize("sizes", UPSCALE_SIZES[:2])
+def test_tonemap_upscale_equals_sequence(cuda, kind, sizes):
+    from strelka_b200.render import tonemap_upscale, upscale_param
+
+    iw, ih, ow, oh = sizes
+    rng = np.random.default_rng(kind + iw)
+    img = np.concatenate([rng.gamma(0.7, 1.0, (iw * ih, 3)), np.ones((iw * ih, 1))], 1).astype(np.float32).ravel()
+    tp = tonemap_param(iw, ih, kind)
+    up = upscale_param(ow, oh)
+    expect = oracle.upscale(up, oracle.tonemap(tp, img), iw, ih)
+    out = cuda.zeros(ow * oh * 4, dtype=cuda.float32, device="cuda")
+    out8 = cuda.zeros(ow * oh * 4, dtype=cuda.uint8, device="cuda")
+    tonemap_upscale(tp, dev(cuda, img), up, out, out8)
+    cuda.cuda.synchronize()
+    got = host(out)
+    assert np.array_equal(got.view(np.uint32), expect.view(np.uint32))
+    q = np.clip(expect.reshape(-1, 4)[:, :3], 0, 1) * np.float32(255) + np.float32(0.5)
+    assert np.array_equal(host(out8).reshape(-1, 4)[:, :3], q.astype(np.int32).astype(np.uint8))
+    assert (host(out8).reshape(-1, 4)[:, 3] == 255).all()
+
+
+def test_upscale_bad_arguments(cuda):
+    from strelka_b200.render import UpscalePass, tonemap_upscale, upscale_param
+
+    buf = cuda.zeros(64, dtype=cuda.float32, device="cuda")
+    up = upscale_param(4, 4)
+    with pytest.raises(abi.StrelkaError):
+        UpscalePass().execute(abi.UpscaleDesc(up, ptr(buf), 4, 4, ptr(buf)), 5, 4, 0)  # w != dimension
+    with pytest.raises(abi.StrelkaError):
+        UpscalePass().execute(abi.UpscaleDesc(up, ptr(buf), 0, 4, ptr(buf)), 4, 4, 0)
+    with pytest.raises(abi.StrelkaError):
+        tonemap_upscale(tonemap_param(4, 4, 9), buf, up, buf)  # unknown tonemapper

@@ -217,3 +217,30 @@ def test_reduce_order():
     for s in range(3):
         r = f32(r + inv * sb[3 * s])
     assert out[0] == r and out[3] == 1.0
+
+
+def _up(w, h):
+    from strelka_b200 import abi
+    return abi.Upscalepassparam((w, h), (np.float32(1.0) / np.float32(w), np.float32(1.0) / np.float32(h)))
+
+
+def test_upscale_known_answers():
+    # same size: every output centre lands on an input texel centre, exactly
+    # when 1/size is exact in FP32 (powers of two), within rounding otherwise
+    rng = np.random.default_rng(4)
+    img = rng.uniform(0, 3, (4 * 8 * 4)).astype(np.float32)
+    out = oracle.upscale(_up(8, 4), img, 8, 4)
+    a, b = img.reshape(-1, 4), out.reshape(-1, 4)
+    assert np.array_equal(b[:, :3], a[:, :3]) and (b[:, 3] == 1).all()
+    img = rng.uniform(0, 3, (5 * 7 * 4)).astype(np.float32)
+    out = oracle.upscale(_up(7, 5), img, 7, 5)
+    assert np.allclose(out.reshape(-1, 4)[:, :3], img.reshape(-1, 4)[:, :3], rtol=0, atol=1e-5)
+    # a constant image stays constant at any size
+    c = np.tile(np.array([0.25, 0.5, 2.0, 7.0], np.float32), 6 * 4)
+    out = oracle.upscale(_up(13, 9), c, 6, 4).reshape(-1, 4)
+    assert np.allclose(out[:, :3], [0.25, 0.5, 2.0], rtol=1e-6, atol=0)
+    # 2x1 ramp [0, 1] upscaled to 4x2: centres at texel positions -0.25, 0.25, 0.75, 1.25
+    ramp = np.array([0, 0, 0, 1, 1, 1, 1, 1], np.float32)
+    out = oracle.upscale(_up(4, 2), ramp, 2, 1).reshape(2, 4, 4)
+    assert np.array_equal(out[0, :, 0], np.array([0, 0.25, 0.75, 1], np.float32))
+    assert np.array_equal(out[1, :, 0], out[0, :, 0])
