@@ -510,6 +510,34 @@ int strelka_nrc_set_params(StrelkaNrc* nrc, const float* mlp, const float* grid)
 int strelka_nrc_info(StrelkaNrc* nrc, uint32_t* numMlpParams, uint64_t* numGridParams, int32_t* levelRes);
 
 /* ------------------------------------------------------------------------- */
+/* BVH construction on the GPU (an extension: BvhBuilder::build,
+ * src/render/bvh.cpp:107-254, runs Embree on the host).  A linear BVH over
+ * 63-bit Morton codes of the triangle centroids, emitted in the same
+ * flattened depth-first layout as strelka_bvh_build (one triangle per leaf,
+ * 2n-1 nodes, escape indices, +1e-6 padding of the max corner), so every
+ * traversal entry point reads it unchanged.  Faster to build than the host
+ * SAH builder, slower to trace.  The builder object keeps its scratch
+ * memory between builds; calls on one builder must not overlap. */
+typedef struct StrelkaBvhBuilder StrelkaBvhBuilder;
+
+int strelka_bvh_builder_create(StrelkaBvhBuilder** out);
+int strelka_bvh_builder_destroy(StrelkaBvhBuilder* builder);
+/* positions: device array of numPositions corners, 3 per triangle, as
+ * createBvhBuffer fills them (src/render/ptrender.cpp:460-511); nodes:
+ * device array of nodeCapacity >= 2*numPositions/3 - 1 nodes.  Stream
+ * ordered; *numNodes is set on return. */
+int strelka_bvh_build_device(StrelkaBvhBuilder* builder, const BVHInputPosition* positions, uint32_t numPositions,
+                             BVHNode* nodes, uint32_t nodeCapacity, uint32_t* numNodes, void* stream);
+/* The same from the scene's own device buffers: every instance's triangles
+ * (indexOffset, indexCount) transformed by objectToWorld on the device, as
+ * createBvhBuffer does on the host.  Reads the instance table to the host
+ * and synchronises the stream once. */
+int strelka_bvh_build_scene_device(StrelkaBvhBuilder* builder, const Vertex* vb, uint32_t numVertices,
+                                   const uint32_t* ib, uint32_t numIndices, const InstanceConstants* instances,
+                                   uint32_t numInstances, BVHNode* nodes, uint32_t nodeCapacity, uint32_t* numNodes,
+                                   void* stream);
+
+/* ------------------------------------------------------------------------- */
 /* Batched rendering (an extension; the reference renders one view per
  * PathTracer::execute, src/render/pathtracer.cpp:50-59).  Many scene/camera
  * jobs of uneven resolution, sample count, depth and triangle count are

@@ -308,6 +308,11 @@ SIGNATURES = {
     "strelka_batch_info": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "strelka_camera_lookat": (C.c_int, [C.POINTER(PathTracerParam), C.c_uint32, C.c_uint32, C.POINTER(C.c_float),
                                         C.POINTER(C.c_float), C.c_float]),
+    "strelka_bvh_builder_create": (C.c_int, [C.POINTER(vp)]),
+    "strelka_bvh_builder_destroy": (C.c_int, [vp]),
+    "strelka_bvh_build_device": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(C.c_uint32), vp]),
+    "strelka_bvh_build_scene_device": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_uint32,
+                                                 C.POINTER(C.c_uint32), vp]),
     "strelka_bvh_build": (C.c_int, [C.POINTER(BVHInputPosition), C.c_uint32, C.POINTER(C.POINTER(BVHNode)),
                                     C.POINTER(C.c_uint32)]),
     "strelka_host_free": (None, [vp]),

@@ -133,6 +133,53 @@ class DeviceScene:
         return d
 
 
+class BvhBuilder:
+    """BVH construction on the GPU (strelka_bvh_build_*_device): a linear BVH
+    in the flattened depth-first layout of the host builder."""
+
+    def __init__(self):
+        self.lib = abi.load()
+        h = C.c_void_p()
+        abi.check(self.lib.strelka_bvh_builder_create(C.byref(h)))
+        self.handle = h
+
+    def build_scene(self, ds: "DeviceScene", stream=None):
+        """Nodes (a uint8 CUDA tensor, 32 bytes per node) over the scene's own
+        device buffers: every instance's triangles in world space."""
+        torch = _torch()
+        hs = ds.hs
+        counts = hs.instances.view(np.int32).reshape(-1, 52)[:, 50] if hs.instances.size else np.zeros(0, np.int32)
+        tris = int(counts.astype(np.int64).sum()) // 3  # every instance's triangles
+        cap = max(2 * tris - 1, 1)
+        nodes = torch.empty(cap * 32, dtype=torch.uint8, device=ds.device)
+        n = C.c_uint32()
+        abi.check(self.lib.strelka_bvh_build_scene_device(self.handle, ptr(ds.vb), hs.num_vertices, ptr(ds.ib), hs.ib.size,
+                                                          ptr(ds.instances), hs.num_instances, ptr(nodes), cap,
+                                                          C.byref(n), _stream_handle(stream)))
+        return nodes[:n.value * 32]
+
+    def build(self, positions, num_positions: int, stream=None):
+        """Nodes over a device array of BVHInputPosition (3 per triangle)."""
+        torch = _torch()
+        cap = max(2 * (num_positions // 3) - 1, 1)
+        nodes = torch.empty(cap * 32, dtype=torch.uint8, device="cuda")
+        n = C.c_uint32()
+        abi.check(self.lib.strelka_bvh_build_device(self.handle, ptr(positions), num_positions, ptr(nodes), cap,
+                                                    C.byref(n), _stream_handle(stream)))
+        return nodes[:n.value * 32]
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.strelka_bvh_builder_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class PathTracer:
     """PathTracer pass (include/render/pathtracer.h:33-50)."""
 
