@@ -605,8 +605,10 @@ __global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, P
 
 // ---------------------------------------------------------------------------
 // Ray-query microbenchmark kernels.
+// Resident blocks asked of the ray-query kernel: 8 for closest hit and 9 for
+// any hit measured fastest on the 1M-triangle soup (few spills either way).
 template <bool ANY, bool COUNT, bool REFINE>
-__global__ void __launch_bounds__(kExtendBlock) k_trace(DevScene s, const float4* __restrict__ rays, Hit* __restrict__ hits,
+__global__ void __launch_bounds__(kExtendBlock, ANY ? 9 : 8) k_trace(DevScene s, const float4* __restrict__ rays, Hit* __restrict__ hits,
                                                         uint32_t n, uint32_t* head, uint32_t chunk,
                                                         unsigned long long* counters)
 {
@@ -687,7 +689,7 @@ struct StrelkaPathTracer {
     std::vector<Rec> recs;
     std::vector<cudaEvent_t> eventPool;
     size_t eventsUsed = 0;
-    int extendGrid = 0, shadowGrid = 0, shadeGrid = 0, shadeGridNrc = 0, smallGrid = 0;
+    int extendGrid = 0, shadowGrid = 0, traceGrid = 0, traceGridAny = 0, shadeGrid = 0, shadeGridNrc = 0, smallGrid = 0;
     unsigned long long* visitCounters = nullptr;  // 6 entries (STRELKA_PT_COUNT)
     // radiance cache
     StrelkaNrc* nrc = nullptr;
@@ -929,6 +931,8 @@ extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, 
     }
     pt->extendGrid = occupancy_grid((const void*)k_extend<false>, kExtendBlock, pt->numSMs);
     pt->shadowGrid = occupancy_grid((const void*)k_shadow<false>, kExtendBlock, pt->numSMs);
+    pt->traceGrid = occupancy_grid((const void*)k_trace<false, false, false>, kExtendBlock, pt->numSMs);
+    pt->traceGridAny = occupancy_grid((const void*)k_trace<true, false, false>, kExtendBlock, pt->numSMs);
     pt->shadeGrid = occupancy_grid((const void*)k_shade<false>, kShadeBlock, pt->numSMs);
     pt->shadeGridNrc = occupancy_grid((const void*)k_shade<true>, kShadeBlock, pt->numSMs);
     pt->smallGrid = pt->numSMs * 8;
@@ -1265,7 +1269,7 @@ extern "C" int strelka_trace_execute(StrelkaPathTracer* pt, const TraceDesc* d, 
     const bool any = (d->flags & 1u) != 0;
     const bool cnt = (d->flags & STRELKA_TRACE_COUNT) != 0;
     const bool refine = (d->flags & STRELKA_TRACE_REFINE) != 0;
-    const int grid = std::min<int>((d->numRays + kExtendBlock - 1) / kExtendBlock, pt->extendGrid);
+    const int grid = std::min<int>((d->numRays + kExtendBlock - 1) / kExtendBlock, any ? pt->traceGridAny : pt->traceGrid);
     const float4* rays = reinterpret_cast<const float4*>(d->rays);
     Timer t(pt, KC_EXTEND, st);
     SB_CUDA_TRY(cudaMemsetAsync(pt->traceHead, 0, sizeof(uint32_t), st));
