@@ -538,6 +538,41 @@ int strelka_bvh_build_scene_device(StrelkaBvhBuilder* builder, const Vertex* vb,
                                    void* stream);
 
 /* ------------------------------------------------------------------------- */
+/* Scene ingest: the formats on the host side of the path.  The reference
+ * produces them in its Hydra render delegate; these functions reproduce that
+ * arithmetic so that USD-derived scenes can be replayed here. */
+
+/* packNormal (src/hdStrelka/RenderPass.cpp:50-56): components in [-1, 1]. */
+uint32_t strelka_pack_normal(const float normal[3]);
+/* packUV (src/hdStrelka/RenderPass.cpp:58-64): components in [-10, 10]. */
+uint32_t strelka_pack_uv(const float uv[2]);
+/* The vertex loop of HdStrelkaRenderPass::_BakeMeshInstance
+ * (RenderPass.cpp:66-126): count points and normals (3 floats each), uvs
+ * (2 floats each, may be NULL; v is flipped to 1 - v) into Vertex records;
+ * massCenter (may be NULL) = the mean position. */
+int strelka_bake_vertices(const float* points, const float* normals, const float* uvs, uint32_t count, Vertex* out,
+                          float massCenter[3]);
+/* _BlackbodyTemperatureAsRgb (src/hdStrelka/Light.cpp:59-98). */
+int strelka_blackbody_rgb(float kelvin, float rgb[3]);
+
+/* The USD light parameters HdStrelkaLight::Sync reads (Light.cpp:112-198). */
+typedef struct StrelkaUsdLight {
+    uint32_t type;                   /* 0 rect, 1 disk, 2 sphere */
+    float color[3];
+    uint32_t enableColorTemperature;
+    float colorTemperature;          /* kelvin */
+    float intensity;
+    float exposure;
+    float xform[16];                 /* column-major: xform[4*i + j] = GfMatrix4d[i][j] */
+    float width, height;             /* rect */
+    float radius;                    /* disk, sphere */
+    uint32_t pad;
+} StrelkaUsdLight;
+
+/* HdStrelkaLight::Sync then Scene::updateLight (src/scene/scene.cpp:459-511). */
+int strelka_light_from_usd(const StrelkaUsdLight* light, UniformLight* out);
+
+/* ------------------------------------------------------------------------- */
 /* Batched rendering (an extension; the reference renders one view per
  * PathTracer::execute, src/render/pathtracer.cpp:50-59).  Many scene/camera
  * jobs of uneven resolution, sample count, depth and triangle count are
@@ -638,6 +673,7 @@ STRELKA_STATIC_ASSERT(offsetof(AccumulationParam, dimension) == 384, "acc dimens
 STRELKA_STATIC_ASSERT(offsetof(AccumulationParam, alpha) == 400, "acc alpha offset");
 STRELKA_STATIC_ASSERT(sizeof(Tonemapparam) == 16, "Tonemapparam size");
 STRELKA_STATIC_ASSERT(sizeof(Upscalepassparam) == 16, "Upscalepassparam size");
+STRELKA_STATIC_ASSERT(sizeof(StrelkaUsdLight) == 112, "StrelkaUsdLight size");
 STRELKA_STATIC_ASSERT(sizeof(BVHNode) == 32, "BVHNode size");
 STRELKA_STATIC_ASSERT(sizeof(Vertex) == 32, "Vertex size");
 STRELKA_STATIC_ASSERT(sizeof(InstanceConstants) == 208, "InstanceConstants size");

@@ -189,6 +189,13 @@ class UpscaleDesc(C.Structure):
                 ("output", vp)]
 
 
+class StrelkaUsdLight(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("color", C.c_float * 3), ("enableColorTemperature", C.c_uint32),
+                ("colorTemperature", C.c_float), ("intensity", C.c_float), ("exposure", C.c_float),
+                ("xform", C.c_float * 16), ("width", C.c_float), ("height", C.c_float), ("radius", C.c_float),
+                ("pad", C.c_uint32)]
+
+
 class StrelkaPathTracerConfig(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("chunkPaths", C.c_uint32), ("blockSize", C.c_uint32), ("flags", C.c_uint32),
                 ("queueChunk", C.c_uint32), ("pad", C.c_uint32 * 3)]
@@ -308,6 +315,11 @@ SIGNATURES = {
     "strelka_batch_info": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "strelka_camera_lookat": (C.c_int, [C.POINTER(PathTracerParam), C.c_uint32, C.c_uint32, C.POINTER(C.c_float),
                                         C.POINTER(C.c_float), C.c_float]),
+    "strelka_pack_normal": (C.c_uint32, [C.POINTER(C.c_float)]),
+    "strelka_pack_uv": (C.c_uint32, [C.POINTER(C.c_float)]),
+    "strelka_bake_vertices": (C.c_int, [vp, vp, vp, C.c_uint32, vp, C.POINTER(C.c_float)]),
+    "strelka_blackbody_rgb": (C.c_int, [C.c_float, C.POINTER(C.c_float)]),
+    "strelka_light_from_usd": (C.c_int, [C.POINTER(StrelkaUsdLight), C.POINTER(UniformLight)]),
     "strelka_bvh_builder_create": (C.c_int, [C.POINTER(vp)]),
     "strelka_bvh_builder_destroy": (C.c_int, [vp]),
     "strelka_bvh_build_device": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(C.c_uint32), vp]),
@@ -330,7 +342,7 @@ SIGNATURES = {
 LAYOUT_CHECK = [PathTracerParam, AccumulationParam, Tonemapparam, BVHNode, Vertex, InstanceConstants, UniformLight,
                 MdlMaterial, Mdl_resource_info, Ray, Hit, BVHInputPosition, StrelkaMaterialArgs, StrelkaTexture,
                 StrelkaEnvMap, PathTracerDesc, ReductionDesc, AccumulationDesc, TonemapDesc, Upscalepassparam,
-                UpscaleDesc, TraceDesc,
+                UpscaleDesc, StrelkaUsdLight, TraceDesc,
                 StrelkaPathTracerConfig, StrelkaNrcRecord, StrelkaNrcConfig, StrelkaNrcRenderConfig,
                 StrelkaBatchConfig, StrelkaBatchTuneEntry]
 

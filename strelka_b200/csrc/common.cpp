@@ -51,6 +51,7 @@ extern "C" size_t strelka_sizeof(const char* name)
     SB_SZ(TonemapDesc)
     SB_SZ(Upscalepassparam)
     SB_SZ(UpscaleDesc)
+    SB_SZ(StrelkaUsdLight)
     SB_SZ(TraceDesc)
     SB_SZ(StrelkaPathTracerConfig)
     SB_SZ(StrelkaNrcRecord)
