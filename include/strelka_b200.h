@@ -572,6 +572,16 @@ typedef struct StrelkaUsdLight {
 /* HdStrelkaLight::Sync then Scene::updateLight (src/scene/scene.cpp:459-511). */
 int strelka_light_from_usd(const StrelkaUsdLight* light, UniformLight* out);
 
+/* The MDL runtime's buffer readers (shaders/mdl_runtime.hlsl:24-75), run on
+ * the device over a device buffer (the argument block or the read-only data
+ * segment of PathTracerDesc), one read per (offset, kind): kind 0 float,
+ * 1 double, 2 int, 3 uint, 4 bool.  out[i] receives the value's bits
+ * (zero-extended to 64).  Reads past `bytes` return 0; word reads ignore the
+ * two low bits of the offset, as a ByteAddressBuffer does.  Device code reads
+ * through the same functions (csrc/mdl_runtime.cuh). */
+int strelka_mdl_read(const uint8_t* buffer, uint64_t bytes, const uint32_t* offsets, const uint32_t* kinds, uint32_t n,
+                     uint64_t* out, void* stream);
+
 /* ------------------------------------------------------------------------- */
 /* Batched rendering (an extension; the reference renders one view per
  * PathTracer::execute, src/render/pathtracer.cpp:50-59).  Many scene/camera

@@ -84,6 +84,7 @@ def load(fast: bool = False) -> C.CDLL:
         "oracle_accumulate": (C.c_int, [vp, vp, vp, vp]),
         "oracle_tonemap": (C.c_int, [vp, vp, vp]),
         "oracle_upscale": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, vp]),
+        "oracle_mdl_read": (None, [vp, C.c_uint64, vp, vp, C.c_uint32, vp]),
         "oracle_tex_lookup": (None, [vp, f32, f32, vp]),
     }
     for name, (res, args) in sigs.items():
@@ -174,6 +175,17 @@ def accumulate(param, inp: np.ndarray, hist: np.ndarray) -> np.ndarray:
     out = np.zeros_like(inp, dtype=np.float32)
     lib.oracle_accumulate(C.byref(param), _ptr(np.ascontiguousarray(inp, np.float32)),
                           _ptr(np.ascontiguousarray(hist, np.float32)), _ptr(out))
+    return out
+
+
+def mdl_read(buffer: np.ndarray, offsets: np.ndarray, kinds: np.ndarray) -> np.ndarray:
+    """mdl_runtime.hlsl:24-75 readers over a byte buffer; uint64 bits per read."""
+    lib = load()
+    b = np.ascontiguousarray(buffer, np.uint8)
+    o = np.ascontiguousarray(offsets, np.uint32)
+    k = np.ascontiguousarray(kinds, np.uint32)
+    out = np.zeros(o.size, np.uint64)
+    lib.oracle_mdl_read(_ptr(b), b.size, _ptr(o), _ptr(k), o.size, _ptr(out))
     return out
 
 

@@ -1750,3 +1750,31 @@ int oracle_upscale(const Upscalepassparam* p, const float* in, uint32_t inW, uin
         }
     return 0;
 }
+
+/* mdl_runtime.hlsl:24-75.  Load(offs) of a ByteAddressBuffer reads the word
+ * at offs with the two low bits ignored; past the end it reads 0 (robust
+ * buffer access).  asdouble(lo, hi) puts the first word low; the bool reader
+ * tests the byte at offs within its aligned word. */
+static uint32_t mdl_word(const uint8_t* b, uint64_t bytes, uint32_t offs)
+{
+    uint64_t a = offs & ~3u;
+    uint32_t w = 0;
+    if (b && a + 4 <= bytes) memcpy(&w, b + a, 4);
+    return w;
+}
+
+void oracle_mdl_read(const uint8_t* b, uint64_t bytes, const uint32_t* offs, const uint32_t* kinds, uint32_t n,
+                     uint64_t* out)
+{
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t o = offs[i];
+        uint64_t r = 0;
+        switch (kinds[i]) {
+            case 0: case 2: case 3: r = mdl_word(b, bytes, o); break;
+            case 1: r = (uint64_t)mdl_word(b, bytes, o) | ((uint64_t)mdl_word(b, bytes, o + 4u) << 32); break;
+            case 4: r = (mdl_word(b, bytes, o & ~3u) & (0xffu << (8u * (o & 3u)))) != 0u; break;
+            default: r = 0; break;
+        }
+        out[i] = r;
+    }
+}

@@ -113,6 +113,10 @@ int oracle_accumulate(const AccumulationParam* p, const float* input, const floa
 int oracle_tonemap(const Tonemapparam* p, const float* input, float* output);
 /* upscalepass.hlsl:9-21 with the pass's linear clamp-to-edge sampler
  * (upscalepass.cpp:12-38); input RGBA32F inW x inH, output p->dimension. */
+/* mdl_runtime.hlsl:24-75: ByteAddressBuffer reads (kinds 0 float, 1 double,
+ * 2 int, 3 uint, 4 bool); 0 past the end. */
+void oracle_mdl_read(const uint8_t* buffer, uint64_t bytes, const uint32_t* offsets, const uint32_t* kinds, uint32_t n,
+                     uint64_t* out);
 int oracle_upscale(const Upscalepassparam* p, const float* input, uint32_t inW, uint32_t inH, float* output);
 
 /* texture lookup, mdl_runtime.hlsl:173-208 (REPEAT, no crop) */

@@ -315,6 +315,7 @@ SIGNATURES = {
     "strelka_batch_info": (C.c_int, [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "strelka_camera_lookat": (C.c_int, [C.POINTER(PathTracerParam), C.c_uint32, C.c_uint32, C.POINTER(C.c_float),
                                         C.POINTER(C.c_float), C.c_float]),
+    "strelka_mdl_read": (C.c_int, [vp, C.c_uint64, vp, vp, C.c_uint32, vp, vp]),
     "strelka_pack_normal": (C.c_uint32, [C.POINTER(C.c_float)]),
     "strelka_pack_uv": (C.c_uint32, [C.POINTER(C.c_float)]),
     "strelka_bake_vertices": (C.c_int, [vp, vp, vp, C.c_uint32, vp, C.POINTER(C.c_float)]),

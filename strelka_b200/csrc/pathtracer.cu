@@ -879,6 +879,8 @@ DevScene scene_from_desc(const PathTracerDesc* d, const float4* rec, const float
     s.numMaterials = d->mdl_mdlMaterial ? d->numMaterials : 0;
     s.argBlock = d->mdl_argument_block;
     s.argBlockBytes = d->mdl_argument_block ? d->argBlockBytes : 0;
+    s.roData = d->mdl_ro_data_segment;
+    s.roDataBytes = d->mdl_ro_data_segment ? d->roDataBytes : 0;
     s.materials = d->mdl_mdlMaterial;
     s.resInfos = d->mdl_resource_infos;
     s.numResInfos = d->mdl_resource_infos ? d->numResourceInfos : 0;

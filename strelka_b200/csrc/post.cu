@@ -9,6 +9,7 @@
 #include <cstdint>
 
 #include "common.h"
+#include "mdl_runtime.cuh"
 #include "device_math.cuh"
 
 using namespace sb;
@@ -321,6 +322,41 @@ extern "C" int strelka_tonemap_upscale_execute(const Tonemapparam* tm, const flo
         reinterpret_cast<const float4*>(input), tm->dimension[0], tm->dimension[1], tm->tonemapperType,
         reinterpret_cast<float4*>(output), reinterpret_cast<uchar4*>(outputRGBA8), (uint32_t)up->dimension[0],
         (uint32_t)up->dimension[1], up->invDimension[0], up->invDimension[1]);
+    SB_CUDA_TRY(cudaGetLastError());
+    return STRELKA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// MDL runtime readers over a buffer (mdl_runtime.hlsl:24-75), one read per
+// (offset, kind) pair: kind 0 float, 1 double, 2 int, 3 uint, 4 bool; out[i]
+// receives the value's bits (float/int/uint/bool zero-extended to 64 bits).
+namespace {
+__global__ void k_mdl_read(const uint8_t* base, uint64_t bytes, const uint32_t* __restrict__ offs,
+                           const uint32_t* __restrict__ kinds, uint32_t n, uint64_t* out)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t o = offs[i];
+        uint64_t r = 0;
+        switch (kinds[i]) {
+            case 0: r = __float_as_uint(sb::mdl_read_as_float(base, bytes, o)); break;
+            case 1: r = (uint64_t)__double_as_longlong(sb::mdl_read_as_double(base, bytes, o)); break;
+            case 2: r = (uint32_t)sb::mdl_read_as_int(base, bytes, o); break;
+            case 3: r = sb::mdl_read_as_uint(base, bytes, o); break;
+            case 4: r = sb::mdl_read_as_bool(base, bytes, o) ? 1u : 0u; break;
+            default: r = 0; break;
+        }
+        out[i] = r;
+    }
+}
+}  // namespace
+
+extern "C" int strelka_mdl_read(const uint8_t* buffer, uint64_t bytes, const uint32_t* offsets, const uint32_t* kinds,
+                                uint32_t n, uint64_t* out, void* stream)
+{
+    if (n == 0) return STRELKA_OK;
+    if (!offsets || !kinds || !out) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (buffer && (reinterpret_cast<uintptr_t>(buffer) & 3)) return fail(STRELKA_ERR_INVALID_ARGUMENT, "buffer must be 4-byte aligned");
+    k_mdl_read<<<grid_for(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(buffer, bytes, offsets, kinds, n, out);
     SB_CUDA_TRY(cudaGetLastError());
     return STRELKA_OK;
 }

@@ -36,6 +36,8 @@ struct DevScene {
     uint32_t numMaterials;
     const uint8_t* argBlock;
     uint64_t argBlockBytes;
+    const uint8_t* roData;  // MDL read-only data segment
+    uint64_t roDataBytes;
     const MdlMaterial* materials;
     const Mdl_resource_info* resInfos;
     uint32_t numResInfos;

@@ -150,3 +150,19 @@ def test_upscale_bad_arguments(cuda):
         UpscalePass().execute(abi.UpscaleDesc(up, ptr(buf), 0, 4, ptr(buf)), 4, 4, 0)
     with pytest.raises(abi.StrelkaError):
         tonemap_upscale(tonemap_param(4, 4, 9), buf, up, buf)  # unknown tonemapper
+
+
+def test_mdl_readers_match_oracle(cuda):
+    rng = np.random.default_rng(11)
+    buf = rng.integers(0, 256, 4096, dtype=np.uint8)
+    buf[rng.integers(0, 4096, 500)] = 0  # zero bytes for the bool reader
+    n = 20000
+    offs = rng.integers(0, 4200, n).astype(np.uint32)  # unaligned and past the end too
+    kinds = rng.integers(0, 5, n).astype(np.uint32)
+    expect = oracle.mdl_read(buf, offs, kinds)
+    out = cuda.zeros(n, dtype=cuda.int64, device="cuda")
+    b = to_device(buf)
+    o, k = to_device(offs), to_device(kinds)
+    abi.check(abi.load().strelka_mdl_read(ptr(b), buf.size, ptr(o), ptr(k), n, ptr(out), None))
+    cuda.cuda.synchronize()
+    assert np.array_equal(host(out).view(np.uint64), expect)

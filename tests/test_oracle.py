@@ -244,3 +244,18 @@ def test_upscale_known_answers():
     out = oracle.upscale(_up(4, 2), ramp, 2, 1).reshape(2, 4, 4)
     assert np.array_equal(out[0, :, 0], np.array([0, 0.25, 0.75, 1], np.float32))
     assert np.array_equal(out[1, :, 0], out[0, :, 0])
+
+
+def test_mdl_read_known_answers():
+    buf = np.zeros(16, np.uint8)
+    buf[0:4] = np.frombuffer(np.float32(1.5).tobytes(), np.uint8)
+    buf[4:12] = np.frombuffer(np.float64(-2.25).tobytes(), np.uint8)
+    buf[13] = 7  # a bool in byte 1 of the last word
+    offs = np.array([0, 2, 4, 12, 13, 14, 16, 1000], np.uint32)
+    kinds = np.array([0, 0, 1, 4, 4, 4, 3, 0], np.uint32)
+    r = oracle.mdl_read(buf, offs, kinds)
+    assert np.uint32(r[0]).view(np.float32) == np.float32(1.5)
+    assert r[1] == r[0]  # the two low bits of a word offset are ignored
+    assert np.uint64(r[2]).view(np.float64) == -2.25
+    assert list(r[3:6]) == [0, 1, 0]  # byte 1 of the word is set, bytes 0 and 2 are not
+    assert r[6] == 0 and r[7] == 0  # past the end reads 0
