@@ -357,8 +357,14 @@ __global__ void __launch_bounds__(kSmallBlock) k_sort_scatter(Wave w, int qin, u
 
 // shade: one bounce of shading for every queued path; pushes surviving
 // paths to the other queue and next-event requests to the shadow queue.
+// Shading is latency-bound at the 128 registers it would take; 5 resident
+// blocks (a few spills) hide more of its gathers than 4.
+#ifndef SB_SHADE_MINBLOCKS
+#define SB_SHADE_MINBLOCKS 5
+#endif
+
 template <bool NRC>
-__global__ void __launch_bounds__(kShadeBlock) k_shade(DevScene s, PathTracerParam ubo, Wave w, int qin,
+__global__ void __launch_bounds__(kShadeBlock, SB_SHADE_MINBLOCKS) k_shade(DevScene s, PathTracerParam ubo, Wave w, int qin,
                                                        const uint32_t* order, uint32_t chunk, NrcWave nw)
 {
     const uint32_t count = w.counters[qin];
@@ -685,7 +691,7 @@ struct StrelkaPathTracer {
     // environment descriptor copy
     StrelkaEnvMap env{};
     // profiling
-    struct Rec { int kc; cudaEvent_t a, b; };
+    struct Rec { int kc; cudaEvent_t a, b; uint32_t kernels; };
     std::vector<Rec> recs;
     std::vector<cudaEvent_t> eventPool;
     size_t eventsUsed = 0;
@@ -759,12 +765,14 @@ cudaEvent_t next_event(StrelkaPathTracer* pt)
     return pt->eventPool[pt->eventsUsed++];
 }
 
+// CUDA-event interval around the `kernels` launches of one kernel class.
 struct Timer {
     StrelkaPathTracer* pt;
     int kc;
     cudaStream_t st;
+    uint32_t kernels;
     cudaEvent_t a = nullptr;
-    Timer(StrelkaPathTracer* p, int k, cudaStream_t s) : pt(p), kc(k), st(s)
+    Timer(StrelkaPathTracer* p, int k, cudaStream_t s, uint32_t nk = 1) : pt(p), kc(k), st(s), kernels(nk)
     {
         if (pt->cfg.flags & STRELKA_PT_PROFILE) {
             a = next_event(pt);
@@ -777,7 +785,7 @@ struct Timer {
             cudaEvent_t b = next_event(pt);
             if (b) {
                 cudaEventRecord(b, st);
-                pt->recs.push_back({kc, a, b});
+                pt->recs.push_back({kc, a, b, kernels});
             }
         }
     }
@@ -1121,7 +1129,7 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             }
             const uint32_t* order = nullptr;
             if (sortKeys) {
-                Timer t(pt, KC_SORT, st);
+                Timer t(pt, KC_SORT, st, 3);
                 const int gridK = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, pt->numSMs * 4);
                 k_sort_count<<<gridK, kSmallBlock, 0, st>>>(s, pt->main.w, qin, sortKeys, pt->sortHist, pt->main.keys);
                 k_sort_scan<<<1, 1024, 0, st>>>(pt->sortHist, sortKeys, pt->sortOffsets);
@@ -1214,7 +1222,7 @@ extern "C" int strelka_pathtracer_get_kernel_times(StrelkaPathTracer* pt, void* 
         float t = 0.0f;
         if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
             ms[r.kc] += t;
-            cnt[r.kc] += 1;
+            cnt[r.kc] += r.kernels;
         }
     }
     for (uint32_t i = 0; i < capacity && i < (uint32_t)KC_COUNT; ++i) {
