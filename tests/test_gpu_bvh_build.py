@@ -117,3 +117,22 @@ def test_render_over_gpu_bvh(cuda, gpu_bvh_scenes):
     ref = oracle.pathtrace(view, p)
     assert relmse(got, ref) <= 1e-4
     assert bits_equal_fraction(got, ref) >= 0.999
+
+
+def test_identical_centroids_and_degenerate_triangles(cuda):
+    # every Morton code equal: the radix tree splits by position alone
+    n = 1000
+    tri = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    pos = np.tile(tri, (n, 1)).astype(np.float32)
+    pos[3 * (n // 2):] *= 0.0  # the second half collapses to points (zero-area triangles)
+    raw = np.zeros((3 * n, 5), np.uint32)
+    raw[:, 0:3] = pos.view(np.uint32)
+    raw[:, 3] = 0
+    raw[:, 4] = np.repeat(np.arange(n, dtype=np.uint32), 3)
+    b = BvhBuilder()
+    nodes = b.build(to_device(raw), 3 * n).cpu().numpy()
+    b.close()
+    check_layout(nodes, n)
+    # the root box covers every corner
+    f = nodes.view(np.float32).reshape(-1, 8)
+    assert np.allclose(f[0, 0:3], 0) and np.allclose(f[0, 4:6], 1, atol=1e-5)
