@@ -511,8 +511,9 @@ int strelka_nrc_info(StrelkaNrc* nrc, uint32_t* numMlpParams, uint64_t* numGridP
 
 /* ------------------------------------------------------------------------- */
 /* BVH construction on the GPU (an extension: BvhBuilder::build,
- * src/render/bvh.cpp:107-254, runs Embree on the host).  A linear BVH over
- * 63-bit Morton codes of the triangle centroids, emitted in the same
+ * src/render/bvh.cpp:107-254, runs Embree on the host).  Clustering over
+ * 63-bit Morton codes of the triangle centroids (PLOC, or a linear BVH),
+ * emitted in the same
  * flattened depth-first layout as strelka_bvh_build (one triangle per leaf,
  * 2n-1 nodes, escape indices, +1e-6 padding of the max corner), so every
  * traversal entry point reads it unchanged.  Faster to build than the host
@@ -520,7 +521,15 @@ int strelka_nrc_info(StrelkaNrc* nrc, uint32_t* numMlpParams, uint64_t* numGridP
  * memory between builds; calls on one builder must not overlap. */
 typedef struct StrelkaBvhBuilder StrelkaBvhBuilder;
 
+enum {
+    STRELKA_BVH_LBVH = 0, /* radix tree over the Morton order: fastest build */
+    STRELKA_BVH_PLOC = 1  /* parallel locally-ordered clustering (default): SAH-like trees */
+};
+
 int strelka_bvh_builder_create(StrelkaBvhBuilder** out);
+/* Tree construction of the builder: STRELKA_BVH_PLOC with a neighbour
+ * search radius in [1, 32] (default 16), or STRELKA_BVH_LBVH (radius ignored). */
+int strelka_bvh_builder_set_mode(StrelkaBvhBuilder* builder, uint32_t mode, uint32_t radius);
 int strelka_bvh_builder_destroy(StrelkaBvhBuilder* builder);
 /* positions: device array of numPositions corners, 3 per triangle, as
  * createBvhBuffer fills them (src/render/ptrender.cpp:460-511); nodes:

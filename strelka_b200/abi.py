@@ -41,6 +41,8 @@ FN_GGX_DIELECTRIC = 2
 BATCH_PERSISTENT = 0
 BATCH_WAVEFRONT = 1
 BATCH_MAX_JOBS = 64
+BVH_LBVH = 0
+BVH_PLOC = 1
 MODE_WAVEFRONT = 0
 MODE_MEGAKERNEL = 1
 PT_PROFILE = 1
@@ -323,6 +325,7 @@ SIGNATURES = {
     "strelka_light_from_usd": (C.c_int, [C.POINTER(StrelkaUsdLight), C.POINTER(UniformLight)]),
     "strelka_bvh_builder_create": (C.c_int, [C.POINTER(vp)]),
     "strelka_bvh_builder_destroy": (C.c_int, [vp]),
+    "strelka_bvh_builder_set_mode": (C.c_int, [vp, C.c_uint32, C.c_uint32]),
     "strelka_bvh_build_device": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.POINTER(C.c_uint32), vp]),
     "strelka_bvh_build_scene_device": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_uint32,
                                                  C.POINTER(C.c_uint32), vp]),

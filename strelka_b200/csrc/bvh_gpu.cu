@@ -19,11 +19,20 @@
 //      the bits of the per-instance triangle index in minBounds[0].
 // One triangle per leaf, 2n-1 nodes, as bvh.cpp:169-235 lays them out, so the
 // traversal kernels and the oracle read the result unchanged.
+//
+// The default tree comes from PLOC instead of step 3-4 (Meister and Bittner
+// 2018, "Parallel Locally-Ordered Clustering for Bounding Volume Hierarchy
+// Construction"): over the Morton-sorted clusters, each cluster picks the
+// neighbour within +-radius whose merged box has the least surface area;
+// mutual pairs merge (the lower position becomes the left child), the
+// survivors are compacted in order, and rounds repeat until one cluster is
+// left.  It traces like a SAH tree and still builds in milliseconds.
 #include <algorithm>
 #include <cstring>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "common.h"
 #include "device_math.cuh"
@@ -60,6 +69,16 @@ struct Scratch {
     uint32_t* cbounds;   // 6: centroid bounds (ordered)
     void* cub;
     size_t cubBytes;
+    // PLOC clusters (double-buffered): node id and box per cluster
+    uint32_t* cid[2];
+    float4* clo[2];
+    float4* chi[2];
+    uint32_t* nn;
+    uint32_t* keep;
+    uint32_t* pos;
+    uint32_t* counters;  // [0] next internal node
+    void* scan;
+    size_t scanBytes;
 };
 
 __global__ void k_init_bounds(uint32_t* cb)
@@ -277,6 +296,123 @@ __global__ void __launch_bounds__(kBlock) k_scene_positions(const Vertex* __rest
     }
 }
 
+// ---------------------------------------------------------------------------
+// PLOC
+__device__ __forceinline__ float half_area(float4 l, float4 h)
+{
+    const float dx = h.x - l.x, dy = h.y - l.y, dz = h.z - l.z;
+    return dx * (dy + dz) + dy * dz;
+}
+
+__global__ void __launch_bounds__(kBlock) k_ploc_init(const float4* __restrict__ lo, const float4* __restrict__ hi,
+                                                      const uint32_t* __restrict__ order, uint32_t n, uint32_t* cid,
+                                                      float4* clo, float4* chi, uint32_t* size, uint32_t* parent)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t t = order[k];
+        cid[k] = n - 1 + k;
+        clo[k] = lo[t];
+        chi[k] = hi[t];
+        size[n - 1 + k] = 1;
+        parent[n - 1 + k] = kNone;
+        if (k + 1 < n) parent[k] = kNone;
+    }
+}
+
+// nearest neighbour of every cluster within +-radius (least merged area,
+// ties to the lower position); boxes of a block's window staged in shared memory
+constexpr int kMaxRadius = 32;
+
+__global__ void __launch_bounds__(kBlock) k_ploc_nn(const float4* __restrict__ clo, const float4* __restrict__ chi, uint32_t C,
+                                                    int radius, uint32_t* nn)
+{
+    __shared__ float4 slo[kBlock + 2 * kMaxRadius], shi[kBlock + 2 * kMaxRadius];
+    for (uint32_t base = blockIdx.x * kBlock; base < C; base += gridDim.x * kBlock) {
+        const int first = (int)base - radius;
+        const int span = kBlock + 2 * radius;
+        for (int t = threadIdx.x; t < span; t += kBlock) {
+            const int g = first + t;
+            if (g >= 0 && g < (int)C) {
+                slo[t] = clo[g];
+                shi[t] = chi[g];
+            }
+        }
+        __syncthreads();
+        const uint32_t i = base + threadIdx.x;
+        if (i < C) {
+            const int li = (int)threadIdx.x + radius;
+            const float4 l = slo[li], h = shi[li];
+            float best = INFINITY;
+            uint32_t bj = i;
+            const int j0 = max(0, (int)i - radius), j1 = min((int)C - 1, (int)i + radius);
+            for (int j = j0; j <= j1; ++j) {
+                if (j == (int)i) continue;
+                const float4 ol = slo[j - first], oh = shi[j - first];
+                const float4 ml = make_float4(fminf(l.x, ol.x), fminf(l.y, ol.y), fminf(l.z, ol.z), 0.0f);
+                const float4 mh = make_float4(fmaxf(h.x, oh.x), fmaxf(h.y, oh.y), fmaxf(h.z, oh.z), 0.0f);
+                const float a = half_area(ml, mh);
+                if (a < best) {
+                    best = a;
+                    bj = (uint32_t)j;
+                }
+            }
+            nn[i] = bj;
+        }
+        __syncthreads();
+    }
+}
+
+// mutual nearest neighbours merge in place at the lower position
+__global__ void __launch_bounds__(kBlock) k_ploc_merge(uint32_t C, const uint32_t* __restrict__ nn, uint32_t* cid, float4* clo,
+                                                       float4* chi, uint32_t* keep, uint32_t* counters, uint32_t* child,
+                                                       uint32_t* parent, float4* nlo, float4* nhi, uint32_t* size)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < C; i += gridDim.x * blockDim.x) {
+        const uint32_t j = nn[i];
+        const bool mutual = j != i && nn[j] == i;
+        if (!mutual) {
+            keep[i] = 1;
+            continue;
+        }
+        if (i > j) {
+            keep[i] = 0;
+            continue;
+        }
+        const uint32_t a = cid[i], b = cid[j];
+        const uint32_t node = atomicAdd(&counters[0], 1u);
+        const float4 l0 = clo[i], h0 = chi[i], l1 = clo[j], h1 = chi[j];
+        const float4 ml = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f);
+        const float4 mh = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f);
+        child[2 * node] = a;
+        child[2 * node + 1] = b;
+        parent[a] = node;
+        parent[b] = node;
+        nlo[node] = ml;
+        nhi[node] = mh;
+        size[node] = 1 + size[a] + size[b];
+        cid[i] = node;
+        clo[i] = ml;
+        chi[i] = mh;
+        keep[i] = 1;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_ploc_compact(uint32_t C, const uint32_t* __restrict__ keep,
+                                                         const uint32_t* __restrict__ pos, const uint32_t* __restrict__ cid,
+                                                         const float4* __restrict__ clo, const float4* __restrict__ chi,
+                                                         uint32_t* cid2, float4* clo2, float4* chi2, uint32_t* count)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < C; i += gridDim.x * blockDim.x) {
+        if (keep[i]) {
+            const uint32_t d = pos[i];
+            cid2[d] = cid[i];
+            clo2[d] = clo[i];
+            chi2[d] = chi[i];
+        }
+        if (i == C - 1) *count = pos[i] + keep[i];
+    }
+}
+
 int grid_for(uint32_t n, int sms)
 {
     const uint32_t b = (n + kBlock - 1) / kBlock;
@@ -287,6 +423,8 @@ int grid_for(uint32_t n, int sms)
 
 struct StrelkaBvhBuilder {
     int numSMs = 148;
+    uint32_t mode = STRELKA_BVH_PLOC;
+    uint32_t radius = 16;
     uint32_t cap = 0;  // triangles the scratch holds
     Scratch s{};
     std::vector<void*> allocs;
@@ -328,10 +466,22 @@ int ensure(StrelkaBvhBuilder* b, uint32_t n)
         (rc = salloc(b, &s.codes[1], n)) || (rc = salloc(b, &s.order[0], n)) || (rc = salloc(b, &s.order[1], n)) ||
         (rc = salloc(b, &s.child, 2 * (size_t)n)) || (rc = salloc(b, &s.parent, 2 * (size_t)n)) ||
         (rc = salloc(b, &s.nlo, n)) || (rc = salloc(b, &s.nhi, n)) || (rc = salloc(b, &s.size, 2 * (size_t)n)) ||
-        (rc = salloc(b, &s.arrive, n)) || (rc = salloc(b, &s.cbounds, 8))) {
+        (rc = salloc(b, &s.arrive, n)) || (rc = salloc(b, &s.cbounds, 8)) || (rc = salloc(b, &s.cid[0], n)) ||
+        (rc = salloc(b, &s.cid[1], n)) || (rc = salloc(b, &s.clo[0], n)) || (rc = salloc(b, &s.clo[1], n)) ||
+        (rc = salloc(b, &s.chi[0], n)) || (rc = salloc(b, &s.chi[1], n)) || (rc = salloc(b, &s.nn, n)) ||
+        (rc = salloc(b, &s.keep, n)) || (rc = salloc(b, &s.pos, n)) || (rc = salloc(b, &s.counters, 4))) {
         release(b);
         return rc;
     }
+    size_t scanBytes = 0;
+    SB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scanBytes, s.keep, s.pos, (int)n));
+    uint8_t* scanBuf = nullptr;
+    if ((rc = salloc(b, &scanBuf, scanBytes))) {
+        release(b);
+        return rc;
+    }
+    s.scan = scanBuf;
+    s.scanBytes = scanBytes;
     size_t bytes = 0;
     SB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, bytes, s.codes[0], s.codes[1], s.order[0], s.order[1], (int)n, 0,
                                                 63));
@@ -343,6 +493,39 @@ int ensure(StrelkaBvhBuilder* b, uint32_t n)
     s.cub = cubBuf;
     s.cubBytes = bytes;
     b->cap = n;
+    return STRELKA_OK;
+}
+
+// PLOC rounds over the Morton-sorted leaves; the host reads the cluster count
+// after each round (one synchronisation per round) and stops when one is left
+// or fails when a round makes no progress.
+int ploc(StrelkaBvhBuilder* b, uint32_t n, cudaStream_t st)
+{
+    Scratch& s = b->s;
+    k_ploc_init<<<grid_for(n, b->numSMs), kBlock, 0, st>>>(s.lo, s.hi, s.order[1], n, s.cid[0], s.clo[0], s.chi[0],
+                                                           s.size, s.parent);
+    SB_CUDA_TRY(cudaMemsetAsync(s.counters, 0, 4 * sizeof(uint32_t), st));
+    uint32_t C = n;
+    int cur = 0;
+    const int radius = (int)std::min<uint32_t>(b->radius, (uint32_t)kMaxRadius);
+    for (uint32_t round = 0; C > 1; ++round) {
+        if (round > 4 * n) return fail(STRELKA_ERR_UNSUPPORTED, "PLOC did not converge");
+        const int g = grid_for(C, b->numSMs);
+        k_ploc_nn<<<g, kBlock, 0, st>>>(s.clo[cur], s.chi[cur], C, radius, s.nn);
+        k_ploc_merge<<<g, kBlock, 0, st>>>(C, s.nn, s.cid[cur], s.clo[cur], s.chi[cur], s.keep, s.counters, s.child,
+                                            s.parent, s.nlo, s.nhi, s.size);
+        size_t bytes = s.scanBytes;
+        SB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(s.scan, bytes, s.keep, s.pos, (int)C, st));
+        k_ploc_compact<<<g, kBlock, 0, st>>>(C, s.keep, s.pos, s.cid[cur], s.clo[cur], s.chi[cur], s.cid[cur ^ 1],
+                                              s.clo[cur ^ 1], s.chi[cur ^ 1], s.counters + 1);
+        SB_CUDA_TRY(cudaGetLastError());
+        uint32_t next = 0;
+        SB_CUDA_TRY(cudaMemcpyAsync(&next, s.counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        SB_CUDA_TRY(cudaStreamSynchronize(st));
+        if (next >= C || next == 0) return fail(STRELKA_ERR_INVALID_ARGUMENT, "BVH build made no progress (non-finite positions?)");
+        C = next;
+        cur ^= 1;
+    }
     return STRELKA_OK;
 }
 
@@ -360,13 +543,18 @@ int build(StrelkaBvhBuilder* b, const BVHInputPosition* positions, uint32_t numT
     size_t bytes = s.cubBytes;
     SB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(s.cub, bytes, s.codes[0], s.codes[1], s.order[0], s.order[1], (int)n, 0,
                                                 63, st));
-    if (n > 1) {
-        k_radix_tree<<<grid_for(n - 1, b->numSMs), kBlock, 0, st>>>(s.codes[1], (int)n, s.child, s.parent);
-        SB_CUDA_TRY(cudaMemsetAsync(s.arrive, 0, (size_t)(n - 1) * sizeof(uint32_t), st));
+    if (b->mode == STRELKA_BVH_PLOC && n > 1) {
+        rc = ploc(b, n, st);
+        if (rc) return rc;
     } else {
-        SB_CUDA_TRY(cudaMemsetAsync(s.parent, 0xFF, sizeof(uint32_t), st));
+        if (n > 1) {
+            k_radix_tree<<<grid_for(n - 1, b->numSMs), kBlock, 0, st>>>(s.codes[1], (int)n, s.child, s.parent);
+            SB_CUDA_TRY(cudaMemsetAsync(s.arrive, 0, (size_t)(n - 1) * sizeof(uint32_t), st));
+        } else {
+            SB_CUDA_TRY(cudaMemsetAsync(s.parent, 0xFF, sizeof(uint32_t), st));
+        }
+        k_bottom_up<<<g, kBlock, 0, st>>>(s.lo, s.hi, s.order[1], n, s.child, s.parent, s.nlo, s.nhi, s.size, s.arrive);
     }
-    k_bottom_up<<<g, kBlock, 0, st>>>(s.lo, s.hi, s.order[1], n, s.child, s.parent, s.nlo, s.nhi, s.size, s.arrive);
     k_flatten<<<grid_for(2 * n - 1, b->numSMs), kBlock, 0, st>>>(s.lo, s.hi, s.order[1], n, s.child, s.parent, s.nlo,
                                                                  s.nhi, s.size, nodes);
     SB_CUDA_TRY(cudaGetLastError());
@@ -389,6 +577,17 @@ extern "C" int strelka_bvh_builder_create(StrelkaBvhBuilder** out)
         return fail(STRELKA_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
     }
     *out = b;
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_bvh_builder_set_mode(StrelkaBvhBuilder* b, uint32_t mode, uint32_t radius)
+{
+    if (!b) return fail(STRELKA_ERR_INVALID_ARGUMENT, "builder is NULL");
+    if (mode != STRELKA_BVH_LBVH && mode != STRELKA_BVH_PLOC) return fail(STRELKA_ERR_INVALID_ARGUMENT, "unknown mode %u", mode);
+    if (mode == STRELKA_BVH_PLOC && (radius < 1 || radius > (uint32_t)kMaxRadius))
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "radius must be in [1, %d]", kMaxRadius);
+    b->mode = mode;
+    if (mode == STRELKA_BVH_PLOC) b->radius = radius;
     return STRELKA_OK;
 }
 

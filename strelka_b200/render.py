@@ -137,11 +137,12 @@ class BvhBuilder:
     """BVH construction on the GPU (strelka_bvh_build_*_device): a linear BVH
     in the flattened depth-first layout of the host builder."""
 
-    def __init__(self):
+    def __init__(self, mode: int = abi.BVH_PLOC, radius: int = 16):
         self.lib = abi.load()
         h = C.c_void_p()
         abi.check(self.lib.strelka_bvh_builder_create(C.byref(h)))
         self.handle = h
+        abi.check(self.lib.strelka_bvh_builder_set_mode(h, mode, radius))
 
     def build_scene(self, ds: "DeviceScene", stream=None):
         """Nodes (a uint8 CUDA tensor, 32 bytes per node) over the scene's own

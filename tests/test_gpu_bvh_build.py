@@ -35,15 +35,28 @@ def run_trace(torch, pt, ds, rays, flags):
     return hits.cpu().numpy().view(np.uint32).reshape(n, 5)
 
 
+MODES = [abi.BVH_PLOC, abi.BVH_LBVH]
+
+
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("ntris", [1, 2, 3, 17, 3000])
-def test_layout_from_positions(cuda, ntris):
+def test_layout_from_positions(cuda, ntris, mode):
     s = scenes.soup(ntris, 7)
     raw, n = positions_of(s)
-    b = BvhBuilder()
+    b = BvhBuilder(mode)
     nodes = b.build(to_device(raw), 3 * n)
     check_layout(nodes.cpu().numpy(), n)
     again = b.build(to_device(raw), 3 * n)
     assert np.array_equal(nodes.cpu().numpy(), again.cpu().numpy())  # deterministic
+    b.close()
+
+
+def test_bad_mode(cuda):
+    b = BvhBuilder()
+    with pytest.raises(abi.StrelkaError):
+        abi.check(b.lib.strelka_bvh_builder_set_mode(b.handle, 7, 16))
+    with pytest.raises(abi.StrelkaError):
+        abi.check(b.lib.strelka_bvh_builder_set_mode(b.handle, abi.BVH_PLOC, 0))
     b.close()
 
 
@@ -54,12 +67,13 @@ def test_empty(cuda):
     b.close()
 
 
-def test_scene_build_matches_positions_build(cuda):
+@pytest.mark.parametrize("mode", MODES)
+def test_scene_build_matches_positions_build(cuda, mode):
     # the on-device world transform equals the host's (same arithmetic), so
     # both routes give the same nodes
     s = scenes.cornell(16, 16, sphere_levels=2)
     ds = DeviceScene(s)
-    b = BvhBuilder()
+    b = BvhBuilder(mode)
     a = b.build_scene(ds).cpu().numpy()
     raw, n = positions_of(s)
     c = b.build(to_device(raw), 3 * n).cpu().numpy()
@@ -68,13 +82,13 @@ def test_scene_build_matches_positions_build(cuda):
     b.close()
 
 
-@pytest.fixture(scope="module")
-def gpu_bvh_scenes(cuda):
+@pytest.fixture(scope="module", params=MODES)
+def gpu_bvh_scenes(cuda, request):
     out = []
     for s in (scenes.cornell(24, 16, sphere_levels=4),
               scenes.large(width=20, height=12, instances=3, frequency=16, num_textures=2, tex_size=64, env_width=64,
                            env_height=32, max_depth=6, spp=2, seed=4)):
-        b = BvhBuilder()
+        b = BvhBuilder(request.param)
         nodes = b.build_scene(DeviceScene(s)).cpu().numpy()
         b.close()
         g = dataclasses.replace(s, nodes=nodes)
@@ -119,7 +133,8 @@ def test_render_over_gpu_bvh(cuda, gpu_bvh_scenes):
     assert bits_equal_fraction(got, ref) >= 0.999
 
 
-def test_identical_centroids_and_degenerate_triangles(cuda):
+@pytest.mark.parametrize("mode", MODES)
+def test_identical_centroids_and_degenerate_triangles(cuda, mode):
     # every Morton code equal: the radix tree splits by position alone
     n = 1000
     tri = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
@@ -129,7 +144,7 @@ def test_identical_centroids_and_degenerate_triangles(cuda):
     raw[:, 0:3] = pos.view(np.uint32)
     raw[:, 3] = 0
     raw[:, 4] = np.repeat(np.arange(n, dtype=np.uint32), 3)
-    b = BvhBuilder()
+    b = BvhBuilder(mode)
     nodes = b.build(to_device(raw), 3 * n).cpu().numpy()
     b.close()
     check_layout(nodes, n)
