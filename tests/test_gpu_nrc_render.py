@@ -104,3 +104,30 @@ def test_cache_disabled_is_bit_identical_to_plain(cuda, setup):
     a.close()
     b.close()
     cache.close()
+
+
+def test_chunked_wavefront_with_frozen_cache(cuda, setup):
+    # with training off the cache is fixed, and a frame split into several
+    # wavefront chunks (each with its own queries and inference) must equal
+    # the frame rendered in one chunk, bit for bit
+    s, ds, _, _ = setup
+    lo, hi = s.bounds()
+    cache = RadianceCache(lo, hi, log2_table_size=14, seed=7)
+    rng = np.random.default_rng(0)
+    mlp, grid = cache.params()
+    cache.set_params(None, rng.normal(0, 0.2, grid.size).astype(np.float32))  # a cache that predicts something
+    whole = PathTracer(mode=abi.MODE_WAVEFRONT)
+    parts = PathTracer(mode=abi.MODE_WAVEFRONT, chunk_paths=1000)
+    for pt in (whole, parts):
+        pt.set_nrc(cache, train_paths=0, train_steps=1, diffuse_roughness=0.25)
+    a = frame(cuda, s, ds, whole, 11, spp=2).cpu().numpy()
+    b = frame(cuda, s, ds, parts, 11, spp=2).cpu().numpy()
+    assert whole.device_status() == 0 and parts.device_status() == 0
+    assert np.isfinite(a).all()
+    assert np.array_equal(a, b)
+    plain = PathTracer(mode=abi.MODE_WAVEFRONT)
+    c = frame(cuda, s, ds, plain, 11, spp=2).cpu().numpy()
+    assert not np.array_equal(a, c)  # the cache did take part
+    for pt in (whole, parts, plain):
+        pt.close()
+    cache.close()
