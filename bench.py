@@ -775,6 +775,9 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
         "kernel_ms_per_frame": {k: v[0] / args.steps for k, v in times.items() if v[1]},
+        "kernel_ms_note": "event intervals per kernel class; shadow(k) runs on a second stream beside extend(k+1), "
+                          "so the shadow and sort intervals include time shared with the other stream and the "
+                          "classes sum to more than ms_per_step",
     }
     print(json.dumps(line), flush=True)
 

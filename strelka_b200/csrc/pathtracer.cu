@@ -41,6 +41,10 @@ constexpr uint32_t kDefaultQueueChunk = 32;
 #endif
 // The closest-hit kernel is latency-bound: 9 resident blocks (56 registers,
 // a few spilled) hide more of its dependent fetches than 8 without spills.
+// Shadow queries of bounce k overlap the closest-hit queries of bounce k+1.
+#ifndef SB_OVERLAP_SHADOW
+#define SB_OVERLAP_SHADOW 1
+#endif
 #ifndef SB_EXTEND_MINBLOCKS
 #define SB_EXTEND_MINBLOCKS 9
 #endif
@@ -188,6 +192,11 @@ struct NrcWave {
     float diffuseRoughness;
 };
 
+// Shadow-request count of a bounce: counters[2] on even bounces, [6] on odd
+// ones, so that shadow(k) can read its count while extend(k+1) resets the
+// count shade(k+1) will fill.
+__host__ __device__ __forceinline__ int shadow_count(int qin) { return qin ? 6 : 2; }
+
 __global__ void __launch_bounds__(kSmallBlock) k_generate(PathTracerParam ubo, Wave w, uint64_t first, uint32_t n)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -195,6 +204,7 @@ __global__ void __launch_bounds__(kSmallBlock) k_generate(PathTracerParam ubo, W
         w.counters[1] = 0;
         w.counters[2] = 0;
         w.counters[3] = 0;  // extend's work-queue head
+        w.counters[6] = 0;
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         PathState ps;
@@ -218,9 +228,9 @@ __global__ void __launch_bounds__(kExtendBlock, SB_EXTEND_MINBLOCKS) k_extend(De
 {
     const uint32_t count = w.counters[qin];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        w.counters[qin ^ 1] = 0;  // consumed by shade(k-1); refilled by shade(k)
-        w.counters[2] = 0;        // consumed by shadow(k-1); refilled by shade(k)
-        w.counters[4] = 0;        // shade's work-queue head
+        w.counters[qin ^ 1] = 0;           // consumed by shade(k-1); refilled by shade(k)
+        w.counters[shadow_count(qin)] = 0; // consumed by shadow(k-2); refilled by shade(k)
+        w.counters[4] = 0;                 // shade's work-queue head
     }
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
     uint32_t stackN[SB_STACK];
@@ -368,7 +378,10 @@ __global__ void __launch_bounds__(kShadeBlock, SB_SHADE_MINBLOCKS) k_shade(DevSc
                                                        const uint32_t* order, uint32_t chunk, NrcWave nw)
 {
     const uint32_t count = w.counters[qin];
-    if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[5] = 0;  // shadow's work-queue head
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.counters[3] = 0;  // the next extend's work-queue head
+        w.counters[5] = 0;  // this bounce's shadow work-queue head
+    }
     const uint32_t* __restrict__ q = order ? order : (qin ? w.queue[1] : w.queue[0]);
     uint32_t* qout = qin ? w.queue[0] : w.queue[1];
     const int maxDepth = (int)ubo.maxDepth;
@@ -464,7 +477,7 @@ __global__ void __launch_bounds__(kShadeBlock, SB_SHADE_MINBLOCKS) k_shade(DevSc
             }
         }
         const bool hasShadow = sr.kind != 0;
-        const uint32_t spos = warp_push(&w.counters[2], hasShadow);
+        const uint32_t spos = warp_push(&w.counters[shadow_count(qin)], hasShadow);
         if (hasShadow) {
             w.sh_o[spos] = f4(sr.o, sr.tmax);
             w.sh_d[spos] = f4(sr.d, __uint_as_float(slot));
@@ -478,11 +491,10 @@ __global__ void __launch_bounds__(kShadeBlock, SB_SHADE_MINBLOCKS) k_shade(DevSc
 // order); adds the visible ones.  Work is taken from an atomic queue in
 // `chunk` units as in k_extend.
 template <bool COUNT>
-__global__ void __launch_bounds__(kExtendBlock, SB_SHADOW_MINBLOCKS) k_shadow(DevScene s, Wave w, uint32_t chunk,
+__global__ void __launch_bounds__(kExtendBlock, SB_SHADOW_MINBLOCKS) k_shadow(DevScene s, Wave w, int qin, uint32_t chunk,
                                                                               unsigned long long* visitCounters)
 {
-    const uint32_t count = w.counters[2];
-    if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[3] = 0;  // the next extend's work-queue head
+    const uint32_t count = w.counters[shadow_count(qin)];
     uint32_t stackN[SB_STACK];
     uint32_t nI = 0, nL = 0, nR = 0;
     WarpPool pool{0, 0, 0};
@@ -709,6 +721,8 @@ struct StrelkaPathTracer {
     cudaStream_t side = nullptr;    // training runs here, beside the frame
     cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
     uint32_t* traceHead = nullptr;    // work-queue head of the ray-query kernel
+    cudaStream_t aux = nullptr;       // shadow(k) beside extend(k+1)
+    cudaEvent_t shadeDone = nullptr, shadowDone = nullptr;
     uint32_t* sortHist = nullptr;     // shade-queue sort histogram (cleared by each scan)
     uint32_t* sortOffsets = nullptr;
 };
@@ -964,6 +978,9 @@ extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
     if (pt->traceHead) cudaFree(pt->traceHead);
     if (pt->sortHist) cudaFree(pt->sortHist);
     if (pt->sortOffsets) cudaFree(pt->sortOffsets);
+    if (pt->shadeDone) cudaEventDestroy(pt->shadeDone);
+    if (pt->shadowDone) cudaEventDestroy(pt->shadowDone);
+    if (pt->aux) cudaStreamDestroy(pt->aux);
     if (pt->forkEvent) cudaEventDestroy(pt->forkEvent);
     if (pt->joinEvent) cudaEventDestroy(pt->joinEvent);
     if (pt->side) cudaStreamDestroy(pt->side);
@@ -1067,6 +1084,13 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
     if (rc) return rc;
     const int maxDepth = (int)ubo.maxDepth;
     const uint32_t qchunk = pt->cfg.queueChunk ? pt->cfg.queueChunk : kDefaultQueueChunk;
+#if SB_OVERLAP_SHADOW
+    if (!pt->aux) {
+        SB_CUDA_TRY(cudaStreamCreateWithFlags(&pt->aux, cudaStreamNonBlocking));
+        SB_CUDA_TRY(cudaEventCreateWithFlags(&pt->shadeDone, cudaEventDisableTiming));
+        SB_CUDA_TRY(cudaEventCreateWithFlags(&pt->shadowDone, cudaEventDisableTiming));
+    }
+#endif
     // shade-queue sort by material: one key per material + miss + light/invalid
     uint32_t sortKeys = 0;
     if (!(pt->cfg.flags & STRELKA_PT_NO_SHADE_SORT) && s.numMaterials + 2 <= kMaxSortKeys) {
@@ -1115,6 +1139,7 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             int grid = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, pt->smallGrid);
             k_generate<<<grid, kSmallBlock, 0, st>>>(ubo, pt->main.w, first, n);
         }
+        bool pendingShadow = false;
         for (int depth = 0; depth < maxDepth; ++depth) {
             const int qin = depth & 1;
             const int gridE = std::min<int>((n + kExtendBlock - 1) / kExtendBlock, pt->extendGrid);
@@ -1138,6 +1163,9 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
                                                              pt->main.sorted);
                 order = pt->main.sorted;
             }
+#if SB_OVERLAP_SHADOW
+            if (pendingShadow) SB_CUDA_TRY(cudaStreamWaitEvent(st, pt->shadowDone, 0));
+#endif
             {
                 Timer t(pt, KC_SHADE, st);
                 if (useNrc)
@@ -1145,12 +1173,27 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
                 else
                     k_shade<false><<<gridS, kShadeBlock, 0, st>>>(s, ubo, pt->main.w, qin, order, qchunk, nw);
             }
+            // shadow(k) runs on the auxiliary stream beside extend(k+1): both
+            // read only shade(k)'s outputs; shade(k+1) waits for both
+            cudaStream_t sst = st;
+#if SB_OVERLAP_SHADOW
+            SB_CUDA_TRY(cudaEventRecord(pt->shadeDone, st));
+            SB_CUDA_TRY(cudaStreamWaitEvent(pt->aux, pt->shadeDone, 0));
+            sst = pt->aux;
+#endif
             {
-                Timer t(pt, KC_SHADOW, st);
-                if (count) k_shadow<true><<<gridW, kExtendBlock, 0, st>>>(s, pt->main.w, qchunk, pt->visitCounters);
-                else k_shadow<false><<<gridW, kExtendBlock, 0, st>>>(s, pt->main.w, qchunk, nullptr);
+                Timer t(pt, KC_SHADOW, sst);
+                if (count) k_shadow<true><<<gridW, kExtendBlock, 0, sst>>>(s, pt->main.w, qin, qchunk, pt->visitCounters);
+                else k_shadow<false><<<gridW, kExtendBlock, 0, sst>>>(s, pt->main.w, qin, qchunk, nullptr);
             }
+#if SB_OVERLAP_SHADOW
+            SB_CUDA_TRY(cudaEventRecord(pt->shadowDone, pt->aux));
+            pendingShadow = true;
+#endif
         }
+#if SB_OVERLAP_SHADOW
+        if (pendingShadow) SB_CUDA_TRY(cudaStreamWaitEvent(st, pt->shadowDone, 0));
+#endif
         if (useNrc) {
             if (first == 0) SB_CUDA_TRY(cudaStreamWaitEvent(st, pt->joinEvent, 0));
             Timer t(pt, KC_NRC_INFER, st);
