@@ -279,6 +279,27 @@ def nrc_mlp_microbench(torch, RadianceCache, lo, hi, log2t, peak_tflops):
     return out
 
 
+def run_nrc_mlp(args):
+    """--workload nrc-mlp: the radiance cache's fused kernels alone on
+    resident random records (nrc_mlp_microbench), one JSON line."""
+    import torch
+
+    from strelka_b200.render import RadianceCache
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak_tf = json.load(open(peaks_path)).get("bf16_tflops_sustained", 1400.0) if os.path.exists(peaks_path) else 1400.0
+    lo, hi = np.array([-20.0, -2.0, -20.0], np.float32), np.array([20.0, 8.0, 20.0], np.float32)
+    mlp = nrc_mlp_microbench(torch, RadianceCache, lo, hi, args.nrc_log2t, peak_tf)
+    line = {"metric": "radiance-cache inference Gqueries/s", "value": mlp["infer"]["gqueries_s"], "unit": "Gqueries/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f16 (f32 accumulation)", "data": "synthetic",
+            "config": {"workload": "hash grid (16 levels x 2^%d) + 64-wide 5-layer MLP, random records" % args.nrc_log2t},
+            "detail": mlp}
+    print(json.dumps(line), flush=True)
+
+
 def run_nrc(args):
     """--workload nrc: wall time of the radiance-cache renderer to reach the
     relMSE of one plain frame (the large render at --spp samples per pixel),
@@ -593,7 +614,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-step-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="large", choices=["large", "traversal", "nrc", "batch"])
+    ap.add_argument("--workload", default="large", choices=["large", "traversal", "nrc", "nrc-mlp", "batch"])
     ap.add_argument("--batch-jobs", type=int, default=32)
     ap.add_argument("--batch-scenes", type=int, default=6)
     ap.add_argument("--batch-seed", type=int, default=0)
@@ -617,6 +638,9 @@ def main():
         return
     if args.workload == "nrc":
         run_nrc(args)
+        return
+    if args.workload == "nrc-mlp":
+        run_nrc_mlp(args)
         return
     if args.workload == "batch":
         run_batch(args)
