@@ -315,7 +315,9 @@ typedef struct StrelkaPathTracerConfig {
     uint32_t blockSize;       /* threads per block (0 = auto) */
     uint32_t flags;           /* STRELKA_PT_* */
     uint32_t queueChunk;      /* wavefront: queue entries a warp takes at a time (0 = 32; a multiple of 32) */
-    uint32_t pad[3];
+    uint32_t tailDepth;       /* wavefront: bounces from this one on are finished by one persistent kernel per
+                                 path (0 = 5; >= maxDepth: never); ignored with the radiance cache */
+    uint32_t pad[2];
 } StrelkaPathTracerConfig;
 
 enum {

@@ -55,7 +55,7 @@ TRACE_COUNT = 1 << 4
 TRACE_REFINE = 1 << 5
 
 KERNEL_CLASSES = ["generate", "extend", "shade", "shadow", "finalize", "megakernel", "prep", "nrc_paths", "nrc_train",
-                  "nrc_infer", "sort"]
+                  "nrc_infer", "sort", "tail"]
 
 vp = C.c_void_p
 u8p = C.POINTER(C.c_uint8)
@@ -200,7 +200,7 @@ class StrelkaUsdLight(C.Structure):
 
 class StrelkaPathTracerConfig(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("chunkPaths", C.c_uint32), ("blockSize", C.c_uint32), ("flags", C.c_uint32),
-                ("queueChunk", C.c_uint32), ("pad", C.c_uint32 * 3)]
+                ("queueChunk", C.c_uint32), ("tailDepth", C.c_uint32), ("pad", C.c_uint32 * 2)]
 
 
 class TraceDesc(C.Structure):

@@ -31,6 +31,7 @@ constexpr int kShadeBlock = 128;
 constexpr int kSmallBlock = 256;
 constexpr uint32_t kMaxSortKeys = 4096;
 constexpr uint32_t kDefaultQueueChunk = 32;
+constexpr uint32_t kDefaultTailDepth = 5;  // first bounce finished by k_tail
 
 // Minimum resident blocks per SM requested for the any-hit (shadow) kernel:
 // 8 blocks of 128 threads fit its registers without spills and measured
@@ -61,10 +62,11 @@ enum KernelClass {
     KC_NRC_TRAIN,
     KC_NRC_INFER,
     KC_SORT,
+    KC_TAIL,
     KC_COUNT
 };
 const char* kKernelNames[KC_COUNT] = {"generate",  "extend",    "shade",     "shadow",    "finalize", "megakernel",
-                                      "prep",      "nrc_paths", "nrc_train", "nrc_infer", "sort"};
+                                      "prep",      "nrc_paths", "nrc_train", "nrc_infer", "sort", "tail"};
 
 // ---------------------------------------------------------------------------
 // Scene preparation: the record table of traverse.cuh, per node slot.
@@ -205,6 +207,7 @@ __global__ void __launch_bounds__(kSmallBlock) k_generate(PathTracerParam ubo, W
         w.counters[2] = 0;
         w.counters[3] = 0;  // extend's work-queue head
         w.counters[6] = 0;
+        w.counters[7] = 0;  // the tail kernel's work-queue head
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         PathState ps;
@@ -534,6 +537,56 @@ __global__ void __launch_bounds__(kExtendBlock, SB_SHADOW_MINBLOCKS) k_shadow(De
     }
 }
 
+// Finishes every path still queued for bounce `depth` (queue qin) with the
+// megakernel loop (closest hit, shade, shadow inline) to its end.  Used for
+// the last bounces, where few paths remain and a launch sequence per bounce
+// costs more than their work; each lane takes queued paths from an atomic
+// head.  Same device code and order of additions as the wavefront.
+__global__ void __launch_bounds__(kExtendBlock) k_tail(DevScene s, PathTracerParam ubo, Wave w, int qin, uint32_t chunk)
+{
+    const uint32_t count = w.counters[qin];
+    const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
+    const int maxDepth = (int)ubo.maxDepth;
+    WarpPool pool{0, 0, 0};
+    PathState ps;
+    uint32_t slot = 0;
+    bool have = false;
+    while (true) {
+        // one bounce per iteration; a lane whose path ended takes the next
+        const uint32_t got = pool_take(pool, &w.counters[7], count, chunk, !have);
+        if (!have && got != SB_INVALID) {
+            slot = q[got];
+            const float4 o = w.ray_o[slot];
+            const float4 d = w.ray_d[slot];
+            const float4 t4 = w.thr[slot];
+            ps.ro = xyz(o);
+            ps.tmax = o.w;
+            ps.rd = xyz(d);
+            ps.lastPdf = d.w;
+            ps.throughput = xyz(t4);
+            const uint32_t fl = __float_as_uint(t4.w);
+            ps.depth = (int)(fl & 0xffffu);
+            ps.specular = (fl >> 16) & 1u;
+            ps.inside = (fl >> 17) & 1u;
+            ps.nrcReady = (fl >> 18) & 1u;
+            ps.color = xyz(w.col[slot]);
+            ps.rng = w.rng[slot];
+            have = true;
+        }
+        if (!__any_sync(0xffffffffu, have)) break;
+        if (!have) continue;
+        HitRec h;
+        uint32_t a = 0, b = 0;
+        const bool found = s.numNodes != 0 && trace_closest_rec<false>(s, ps.ro, ps.tmax, ps.rd, h, a, b);
+        ShadowReq sr;
+        const bool cont = shade(s, ubo, ps, found, h, sr);
+        if (sr.kind != 0 && shadow_visible(s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
+        if (cont && ++ps.depth < maxDepth) continue;
+        w.col[slot] = f4(ps.color, 0.0f);
+        have = false;
+    }
+}
+
 __global__ void __launch_bounds__(kSmallBlock) k_finalize(Wave w, float* __restrict__ sampleBuffer, uint64_t first, uint32_t n)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -707,7 +760,7 @@ struct StrelkaPathTracer {
     std::vector<Rec> recs;
     std::vector<cudaEvent_t> eventPool;
     size_t eventsUsed = 0;
-    int extendGrid = 0, shadowGrid = 0, traceGrid = 0, traceGridAny = 0, shadeGrid = 0, shadeGridNrc = 0, smallGrid = 0;
+    int extendGrid = 0, shadowGrid = 0, tailGrid = 0, traceGrid = 0, traceGridAny = 0, shadeGrid = 0, shadeGridNrc = 0, smallGrid = 0;
     unsigned long long* visitCounters = nullptr;  // 6 entries (STRELKA_PT_COUNT)
     // radiance cache
     StrelkaNrc* nrc = nullptr;
@@ -955,6 +1008,7 @@ extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, 
     }
     pt->extendGrid = occupancy_grid((const void*)k_extend<false>, kExtendBlock, pt->numSMs);
     pt->shadowGrid = occupancy_grid((const void*)k_shadow<false>, kExtendBlock, pt->numSMs);
+    pt->tailGrid = occupancy_grid((const void*)k_tail, kExtendBlock, pt->numSMs);
     pt->traceGrid = occupancy_grid((const void*)k_trace<false, false, false>, kExtendBlock, pt->numSMs);
     pt->traceGridAny = occupancy_grid((const void*)k_trace<true, false, false>, kExtendBlock, pt->numSMs);
     pt->shadeGrid = occupancy_grid((const void*)k_shade<false>, kShadeBlock, pt->numSMs);
@@ -1140,7 +1194,9 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             k_generate<<<grid, kSmallBlock, 0, st>>>(ubo, pt->main.w, first, n);
         }
         bool pendingShadow = false;
-        for (int depth = 0; depth < maxDepth; ++depth) {
+        // bounces from tailDepth on run in one k_tail launch (not with the cache)
+        const int tailDepth = useNrc ? maxDepth : std::min<int>(maxDepth, (int)std::min<uint32_t>(pt->cfg.tailDepth ? pt->cfg.tailDepth : kDefaultTailDepth, 0x7FFFFFFFu));
+        for (int depth = 0; depth < tailDepth; ++depth) {
             const int qin = depth & 1;
             const int gridE = std::min<int>((n + kExtendBlock - 1) / kExtendBlock, pt->extendGrid);
             const int gridW = std::min<int>((n + kExtendBlock - 1) / kExtendBlock, pt->shadowGrid);
@@ -1194,6 +1250,11 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
 #if SB_OVERLAP_SHADOW
         if (pendingShadow) SB_CUDA_TRY(cudaStreamWaitEvent(st, pt->shadowDone, 0));
 #endif
+        if (tailDepth < maxDepth) {
+            Timer t(pt, KC_TAIL, st);
+            const int gridE = std::min<int>((n + kExtendBlock - 1) / kExtendBlock, pt->tailGrid);
+            k_tail<<<gridE, kExtendBlock, 0, st>>>(s, ubo, pt->main.w, tailDepth & 1, qchunk);
+        }
         if (useNrc) {
             if (first == 0) SB_CUDA_TRY(cudaStreamWaitEvent(st, pt->joinEvent, 0));
             Timer t(pt, KC_NRC_INFER, st);

@@ -185,11 +185,11 @@ class PathTracer:
     """PathTracer pass (include/render/pathtracer.h:33-50)."""
 
     def __init__(self, mode: int = abi.MODE_WAVEFRONT, chunk_paths: int = 0, profile: bool = False,
-                 count: bool = False, queue_chunk: int = 0, shade_sort: bool = True):
+                 count: bool = False, queue_chunk: int = 0, shade_sort: bool = True, tail_depth: int = 0):
         self.lib = abi.load()
         flags = ((abi.PT_PROFILE if profile else 0) | (abi.PT_COUNT if count else 0) |
                  (0 if shade_sort else abi.PT_NO_SHADE_SORT))
-        cfg = abi.StrelkaPathTracerConfig(mode, chunk_paths, 0, flags, queue_chunk)
+        cfg = abi.StrelkaPathTracerConfig(mode, chunk_paths, 0, flags, queue_chunk, tail_depth)
         h = C.c_void_p()
         abi.check(self.lib.strelka_pathtracer_create(C.byref(cfg), C.byref(h)))
         self.handle = h

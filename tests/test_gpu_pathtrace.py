@@ -68,6 +68,24 @@ def test_megakernel_equals_wavefront(cuda, cornell):
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
+@pytest.mark.parametrize("tail", [1, 3, 7, 100])
+def test_tail_kernel_equals_megakernel(cuda, tail):
+    # the wavefront finishes bounces >= tail in one persistent kernel; every
+    # switch depth gives the megakernel's samples bit for bit
+    s = scenes.large(width=48, height=32, instances=6, frequency=6, num_textures=2, tex_size=64, env_width=64,
+                     env_height=32, max_depth=8, spp=2, seed=4)
+    ds = DeviceScene(s)
+    p = s.param(frameNumber=3)
+    a, _ = render(cuda, s, ds, p, abi.MODE_MEGAKERNEL)
+    total = p.dimension[0] * p.dimension[1] * p.spp
+    sb = cuda.full((total * 3,), -7.0, dtype=cuda.float32, device="cuda")
+    pt = PathTracer(mode=abi.MODE_WAVEFRONT, chunk_paths=1111, tail_depth=tail)
+    pt.execute(ds.desc(p, sb), total, 1, 0)
+    assert pt.device_status() == 0
+    b = sb.cpu().numpy()
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
 def test_debug_normals(cuda, cornell):
     # ubo.debug == 1 returns (N + 1) / 2 of the first surface hit
     s, view, ds = cornell
