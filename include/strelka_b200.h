@@ -57,7 +57,8 @@ enum {
     STRELKA_DEV_LIGHT_OOB = 1u << 4,    /* light id >= light capacity */
     STRELKA_DEV_TRAVERSAL_CAP = 1u << 5,/* traversal exceeded 2*numNodes+2 visits (cycle) */
     STRELKA_DEV_TEXTURE_OOB = 1u << 6,
-    STRELKA_DEV_QUEUE_TIMEOUT = 1u << 7
+    STRELKA_DEV_QUEUE_TIMEOUT = 1u << 7,
+    STRELKA_DEV_MMA_TIMEOUT = 1u << 8   /* a tensor-core completion wait hit its time limit */
 };
 
 /* ------------------------------------------------------------------------- */
@@ -509,6 +510,9 @@ int strelka_nrc_gradients(StrelkaNrc* nrc, const StrelkaNrcRecord* samples, uint
 int strelka_nrc_get_params(StrelkaNrc* nrc, float* mlp, float* grid);
 int strelka_nrc_set_params(StrelkaNrc* nrc, const float* mlp, const float* grid);
 /* Sizes and the per-level grid resolution (negative when the level is hashed). */
+/* Reads and clears the cache's device status word (STRELKA_DEV_* bits);
+ * synchronises the stream. */
+int strelka_nrc_get_device_status(StrelkaNrc* nrc, void* stream, uint32_t* status);
 int strelka_nrc_info(StrelkaNrc* nrc, uint32_t* numMlpParams, uint64_t* numGridParams, int32_t* levelRes);
 
 /* ------------------------------------------------------------------------- */

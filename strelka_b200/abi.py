@@ -33,6 +33,7 @@ DEV_LIGHT_OOB = 1 << 4
 DEV_TRAVERSAL_CAP = 1 << 5
 DEV_TEXTURE_OOB = 1 << 6
 DEV_QUEUE_TIMEOUT = 1 << 7
+DEV_MMA_TIMEOUT = 1 << 8
 
 FN_LAMBERT = 0
 FN_GGX_CONDUCTOR = 1
@@ -305,6 +306,7 @@ SIGNATURES = {
     "strelka_nrc_get_params": (C.c_int, [vp, vp, vp]),
     "strelka_nrc_set_params": (C.c_int, [vp, vp, vp]),
     "strelka_nrc_info": (C.c_int, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), vp]),
+    "strelka_nrc_get_device_status": (C.c_int, [vp, vp, C.POINTER(C.c_uint32)]),
     "strelka_batch_create": (C.c_int, [C.POINTER(vp)]),
     "strelka_batch_destroy": (C.c_int, [vp]),
     "strelka_batch_set_jobs": (C.c_int, [vp, vp, C.c_uint32, vp]),

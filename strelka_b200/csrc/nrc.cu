@@ -1,6 +1,6 @@
 // nrc.cu — online-trained neural radiance cache: multiresolution hash-grid
-// encoding + a fully fused 64-wide MLP on FP16 tensor cores (mma.sync
-// m16n8k16, FP32 accumulation), forward and backward, with Adam.
+// encoding + a fully fused 64-wide MLP on FP16 tensor cores (FP32
+// accumulation), forward and backward, with Adam.
 //
 // The cache predicts the outgoing radiance at a path vertex from its
 // position (16-level hash grid, 2 features per level, 2^19 entries per
@@ -10,15 +10,20 @@
 // (linear), no biases (a constant-1 input stands in), trained with the
 // relative L2 loss (y - t)^2 / (sg(y)^2 + 0.01) (Müller et al. 2021).
 //
-// Tensor-core mapping: each warp owns a tile of 16 queries.  For a layer
-// out = W * in, the 16x64 activation tile is the A operand (row-major) and
-// W (out x in, row-major in shared memory with a 72-half row stride, which
-// keeps the fragment loads bank-conflict free) is the column-major B operand;
-// the m16n8k16 accumulator layout of one layer is exactly the A-fragment
-// layout of the next layer's k-steps, so activations stay in registers
-// between layers.  Backward uses the same instruction with W^T (fragments
-// gathered from the same shared copy) and accumulates weight gradients
-// d^T * a over each tile with a third mma shape, reduced in shared memory.
+// Inference runs on the tcgen05 tensor cores (k_nrc_infer): 128-record
+// tiles, activations resident in tensor memory between layers, weights read
+// by the tensor core from shared memory (details at the kernel).
+//
+// Training (k_nrc_train) uses mma.sync m16n8k16: each warp owns a tile of 16
+// records.  For a layer out = W * in, the 16x64 activation tile is the A
+// operand (row-major) and W (out x in, row-major in shared memory with a
+// 72-half row stride, which keeps the fragment loads bank-conflict free) is
+// the column-major B operand; the m16n8k16 accumulator layout of one layer is
+// exactly the A-fragment layout of the next layer's k-steps, so activations
+// stay in registers between layers.  Backward uses the same instruction with
+// W^T (fragments gathered from the same shared copy) and accumulates weight
+// gradients d^T * a over each tile with a third mma shape, reduced in shared
+// memory.
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -29,10 +34,12 @@
 
 #include "common.h"
 #include "nrc.h"
+#include "tc.cuh"
 
 namespace {
 
 using sb::fail;
+namespace tc = sb::tc;
 
 constexpr int kLevels = 16;
 constexpr int kIn = 64;
@@ -262,57 +269,225 @@ __device__ __forceinline__ void output_layer(const __half* sW4, const uint32_t (
 }
 
 // ---------------------------------------------------------------------------
-// Inference: y for every record.  mode 0: out[3*i + c] = y_c; mode 1:
-// col[slot] += throughput * max(y, 0) (the throughput rides in target[]).
-__global__ void __launch_bounds__(256) k_nrc_infer(const StrelkaNrcRecord* __restrict__ recs, const uint32_t* countPtr,
-                                                   uint32_t maxN, const __half* __restrict__ w,
-                                                   const __half2* __restrict__ grid, NrcGeom g, float* __restrict__ out,
-                                                   float4* __restrict__ col)
+// Inference on the tcgen05 tensor cores.  A CTA owns tiles of 128 records;
+// record i of a tile lives in TMEM lane i.  Its two warpgroups both reach
+// every lane (a warp addresses lanes 32*(warp % 4) .. +31) and split the
+// work by columns: warpgroup 0 encodes grid levels 0..7 plus the direction /
+// normal / roughness inputs, warpgroup 1 levels 8..15.  One thread issues
+// each layer as four 128xNx16 MMAs (A = activations in TMEM, B = the layer's
+// weights in shared memory, D = FP32 in TMEM).  Between layers each
+// warpgroup reads its 32 columns of D, applies ReLU, rounds to FP16 and
+// writes them back as its half of the next layer's A, so activations never
+// leave tensor memory.
+constexpr int kTcTile = 128;
+constexpr int kTcThreads = 256;
+constexpr int kTcBlocksPerSM = 3;  // resident CTAs per SM: the register bound of the launch bounds
+constexpr uint32_t kTcLayerBytes = kWidth * kIn * 2;                      // 8192
+constexpr uint32_t kTcWeightBytes = 4 * kTcLayerBytes + kOutPad * kIn * 2;  // 34816
+constexpr uint32_t kTcColD = 0;     // accumulator, 64 columns
+constexpr uint32_t kTcColA = 64;    // activations, 32 columns (64 halves)
+constexpr uint32_t kTcCols = 128;   // TMEM columns per CTA
+constexpr uint64_t kTcWaitNs = 1000000000ull;  // MMA completion wait limit (1 s)
+// Shared memory per CTA: the weights, the mbarrier and the TMEM address.
+constexpr uint32_t kTcSmem = kTcWeightBytes + 64;
+// Shared-memory carveout (percent of the maximum), chosen so that at most
+// three CTAs fit by shared memory (3 x 128 TMEM columns <= 512) and the L1
+// keeps about half the SM's memory for the hash-grid gathers.
+constexpr int kTcCarveoutPercent = 50;
+
+// Byte offset of weight (row r, input k) in the K-major core-matrix layout:
+// 8x8 blocks of 128 contiguous bytes, 128 B apart along K, 1024 B apart
+// along the rows.
+__device__ __forceinline__ uint32_t core_offset(int r, int k)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __half* sW = reinterpret_cast<__half*>(smem);
-    __half* sX = sW + kMatRows * kRow + (threadIdx.x >> 5) * 16 * kRow;
-    load_weights(w, sW);
+    return (uint32_t)((r >> 3) * 1024 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// Corner weights of level l and the 8 grid entries they blend (loads issued).
+__device__ __forceinline__ void level_fetch(const NrcGeom& g, const __half2* __restrict__ grid, int l, float px, float py,
+                                            float pz, float (&w)[8], uint32_t (&v)[8])
+{
+    Corner c;
+    level_corners(g, l, px, py, pz, c);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        w[k] = c.w[k];
+        // grid entries are kept in L1 ahead of other lines: corners along x
+        // often share a sector, and the coarse levels are reused across records
+        uint32_t r;
+        asm volatile("ld.global.nc.L1::evict_last.b32 %0, [%1];"
+                     : "=r"(r)
+                     : "l"(reinterpret_cast<const unsigned int*>(grid) + c.idx[k]));
+        v[k] = r;
+    }
+}
+// trilinear blend of one level's two features, as an FP16 pair
+__device__ __forceinline__ uint32_t level_mix(const float (&w)[8], const uint32_t (&v)[8])
+{
+    float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float2 x = __half22float2(*reinterpret_cast<const __half2*>(&v[k]));
+        f0 += w[k] * x.x;
+        f1 += w[k] * x.y;
+    }
+    return pack2(f0, f1);
+}
+// grid levels l0 .. l0+7 as 8 FP16 pairs
+__device__ __forceinline__ void encode_levels8(const NrcGeom& g, const __half2* __restrict__ grid, int l0, float px,
+                                               float py, float pz, uint32_t (&a)[8])
+{
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        float w0[8];
+        uint32_t v0[8];
+        level_fetch(g, grid, l0 + i, px, py, pz, w0, v0);
+        a[i] = level_mix(w0, v0);
+    }
+}
+// inputs 32..63: 16 SH coefficients, normal, roughness, the constant 1, zeros
+__device__ __forceinline__ void encode_rest(const StrelkaNrcRecord& rec, uint32_t (&a)[16])
+{
+    float sh[16];
+    sh16(rec.dir[0], rec.dir[1], rec.dir[2], sh);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = pack2(sh[2 * i], sh[2 * i + 1]);
+    a[8] = pack2(rec.normal[0] * 0.5f + 0.5f, rec.normal[1] * 0.5f + 0.5f);
+    a[9] = pack2(rec.normal[2] * 0.5f + 0.5f, rec.roughness);
+    a[10] = pack2(1.0f, 0.0f);
+#pragma unroll
+    for (int i = 11; i < 16; ++i) a[i] = 0u;
+}
+
+// ReLU + FP16 of 16 accumulator columns into 8 packed pairs
+__device__ __forceinline__ void relu_pack16(const uint32_t* d, uint32_t* a)
+{
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        a[j] = pack2(fmaxf(__uint_as_float(d[2 * j]), 0.0f), fmaxf(__uint_as_float(d[2 * j + 1]), 0.0f));
+}
+
+// y for every record.  out != NULL: out[3*i + c] = y_c; otherwise
+// col[slot] += throughput * max(y, 0) (the throughput rides in target[]).
+// A tensor-core wait that runs out sets STRELKA_DEV_MMA_TIMEOUT in *status
+// and ends the CTA after releasing its TMEM.
+__global__ void __launch_bounds__(kTcThreads, kTcBlocksPerSM) k_nrc_infer(const StrelkaNrcRecord* __restrict__ recs, const uint32_t* countPtr,
+                                                             uint32_t maxN, const __half* __restrict__ w,
+                                                             const __half2* __restrict__ grid, NrcGeom g,
+                                                             float* __restrict__ out, float4* __restrict__ col,
+                                                             uint32_t* __restrict__ status)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* sW = smem;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTcWeightBytes);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(smem + kTcWeightBytes + 8);
+    const int tid = threadIdx.x, warp = tid >> 5, wg = tid >> 7, row = tid & (kTcTile - 1);
+    // W0..W3 (64 rows) and W4 (16 rows) into the core-matrix layout, 16 B at a time
+    for (int i = tid; i < kMatRows * (kIn / 8); i += kTcThreads) {
+        const int r0 = i >> 3, c = i & 7;
+        const int layer = r0 < 4 * kWidth ? r0 / kWidth : 4;
+        const int r = r0 - layer * kWidth;
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(w + (size_t)r0 * kIn + c * 8));
+        *reinterpret_cast<uint4*>(sW + layer * kTcLayerBytes + core_offset(r, c * 8)) = v;
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(slot, kTcCols);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) tc::mbar_init(bar, 1);
+    tc::fence_proxy_async_smem();
+    tc::fence_before_sync();
     __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tb = *slot;
+    const uint32_t lane = tb + ((uint32_t)((warp & 3) * 32) << 16);  // this warp's 32 TMEM lanes
+    const uint32_t sW0 = tc::smem_u32(sW);
     const uint32_t n = countPtr ? min(*countPtr, maxN) : maxN;
-    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-    const uint32_t warpsTotal = gridDim.x * (blockDim.x >> 5);
-    const uint32_t tiles = (n + 15) / 16;
-    for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < tiles; t += warpsTotal) {
-        const uint32_t base = t * 16;
-        encode_tile(g, grid, recs, base, n, sX);
-        __syncwarp();
-        uint32_t a[4][4];
-        load_a(sX, a);
-        float acc[8][4];
-#pragma unroll
-        for (int l = 0; l < 4; ++l) {
-            layer64(sW + l * kWidth * kRow, a, acc);
-            relu_to_a(acc, a);
-        }
-        float y[4];
-        output_layer(sW + 4 * kWidth * kRow, a, y);
-        // lanes with tig 0 hold outputs 0,1; tig 1 holds output 2 (and a pad)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const uint32_t q = base + (uint32_t)gid + 8u * (uint32_t)h;
-            if (q >= n || tig > 1) continue;
-            const float y0 = y[2 * h], y1 = y[2 * h + 1];
-            if (out) {
-                out[3 * (size_t)q + 2 * tig] = y0;
-                if (tig == 0) out[3 * (size_t)q + 1] = y1;
+    const uint32_t tiles = (n + kTcTile - 1) / kTcTile;
+    uint32_t phase = 0;
+    bool timedOut = false;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint32_t q = t * kTcTile + (uint32_t)row;
+        {
+            // (tcgen05.st is warp-collective: every lane reaches the same stores)
+            uint32_t a[8], b[16];
+            if (q < n) {
+                const StrelkaNrcRecord& rec = recs[q];
+                float px, py, pz;
+                normalized_position(g, rec, px, py, pz);
+                encode_levels8(g, grid, 8 * wg, px, py, pz, a);
+                if (wg == 0) encode_rest(rec, b);
             } else {
-                const StrelkaNrcRecord& r = recs[q];
-                float* c = reinterpret_cast<float*>(&col[r.slot]);
-                if (tig == 0) {
-                    c[0] += r.target[0] * fmaxf(y0, 0.0f);
-                    c[1] += r.target[1] * fmaxf(y1, 0.0f);
-                } else {
-                    c[2] += r.target[2] * fmaxf(y0, 0.0f);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) a[i] = 0u;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) b[i] = 0u;
+            }
+            if (wg == 0) tc::tmem_st16(lane + kTcColA + 16, b);
+            tc::tmem_st8(lane + kTcColA + 8 * wg, a);
+            tc::tmem_wait_st();
+        }
+        bool abort = false;
+#pragma unroll 1
+        for (int l = 0; l < 5; ++l) {
+            // this layer's A is in TMEM; thread 0 issues the MMAs and alone
+            // waits for them, the others sleep on the CTA barrier meanwhile
+            tc::fence_before_sync();
+            __syncthreads();
+            if (tid == 0) {
+                tc::fence_after_sync();
+                const uint32_t idesc = l < 4 ? tc::idesc_f16_f32(kTcTile, kWidth) : tc::idesc_f16_f32(kTcTile, kOutPad);
+#pragma unroll
+                for (int kb = 0; kb < 4; ++kb)
+                    tc::mma_f16_ts(tb + kTcColD, tb + kTcColA + 8 * kb,
+                                   tc::desc_kmajor(sW0 + l * kTcLayerBytes + 256 * kb, 128, 1024), idesc, kb > 0);
+                tc::mma_commit(bar);
+                if (!tc::mbar_wait_bounded(bar, phase, kTcWaitNs)) timedOut = true;
+            }
+            phase ^= 1;
+            if (__syncthreads_or(timedOut)) {
+                abort = true;
+                break;
+            }
+            tc::fence_after_sync();
+            if (l < 4) {
+                // this warpgroup's outputs 32*wg .. +31 become inputs 32*wg .. +31
+                uint32_t d[32], a[16];
+                tc::tmem_ld16(lane + kTcColD + 32 * wg, d);
+                tc::tmem_ld16(lane + kTcColD + 32 * wg + 16, d + 16);
+                tc::tmem_wait_ld();
+                relu_pack16(d, a);
+                relu_pack16(d + 16, a + 8);
+                tc::tmem_st16(lane + kTcColA + 16 * wg, a);
+                tc::tmem_wait_st();
+            } else if (wg == 0) {
+                uint32_t y[4];
+                tc::tmem_ld4(lane + kTcColD, y);
+                tc::tmem_wait_ld();
+                if (q < n && !timedOut) {
+                    const float y0 = __uint_as_float(y[0]), y1 = __uint_as_float(y[1]), y2 = __uint_as_float(y[2]);
+                    if (out) {
+                        out[3 * (size_t)q + 0] = y0;
+                        out[3 * (size_t)q + 1] = y1;
+                        out[3 * (size_t)q + 2] = y2;
+                    } else {
+                        const StrelkaNrcRecord& r = recs[q];
+                        float* c = reinterpret_cast<float*>(&col[r.slot]);
+                        c[0] += r.target[0] * fmaxf(y0, 0.0f);
+                        c[1] += r.target[1] * fmaxf(y1, 0.0f);
+                        c[2] += r.target[2] * fmaxf(y2, 0.0f);
+                    }
                 }
             }
         }
-        __syncwarp();
+        if (abort) break;
+    }
+    if (timedOut) atomicOr(status, STRELKA_DEV_MMA_TIMEOUT);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tb, kTcCols);
     }
 }
 
@@ -518,7 +693,6 @@ __global__ void k_to_half(const float* __restrict__ p, __half* __restrict__ ph, 
         ph[i] = __float2half(p[i]);
 }
 
-size_t infer_smem() { return (size_t)(kMatRows * kRow + 8 * 16 * kRow) * sizeof(__half); }
 size_t train_smem() { return (size_t)(kMatRows * kRow + 8 * 6 * 16 * kRow) * sizeof(__half) + kParams * sizeof(float); }
 
 }  // namespace
@@ -539,6 +713,7 @@ struct StrelkaNrc {
     float* gridGrad = nullptr;
     __half* gridHalf = nullptr;
     float* loss = nullptr;
+    uint32_t* status = nullptr;  // device status word (STRELKA_DEV_* bits)
     uint64_t step = 0;
 };
 
@@ -546,7 +721,7 @@ namespace {
 void nrc_free(StrelkaNrc* n)
 {
     void* ptrs[] = {n->mlp, n->mlpM, n->mlpV, n->mlpGrad, n->mlpHalf, n->grid, n->gridM, n->gridV, n->gridGrad,
-                    n->gridHalf, n->loss};
+                    n->gridHalf, n->loss, n->status};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -589,7 +764,8 @@ extern "C" int strelka_nrc_create(const StrelkaNrcConfig* cfg, StrelkaNrc** out)
               cudaMalloc(&nrc->grid, nrc->gridN * 4) == cudaSuccess && cudaMalloc(&nrc->gridM, nrc->gridN * 4) == cudaSuccess &&
               cudaMalloc(&nrc->gridV, nrc->gridN * 4) == cudaSuccess &&
               cudaMalloc(&nrc->gridGrad, nrc->gridN * 4) == cudaSuccess &&
-              cudaMalloc(&nrc->gridHalf, nrc->gridN * 2) == cudaSuccess && cudaMalloc(&nrc->loss, 4) == cudaSuccess;
+              cudaMalloc(&nrc->gridHalf, nrc->gridN * 2) == cudaSuccess && cudaMalloc(&nrc->loss, 4) == cudaSuccess &&
+              cudaMalloc(&nrc->status, 4) == cudaSuccess;
     if (!ok) {
         nrc_free(nrc);
         delete nrc;
@@ -614,13 +790,15 @@ extern "C" int strelka_nrc_create(const StrelkaNrcConfig* cfg, StrelkaNrc** out)
     for (auto& v : gr) v = (float)((2.0 * u01() - 1.0) * 1e-4);
     cudaMemcpy(nrc->mlp, w.data(), kParams * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(nrc->grid, gr.data(), nrc->gridN * 4, cudaMemcpyHostToDevice);
+    cudaMemset(nrc->status, 0, 4);
     cudaMemset(nrc->mlpM, 0, kParams * 4);
     cudaMemset(nrc->mlpV, 0, kParams * 4);
     cudaMemset(nrc->gridM, 0, nrc->gridN * 4);
     cudaMemset(nrc->gridV, 0, nrc->gridN * 4);
     k_to_half<<<64, 256>>>(nrc->mlp, nrc->mlpHalf, kParams);
     k_to_half<<<grid_blocks(nrc, nrc->gridN, 256), 256>>>(nrc->grid, nrc->gridHalf, nrc->gridN);
-    cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)infer_smem());
+    cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+    cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributePreferredSharedMemoryCarveout, kTcCarveoutPercent);
     cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem());
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
@@ -642,13 +820,14 @@ extern "C" int strelka_nrc_destroy(StrelkaNrc* nrc)
 
 // internal entry points shared with the path tracer (device-side counts)
 int nrc_infer_device(StrelkaNrc* nrc, const StrelkaNrcRecord* recs, const uint32_t* countPtr, uint32_t maxN, float* out,
-                     float4* col, cudaStream_t st)
+                     float4* col, uint32_t* status, cudaStream_t st)
 {
     if (maxN == 0) return STRELKA_OK;
-    const int tiles = (int)((maxN + 15) / 16);
-    const int blocks = std::max(1, std::min((tiles + 7) / 8, nrc->numSMs * 4));
-    k_nrc_infer<<<blocks, 256, infer_smem(), st>>>(recs, countPtr, maxN, nrc->mlpHalf,
-                                                  reinterpret_cast<const __half2*>(nrc->gridHalf), nrc->geom, out, col);
+    const int tiles = (int)((maxN + kTcTile - 1) / kTcTile);
+    const int blocks = std::max(1, std::min(tiles, nrc->numSMs * kTcBlocksPerSM));
+    k_nrc_infer<<<blocks, kTcThreads, kTcSmem, st>>>(recs, countPtr, maxN, nrc->mlpHalf,
+                                                 reinterpret_cast<const __half2*>(nrc->gridHalf), nrc->geom, out, col,
+                                                 status ? status : nrc->status);
     SB_CUDA_TRY(cudaGetLastError());
     return STRELKA_OK;
 }
@@ -692,7 +871,7 @@ int nrc_adam_device_count(StrelkaNrc* nrc, float batch, const uint32_t* countPtr
 extern "C" int strelka_nrc_infer(StrelkaNrc* nrc, const StrelkaNrcRecord* records, uint32_t n, float* outRGB, void* stream)
 {
     if (!nrc || (n && (!records || !outRGB))) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
-    return nrc_infer_device(nrc, records, nullptr, n, outRGB, nullptr, static_cast<cudaStream_t>(stream));
+    return nrc_infer_device(nrc, records, nullptr, n, outRGB, nullptr, nullptr, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int strelka_nrc_gradients(StrelkaNrc* nrc, const StrelkaNrcRecord* samples, uint32_t n, float* mlpGrad,
@@ -761,6 +940,15 @@ extern "C" int strelka_nrc_set_params(StrelkaNrc* nrc, const float* mlp, const f
         k_to_half<<<grid_blocks(nrc, nrc->gridN, 256), 256>>>(nrc->grid, nrc->gridHalf, nrc->gridN);
     }
     SB_CUDA_TRY(cudaDeviceSynchronize());
+    return STRELKA_OK;
+}
+
+extern "C" int strelka_nrc_get_device_status(StrelkaNrc* nrc, void* stream, uint32_t* status)
+{
+    if (!nrc || !status) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");
+    SB_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    SB_CUDA_TRY(cudaMemcpy(status, nrc->status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    SB_CUDA_TRY(cudaMemset(nrc->status, 0, sizeof(uint32_t)));
     return STRELKA_OK;
 }
 

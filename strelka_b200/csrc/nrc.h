@@ -8,7 +8,7 @@
 // col[slot] += throughput * max(prediction, 0) for queries [0, *count) (out == NULL),
 // or out[3*i + c] = prediction.
 int nrc_infer_device(StrelkaNrc* nrc, const StrelkaNrcRecord* recs, const uint32_t* count, uint32_t maxN, float* out,
-                     float4* col, cudaStream_t st);
+                     float4* col, uint32_t* status, cudaStream_t st);
 // Gradients of the batch [0, *count) into the cache's gradient buffers.
 int nrc_gradients_device(StrelkaNrc* nrc, const StrelkaNrcRecord* recs, const uint32_t* count, uint32_t maxN,
                          cudaStream_t st);

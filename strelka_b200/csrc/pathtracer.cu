@@ -1258,7 +1258,7 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
         if (useNrc) {
             if (first == 0) SB_CUDA_TRY(cudaStreamWaitEvent(st, pt->joinEvent, 0));
             Timer t(pt, KC_NRC_INFER, st);
-            rc = nrc_infer_device(pt->nrc, pt->nrcQueries, pt->nrcCounts, n, nullptr, pt->main.w.col, st);
+            rc = nrc_infer_device(pt->nrc, pt->nrcQueries, pt->nrcCounts, n, nullptr, pt->main.w.col, pt->status, st);
             if (rc) return rc;
         }
         {

@@ -67,6 +67,9 @@ def test_forward_matches_reference(cuda):
     ref = nrc_ref.infer(rec, mlp, grid, BMIN, BMAX, LOG2_T)
     scale = np.abs(ref).max()
     assert np.abs(got - ref).max() <= 2e-2 * scale, (np.abs(got - ref).max(), scale)
+    status = C.c_uint32(123)
+    abi.check(lib.strelka_nrc_get_device_status(h, None, C.byref(status)))
+    assert status.value == 0  # no tensor-core wait ran out
     lib.strelka_nrc_destroy(h)
 
 
