@@ -10,20 +10,11 @@
 // (linear), no biases (a constant-1 input stands in), trained with the
 // relative L2 loss (y - t)^2 / (sg(y)^2 + 0.01) (Müller et al. 2021).
 //
-// Inference runs on the tcgen05 tensor cores (k_nrc_infer): 128-record
-// tiles, activations resident in tensor memory between layers, weights read
-// by the tensor core from shared memory (details at the kernel).
-//
-// Training (k_nrc_train) uses mma.sync m16n8k16: each warp owns a tile of 16
-// records.  For a layer out = W * in, the 16x64 activation tile is the A
-// operand (row-major) and W (out x in, row-major in shared memory with a
-// 72-half row stride, which keeps the fragment loads bank-conflict free) is
-// the column-major B operand; the m16n8k16 accumulator layout of one layer is
-// exactly the A-fragment layout of the next layer's k-steps, so activations
-// stay in registers between layers.  Backward uses the same instruction with
-// W^T (fragments gathered from the same shared copy) and accumulates weight
-// gradients d^T * a over each tile with a third mma shape, reduced in shared
-// memory.
+// Both directions run on the tcgen05 tensor cores with 128-record tiles:
+// inference (k_nrc_infer) keeps activations in tensor memory between
+// layers; training (k_nrc_train) keeps them in shared memory, where the
+// tensor core reads them for the forward pass and, transposed, for the
+// weight gradients.  Details at each kernel.
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -45,7 +36,6 @@ constexpr int kLevels = 16;
 constexpr int kIn = 64;
 constexpr int kWidth = 64;
 constexpr int kOutPad = 16;
-constexpr int kRow = 72;                       // shared-memory row stride (halves)
 constexpr int kMatRows = 4 * kWidth + kOutPad; // 272 rows: W0..W3 (64 each), W4 (16)
 constexpr int kParams = 4 * kWidth * kIn + kOutPad * kWidth;  // 17408
 constexpr float kGradScale = 1.0f / 128.0f;    // loss-gradient scale (FP16 range)
@@ -60,25 +50,11 @@ struct NrcGeom {
 };
 
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
-{
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
 __device__ __forceinline__ uint32_t pack2(float x, float y)
 {
     __half2 h = __floats2half2_rn(x, y);
     return *reinterpret_cast<uint32_t*>(&h);
 }
-__device__ __forceinline__ uint32_t pack2h(__half x, __half y)
-{
-    __half2 h = __halves2half2(x, y);
-    return *reinterpret_cast<uint32_t*>(&h);
-}
-__device__ __forceinline__ uint32_t lds32(const __half* p) { return *reinterpret_cast<const uint32_t*>(p); }
-
 // ---------------------------------------------------------------------------
 // Encoding.  Position -> [0,1]^3 by the scene box; level l has resolution
 // res_l = floor(16 * 1.5^l); dense indexing when (res_l+1)^3 fits the table,
@@ -146,126 +122,6 @@ __device__ __forceinline__ void sh16(float x, float y, float z, float* o)
     o[13] = -c3m1 * x * (5.0f * zz - 1.0f);
     o[14] = c32 * z * (xx - yy);
     o[15] = -c3m3 * x * (xx - 3.0f * yy);
-}
-
-// Encodes rows [0,16) of a tile into sx (16 x kRow halves): lane (r, half)
-// handles row r = lane & 15 and levels 8*(lane >> 4) .. +7; lanes 0..15 also
-// write the direction / normal / roughness / constant inputs.
-__device__ __forceinline__ void encode_tile(const NrcGeom& g, const __half2* __restrict__ grid,
-                                            const StrelkaNrcRecord* __restrict__ recs, uint32_t base, uint32_t n, __half* sx)
-{
-    const int lane = threadIdx.x & 31;
-    const int r = lane & 15;
-    const uint32_t q = base + (uint32_t)r;
-    __half* row = sx + r * kRow;
-    if (q >= n) {
-        for (int c = (lane >> 4) * 32; c < (lane >> 4) * 32 + 32; ++c) row[c] = __float2half(0.0f);
-        return;
-    }
-    const StrelkaNrcRecord rec = recs[q];
-    float px, py, pz;
-    normalized_position(g, rec, px, py, pz);
-    const int l0 = (lane >> 4) * 8;
-    for (int l = l0; l < l0 + 8; ++l) {
-        Corner c;
-        level_corners(g, l, px, py, pz, c);
-        float f0 = 0.0f, f1 = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const float2 v = __half22float2(__ldg(&grid[c.idx[k]]));
-            f0 += c.w[k] * v.x;
-            f1 += c.w[k] * v.y;
-        }
-        row[2 * l] = __float2half(f0);
-        row[2 * l + 1] = __float2half(f1);
-    }
-    if (lane < 16) {
-        float sh[16];
-        sh16(rec.dir[0], rec.dir[1], rec.dir[2], sh);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) row[32 + i] = __float2half(sh[i]);
-        row[48] = __float2half(rec.normal[0] * 0.5f + 0.5f);
-        row[49] = __float2half(rec.normal[1] * 0.5f + 0.5f);
-        row[50] = __float2half(rec.normal[2] * 0.5f + 0.5f);
-        row[51] = __float2half(rec.roughness);
-        row[52] = __float2half(1.0f);
-#pragma unroll
-        for (int i = 53; i < 64; ++i) row[i] = __float2half(0.0f);
-    }
-}
-
-__device__ __forceinline__ void load_weights(const __half* __restrict__ w, __half* sW)
-{
-    for (int i = threadIdx.x; i < kMatRows * kIn; i += blockDim.x) {
-        const int row = i / kIn, col = i - row * kIn;
-        sW[row * kRow + col] = w[i];
-    }
-}
-
-// A fragments of a 16 x 64 tile stored row-major (stride kRow) in shared memory.
-__device__ __forceinline__ void load_a(const __half* s, uint32_t (&a)[4][4])
-{
-    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        a[k][0] = lds32(s + gid * kRow + 16 * k + 2 * tig);
-        a[k][1] = lds32(s + (gid + 8) * kRow + 16 * k + 2 * tig);
-        a[k][2] = lds32(s + gid * kRow + 16 * k + 8 + 2 * tig);
-        a[k][3] = lds32(s + (gid + 8) * kRow + 16 * k + 8 + 2 * tig);
-    }
-}
-
-// acc[j] = (tile) * W^T for a 64x64 W at sW (out rows, in cols)
-__device__ __forceinline__ void layer64(const __half* sWl, const uint32_t (&a)[4][4], float (&acc)[8][4])
-{
-    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const __half* wr = sWl + (8 * j + gid) * kRow + 16 * k + 2 * tig;
-            mma16816(acc[j], a[k], lds32(wr), lds32(wr + 8));
-        }
-    }
-}
-
-// ReLU + FP16 of an accumulator tile, as the next layer's A fragments
-__device__ __forceinline__ void relu_to_a(const float (&acc)[8][4], uint32_t (&a)[4][4])
-{
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        a[k][0] = pack2(fmaxf(acc[2 * k][0], 0.0f), fmaxf(acc[2 * k][1], 0.0f));
-        a[k][1] = pack2(fmaxf(acc[2 * k][2], 0.0f), fmaxf(acc[2 * k][3], 0.0f));
-        a[k][2] = pack2(fmaxf(acc[2 * k + 1][0], 0.0f), fmaxf(acc[2 * k + 1][1], 0.0f));
-        a[k][3] = pack2(fmaxf(acc[2 * k + 1][2], 0.0f), fmaxf(acc[2 * k + 1][3], 0.0f));
-    }
-}
-
-// writes A fragments back as a row-major 16 x 64 tile
-__device__ __forceinline__ void store_a(__half* s, const uint32_t (&a)[4][4])
-{
-    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        *reinterpret_cast<uint32_t*>(s + gid * kRow + 16 * k + 2 * tig) = a[k][0];
-        *reinterpret_cast<uint32_t*>(s + (gid + 8) * kRow + 16 * k + 2 * tig) = a[k][1];
-        *reinterpret_cast<uint32_t*>(s + gid * kRow + 16 * k + 8 + 2 * tig) = a[k][2];
-        *reinterpret_cast<uint32_t*>(s + (gid + 8) * kRow + 16 * k + 8 + 2 * tig) = a[k][3];
-    }
-}
-
-// y = W4 * h4: first 8 outputs (n-tile 0; outputs 0..2 are used)
-__device__ __forceinline__ void output_layer(const __half* sW4, const uint32_t (&a)[4][4], float (&y)[4])
-{
-    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-    y[0] = y[1] = y[2] = y[3] = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const __half* wr = sW4 + gid * kRow + 16 * k + 2 * tig;
-        mma16816(y, a[k], lds32(wr), lds32(wr + 8));
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -440,7 +296,7 @@ __global__ void __launch_bounds__(kTcThreads, kTcBlocksPerSM) k_nrc_infer(const 
 #pragma unroll
                 for (int kb = 0; kb < 4; ++kb)
                     tc::mma_f16_ts(tb + kTcColD, tb + kTcColA + 8 * kb,
-                                   tc::desc_kmajor(sW0 + l * kTcLayerBytes + 256 * kb, 128, 1024), idesc, kb > 0);
+                                   tc::smem_desc(sW0 + l * kTcLayerBytes + 256 * kb, 128, 1024), idesc, kb > 0);
                 tc::mma_commit(bar);
                 if (!tc::mbar_wait_bounded(bar, phase, kTcWaitNs)) timedOut = true;
             }
@@ -492,184 +348,278 @@ __global__ void __launch_bounds__(kTcThreads, kTcBlocksPerSM) k_nrc_infer(const 
 }
 
 // ---------------------------------------------------------------------------
-// Training: forward + backward for every record, summing weight gradients
-// (dW, 17408 floats) and hash-grid gradients (gridGrad) and the loss.
-// Gradients are of sum_i loss_i scaled by kGradScale.
-__global__ void __launch_bounds__(256) k_nrc_train(const StrelkaNrcRecord* __restrict__ recs, const uint32_t* countPtr,
-                                                   uint32_t maxN, const __half* __restrict__ w,
-                                                   const __half2* __restrict__ grid, NrcGeom g, float* __restrict__ dW,
-                                                   float* __restrict__ gridGrad, float* __restrict__ lossSum)
+// Training on the tcgen05 tensor cores: forward + backward for every record,
+// summing weight gradients (dW, kParams floats), hash-grid gradients
+// (gridGrad) and the loss; gradients are of sum_i loss_i scaled by
+// kGradScale.
+//
+// A CTA of 512 threads (four warpgroups) owns tiles of 128 records, record i
+// of a tile in TMEM lane i and in row i of the shared-memory operands.
+// Warpgroup g encodes grid levels 4g..4g+3 (warpgroup 0 also the direction /
+// normal / roughness inputs) and handles accumulator columns 16g..16g+15 in
+// every epilogue.  All operands are in shared memory in one core-matrix
+// layout, (row, col) at (row/8)*1024 + (col/8)*128 + (row%8)*16 + (col%8)*2
+// bytes, which the tensor core reads either way round: as a K-major
+// [rows x K = cols] operand (LBO 128, SBO 1024) or as an MN-major
+// [MN = cols x K = rows] operand (LBO 1024, SBO 128).  So:
+//   forward   h_{l+1} = relu(h_l W_l^T): A = h_l (K-major), B = W_l (K-major);
+//   input gradient d_in = d_l W_l: A = d_l (K-major), B = W_l as MN-major;
+//   weight gradient dW_l += d_l^T h_l over the tile's 128 records (M = 64):
+//     A = d_l as MN-major, B = h_l as MN-major.
+// The five weight-gradient accumulators stay in TMEM for the CTA's lifetime
+// and are added to dW once at the end.  Waits are bounded as in inference.
+constexpr int kTrThreads = 512;
+constexpr uint32_t kTrActBytes = kTcTile * kIn * 2;  // one 128 x 64 FP16 operand, 16 KB
+constexpr uint32_t kTrActOff = kTcWeightBytes;      // x, h1..h4
+constexpr uint32_t kTrDOff = kTrActOff + 5 * kTrActBytes;
+constexpr uint32_t kTrBarOff = kTrDOff + kTrActBytes;
+constexpr uint32_t kTrSmem = kTrBarOff + 64;        // 130 KB: one CTA per SM
+constexpr uint32_t kTrCols = 512;                   // TMEM: D (64) + dW_0..dW_4 (64 each)
+constexpr uint32_t kTrColW = 64;
+
+__device__ __forceinline__ void st_chunk(unsigned char* buf, int row, int chunk, const uint32_t* v)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __half* sW = reinterpret_cast<__half*>(smem);
-    const int warp = threadIdx.x >> 5;
-    __half* sAct = sW + kMatRows * kRow + warp * 5 * 16 * kRow;  // x, h1..h4
-    __half* sD = sW + kMatRows * kRow + 8 * 5 * 16 * kRow + warp * 16 * kRow;
-    float* sDW = reinterpret_cast<float*>(sW + kMatRows * kRow + 8 * 6 * 16 * kRow);
-    load_weights(w, sW);
-    for (int i = threadIdx.x; i < kParams; i += blockDim.x) sDW[i] = 0.0f;
+    *reinterpret_cast<uint4*>(buf + core_offset(row, 8 * chunk)) = make_uint4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ uint4 ld_chunk(const unsigned char* buf, int row, int chunk)
+{
+    return *reinterpret_cast<const uint4*>(buf + core_offset(row, 8 * chunk));
+}
+
+// grid levels l0 .. l0+3 as 4 FP16 pairs
+__device__ __forceinline__ void encode_levels4(const NrcGeom& g, const __half2* __restrict__ grid, int l0, float px,
+                                               float py, float pz, uint32_t (&a)[4])
+{
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float w0[8];
+        uint32_t v0[8];
+        level_fetch(g, grid, l0 + i, px, py, pz, w0, v0);
+        a[i] = level_mix(w0, v0);
+    }
+}
+
+__global__ void __launch_bounds__(kTrThreads, 1) k_nrc_train(const StrelkaNrcRecord* __restrict__ recs, const uint32_t* countPtr,
+                                                             uint32_t maxN, const __half* __restrict__ w,
+                                                             const __half2* __restrict__ grid, NrcGeom g,
+                                                             float* __restrict__ dW, float* __restrict__ gridGrad,
+                                                             float* __restrict__ lossSum, uint32_t* __restrict__ status)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* sW = smem;
+    unsigned char* sAct = smem + kTrActOff;
+    unsigned char* sD = smem + kTrDOff;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + kTrBarOff);
+    uint32_t* slot = reinterpret_cast<uint32_t*>(smem + kTrBarOff + 8);
+    const int tid = threadIdx.x, warp = tid >> 5, wg = tid >> 7, row = tid & (kTcTile - 1);
+    for (int i = tid; i < kMatRows * (kIn / 8); i += kTrThreads) {
+        const int r0 = i >> 3, c = i & 7;
+        const int layer = r0 < 4 * kWidth ? r0 / kWidth : 4;
+        const int r = r0 - layer * kWidth;
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(w + (size_t)r0 * kIn + c * 8));
+        *reinterpret_cast<uint4*>(sW + layer * kTcLayerBytes + core_offset(r, c * 8)) = v;
+    }
+    if (warp == 0) {
+        tc::tmem_alloc(slot, kTrCols);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) tc::mbar_init(bar, 1);
+    tc::fence_proxy_async_smem();
+    tc::fence_before_sync();
     __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tb = *slot;
+    const uint32_t lane = tb + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t sW0 = tc::smem_u32(sW), sA0 = tc::smem_u32(sAct), sD0 = tc::smem_u32(sD);
     const uint32_t n = countPtr ? min(*countPtr, maxN) : maxN;
-    const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-    const uint32_t warpsTotal = gridDim.x * (blockDim.x >> 5);
-    const uint32_t tiles = (n + 15) / 16;
+    const uint32_t tiles = (n + kTcTile - 1) / kTcTile;
+    uint32_t phase = 0;
+    bool timedOut = false, abort = false;
     float lossAcc = 0.0f;
-    for (uint32_t t = blockIdx.x * (blockDim.x >> 5) + warp; t < tiles; t += warpsTotal) {
-        const uint32_t base = t * 16;
-        // forward, keeping x, h1..h4 in shared memory
-        encode_tile(g, grid, recs, base, n, sAct);
-        __syncwarp();
-        uint32_t a[4][4];
-        load_a(sAct, a);
-        float acc[8][4];
-#pragma unroll
-        for (int l = 0; l < 4; ++l) {
-            layer64(sW + l * kWidth * kRow, a, acc);
-            relu_to_a(acc, a);
-            store_a(sAct + (l + 1) * 16 * kRow, a);
+    // one MMA batch: thread 0 waits for it, the others sleep on the barrier
+    auto run = [&](auto issue) -> bool {
+        tc::fence_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after_sync();
+            issue();
+            tc::mma_commit(bar);
+            if (!tc::mbar_wait_bounded(bar, phase, kTcWaitNs)) timedOut = true;
         }
-        float y[4];
-        output_layer(sW + 4 * kWidth * kRow, a, y);
-        // dL/dy of the relative L2 loss, clamped and scaled, as FP16 rows of sD
-        // (16 rows x 16 cols, outputs 3..15 zero)
+        phase ^= 1;
+        const bool bad = __syncthreads_or(timedOut);
+        tc::fence_after_sync();
+        return !bad;
+    };
+    for (uint32_t t = blockIdx.x; t < tiles && !abort; t += gridDim.x) {
+        const bool firstTile = t == blockIdx.x;
+        const uint32_t q = t * kTcTile + (uint32_t)row;
+        const bool valid = q < n;
+        float px = 0.0f, py = 0.0f, pz = 0.0f;
+        // ---- encode: x into sAct[0] ----
+        {
+            uint32_t a[4] = {0u, 0u, 0u, 0u};
+            if (valid) {
+                normalized_position(g, recs[q], px, py, pz);
+                encode_levels4(g, grid, 4 * wg, px, py, pz, a);
+            }
+            st_chunk(sAct, row, wg, a);
+            if (wg == 0) {
+                uint32_t b[16];
+                if (valid) {
+                    encode_rest(recs[q], b);
+                } else {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int r = gid + 8 * h;
-            const uint32_t q = base + (uint32_t)r;
-            float gv[2] = {0.0f, 0.0f};
-            if (q < n) {
+                    for (int i = 0; i < 16; ++i) b[i] = 0u;
+                }
 #pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int c = 2 * tig + e;
-                    if (c < 3) {
-                        const float yy = y[2 * h + e];
+                for (int c = 0; c < 4; ++c) st_chunk(sAct, row, 4 + c, b + 4 * c);
+            }
+            tc::fence_proxy_async_smem();
+        }
+        // ---- forward ----
+        for (int l = 0; l < 5 && !abort; ++l) {
+            const bool ok = run([&] {
+                const uint32_t idesc = l < 4 ? tc::idesc_f16_f32(kTcTile, kWidth) : tc::idesc_f16_f32(kTcTile, kOutPad);
+#pragma unroll
+                for (int kb = 0; kb < 4; ++kb)
+                    tc::mma_f16_ss(tb + kTcColD, tc::smem_desc(sA0 + l * kTrActBytes + 256 * kb, 128, 1024),
+                                   tc::smem_desc(sW0 + l * kTcLayerBytes + 256 * kb, 128, 1024), idesc, kb > 0);
+            });
+            if (!ok) {
+                abort = true;
+                break;
+            }
+            if (l < 4) {
+                uint32_t d[16], a[8];
+                tc::tmem_ld16(lane + kTcColD + 16 * wg, d);
+                tc::tmem_wait_ld();
+                relu_pack16(d, a);
+                st_chunk(sAct + (l + 1) * kTrActBytes, row, 2 * wg, a);
+                st_chunk(sAct + (l + 1) * kTrActBytes, row, 2 * wg + 1, a + 4);
+                tc::fence_proxy_async_smem();
+            } else if (wg == 0) {
+                // dL/dy of the relative L2 loss, clamped and scaled, as row q of d_4
+                uint32_t y[4];
+                tc::tmem_ld4(lane + kTcColD, y);
+                tc::tmem_wait_ld();
+                float gv[3] = {0.0f, 0.0f, 0.0f};
+                if (valid) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const float yy = __uint_as_float(y[c]);
                         const float tt = recs[q].target[c];
                         const float den = yy * yy + 0.01f;
                         const float diff = yy - tt;
                         lossAcc += diff * diff / den;
-                        gv[e] = fminf(fmaxf(2.0f * diff / den, -kGradClamp), kGradClamp) * kGradScale;
+                        gv[c] = fminf(fmaxf(2.0f * diff / den, -kGradClamp), kGradClamp) * kGradScale;
                     }
                 }
+                const uint32_t c0[4] = {pack2(gv[0], gv[1]), pack2(gv[2], 0.0f), 0u, 0u};
+                const uint32_t z[4] = {0u, 0u, 0u, 0u};
+                st_chunk(sD, row, 0, c0);
+#pragma unroll
+                for (int c = 1; c < 8; ++c) st_chunk(sD, row, c, z);
+                tc::fence_proxy_async_smem();
             }
-            *reinterpret_cast<uint32_t*>(sD + r * kRow + 2 * tig) = pack2(gv[0], gv[1]);
-            *reinterpret_cast<uint32_t*>(sD + r * kRow + 8 + 2 * tig) = 0u;
         }
-        __syncwarp();
-
-        // backward through W4 .. W0
-        for (int l = 4; l >= 0; --l) {
-            const int outDim = l == 4 ? kOutPad : kWidth;
-            const __half* sWl = sW + l * kWidth * kRow;
-            const __half* sIn = sAct + l * 16 * kRow;  // this layer's input activation
-            float* gW = sDW + l * kWidth * kIn;
-            // weight gradient dW_l += d^T * in  (M = outDim, N = 64, K = 16 rows)
-            for (int mt = 0; mt < outDim / 16; ++mt) {
-                uint32_t ad[4];
-                {
-                    const int m0 = 16 * mt + gid, m1 = m0 + 8;
-                    ad[0] = pack2h(sD[(2 * tig) * kRow + m0], sD[(2 * tig + 1) * kRow + m0]);
-                    ad[1] = pack2h(sD[(2 * tig) * kRow + m1], sD[(2 * tig + 1) * kRow + m1]);
-                    ad[2] = pack2h(sD[(2 * tig + 8) * kRow + m0], sD[(2 * tig + 9) * kRow + m0]);
-                    ad[3] = pack2h(sD[(2 * tig + 8) * kRow + m1], sD[(2 * tig + 9) * kRow + m1]);
-                }
+        // ---- backward through W4 .. W0 ----
+        for (int l = 4; l >= 0 && !abort; --l) {
+            const bool ok = run([&] {
+                // dW_l += d_l^T h_l: M = 64 outputs, N = 64 inputs, K = the 128 records
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int nn = 8 * j + gid;
-                    const uint32_t b0 = pack2h(sIn[(2 * tig) * kRow + nn], sIn[(2 * tig + 1) * kRow + nn]);
-                    const uint32_t b1 = pack2h(sIn[(2 * tig + 8) * kRow + nn], sIn[(2 * tig + 9) * kRow + nn]);
-                    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                    mma16816(c, ad, b0, b1);
-                    const int row0 = 16 * mt + gid, col0 = 8 * j + 2 * tig;
-                    atomicAdd(&gW[row0 * kIn + col0], c[0]);
-                    atomicAdd(&gW[row0 * kIn + col0 + 1], c[1]);
-                    atomicAdd(&gW[(row0 + 8) * kIn + col0], c[2]);
-                    atomicAdd(&gW[(row0 + 8) * kIn + col0 + 1], c[3]);
-                }
+                for (int ks = 0; ks < 8; ++ks)
+                    tc::mma_f16_ss(tb + kTrColW + 64 * l, tc::smem_desc(sD0 + 2048 * ks, 1024, 128),
+                                   tc::smem_desc(sA0 + l * kTrActBytes + 2048 * ks, 1024, 128),
+                                   tc::idesc_f16_f32(64, kIn, true, true), (!firstTile || ks > 0) ? 1u : 0u);
+                // d_in = d_l W_l: M = 128 records, N = 64 inputs, K = the layer's outputs
+                const int ksteps = l == 4 ? kOutPad / 16 : kWidth / 16;
+                for (int kb = 0; kb < ksteps; ++kb)
+                    tc::mma_f16_ss(tb + kTcColD, tc::smem_desc(sD0 + 256 * kb, 128, 1024),
+                                   tc::smem_desc(sW0 + l * kTcLayerBytes + 2048 * kb, 1024, 128),
+                                   tc::idesc_f16_f32(kTcTile, kIn, false, true), kb > 0 ? 1u : 0u);
+            });
+            if (!ok) {
+                abort = true;
+                break;
             }
-            // input gradient d_in = W_l^T * d  (N = 64 in-dims, K = outDim)
-            float dacc[8][4];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) dacc[j][0] = dacc[j][1] = dacc[j][2] = dacc[j][3] = 0.0f;
-            for (int k = 0; k < outDim / 16; ++k) {
-                uint32_t ak[4];
-                ak[0] = lds32(sD + gid * kRow + 16 * k + 2 * tig);
-                ak[1] = lds32(sD + (gid + 8) * kRow + 16 * k + 2 * tig);
-                ak[2] = lds32(sD + gid * kRow + 16 * k + 8 + 2 * tig);
-                ak[3] = lds32(sD + (gid + 8) * kRow + 16 * k + 8 + 2 * tig);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int nn = 8 * j + gid;
-                    const int k0 = 16 * k + 2 * tig;
-                    const uint32_t b0 = pack2h(sWl[k0 * kRow + nn], sWl[(k0 + 1) * kRow + nn]);
-                    const uint32_t b1 = pack2h(sWl[(k0 + 8) * kRow + nn], sWl[(k0 + 9) * kRow + nn]);
-                    mma16816(dacc[j], ak, b0, b1);
-                }
-            }
-            __syncwarp();
             if (l > 0) {
-                // ReLU mask of the input activation (h_l > 0), then FP16 into sD
+                // ReLU mask of this layer's input (h_l > 0), FP16 into d_{l-1}
+                uint32_t d[16], a[8];
+                tc::tmem_ld16(lane + kTcColD + 16 * wg, d);
+                tc::tmem_wait_ld();
+                const unsigned char* hl = sAct + l * kTrActBytes;
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
+                for (int c = 0; c < 2; ++c) {
+                    const uint4 hv = ld_chunk(hl, row, 2 * wg + c);
+                    const uint32_t hw[4] = {hv.x, hv.y, hv.z, hv.w};
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int r = gid + 8 * h, c0 = 8 * j + 2 * tig;
-                        const float m0 = __half2float(sIn[r * kRow + c0]) > 0.0f ? 1.0f : 0.0f;
-                        const float m1 = __half2float(sIn[r * kRow + c0 + 1]) > 0.0f ? 1.0f : 0.0f;
-                        *reinterpret_cast<uint32_t*>(sD + r * kRow + c0) =
-                            pack2(dacc[j][2 * h] * m0, dacc[j][2 * h + 1] * m1);
+                    for (int j = 0; j < 4; ++j) {
+                        const float2 h2 = __half22float2(*reinterpret_cast<const __half2*>(&hw[j]));
+                        const float g0 = h2.x > 0.0f ? __uint_as_float(d[8 * c + 2 * j]) : 0.0f;
+                        const float g1 = h2.y > 0.0f ? __uint_as_float(d[8 * c + 2 * j + 1]) : 0.0f;
+                        a[4 * c + j] = pack2(g0, g1);
                     }
                 }
-                __syncwarp();
+                st_chunk(sD, row, 2 * wg, a);
+                st_chunk(sD, row, 2 * wg + 1, a + 4);
+                tc::fence_proxy_async_smem();
             } else {
-                // input gradient of the grid features (columns 0..31) as FP32
-                float* sG = reinterpret_cast<float*>(sD);
+                // gradients of this warpgroup's grid features (levels 4g..4g+3),
+                // scattered through the trilinear weights
+                uint32_t d[8];
+                tc::tmem_ld8(lane + kTcColD + 8 * wg, d);
+                tc::tmem_wait_ld();
+                if (valid) {
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
+                    for (int i = 0; i < 4; ++i) {
+                        Corner c;
+                        level_corners(g, 4 * wg + i, px, py, pz, c);
+                        const float g0 = __uint_as_float(d[2 * i]), g1 = __uint_as_float(d[2 * i + 1]);
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int r = gid + 8 * h, c0 = 8 * j + 2 * tig;
-                        sG[r * 32 + c0] = dacc[j][2 * h];
-                        sG[r * 32 + c0 + 1] = dacc[j][2 * h + 1];
-                    }
-                }
-                __syncwarp();
-            }
-        }
-        // scatter the grid gradients through the trilinear weights
-        {
-            const float* sG = reinterpret_cast<const float*>(sD);
-            const int r = lane & 15;
-            const uint32_t q = base + (uint32_t)r;
-            if (q < n) {
-                const StrelkaNrcRecord rec = recs[q];
-                float px, py, pz;
-                normalized_position(g, rec, px, py, pz);
-                const int l0 = (lane >> 4) * 8;
-                for (int l = l0; l < l0 + 8; ++l) {
-                    Corner c;
-                    level_corners(g, l, px, py, pz, c);
-                    const float g0 = sG[r * 32 + 2 * l], g1 = sG[r * 32 + 2 * l + 1];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        atomicAdd(&gridGrad[2 * (size_t)c.idx[k]], c.w[k] * g0);
-                        atomicAdd(&gridGrad[2 * (size_t)c.idx[k] + 1], c.w[k] * g1);
+                        for (int k = 0; k < 8; ++k)
+                            atomicAdd(reinterpret_cast<float2*>(gridGrad) + c.idx[k], make_float2(c.w[k] * g0, c.w[k] * g1));
                     }
                 }
             }
         }
-        __syncwarp();
     }
-    // reduce the block's weight gradients and loss
+    // loss, and the weight gradients accumulated in TMEM (row r of an M = 64
+    // accumulator sits in lane (r % 16) + 32 (r / 16))
     for (int off = 16; off > 0; off >>= 1) lossAcc += __shfl_xor_sync(0xffffffffu, lossAcc, off);
-    if (lane == 0 && lossSum) atomicAdd(lossSum, lossAcc);
+    if ((tid & 31) == 0 && lossSum && lossAcc != 0.0f) atomicAdd(lossSum, lossAcc);
+    tc::fence_before_sync();
     __syncthreads();
-    for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
-        const float v = sDW[i];
-        if (v != 0.0f) atomicAdd(&dW[i], v);
+    tc::fence_after_sync();
+    if (blockIdx.x < tiles && !abort) {
+        const int sub = warp & 3;
+        for (int l = warp >> 2; l < 5; l += kTrThreads / 128) {
+            const int rows = l == 4 ? kOutPad : kWidth;
+            const int r = 16 * sub + (tid & 15);
+            for (int c0 = 0; c0 < kIn; c0 += 16) {
+                uint32_t d[16];
+                tc::tmem_ld16(tb + ((uint32_t)(sub * 32) << 16) + kTrColW + 64 * l + c0, d);
+                tc::tmem_wait_ld();
+                if ((tid & 31) < 16 && r < rows) {
+                    float* dst = dW + (size_t)l * kWidth * kIn + (size_t)r * kIn + c0;
+#pragma unroll
+                    for (int c = 0; c < 16; ++c) {
+                        const float v = __uint_as_float(d[c]);
+                        if (v != 0.0f) atomicAdd(dst + c, v);
+                    }
+                }
+            }
+        }
+    }
+    if (timedOut) atomicOr(status, STRELKA_DEV_MMA_TIMEOUT);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(tb, kTrCols);
     }
 }
 
-// Adam over a parameter array (FP32 master + FP16 copy).
 __global__ void k_nrc_adam(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v, const float* __restrict__ grad,
                            __half* __restrict__ ph, size_t n, float lr, float gscale, float b1, float b2, float eps,
                            float c1, float c2, const uint32_t* countPtr)
@@ -693,7 +643,6 @@ __global__ void k_to_half(const float* __restrict__ p, __half* __restrict__ ph, 
         ph[i] = __float2half(p[i]);
 }
 
-size_t train_smem() { return (size_t)(kMatRows * kRow + 8 * 6 * 16 * kRow) * sizeof(__half) + kParams * sizeof(float); }
 
 }  // namespace
 
@@ -799,7 +748,8 @@ extern "C" int strelka_nrc_create(const StrelkaNrcConfig* cfg, StrelkaNrc** out)
     k_to_half<<<grid_blocks(nrc, nrc->gridN, 256), 256>>>(nrc->grid, nrc->gridHalf, nrc->gridN);
     cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
     cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributePreferredSharedMemoryCarveout, kTcCarveoutPercent);
-    cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)train_smem());
+    cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrSmem);
+    cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributePreferredSharedMemoryCarveout, kTcCarveoutPercent);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         nrc_free(nrc);
@@ -839,11 +789,11 @@ int nrc_gradients_device(StrelkaNrc* nrc, const StrelkaNrcRecord* recs, const ui
     SB_CUDA_TRY(cudaMemsetAsync(nrc->gridGrad, 0, nrc->gridN * 4, st));
     SB_CUDA_TRY(cudaMemsetAsync(nrc->loss, 0, 4, st));
     if (maxN == 0) return STRELKA_OK;
-    const int tiles = (int)((maxN + 15) / 16);
-    const int blocks = std::max(1, std::min((tiles + 7) / 8, nrc->numSMs));
-    k_nrc_train<<<blocks, 256, train_smem(), st>>>(recs, countPtr, maxN, nrc->mlpHalf,
-                                                  reinterpret_cast<const __half2*>(nrc->gridHalf), nrc->geom,
-                                                  nrc->mlpGrad, nrc->gridGrad, nrc->loss);
+    const int tiles = (int)((maxN + kTcTile - 1) / kTcTile);
+    const int blocks = std::max(1, std::min(tiles, nrc->numSMs));
+    k_nrc_train<<<blocks, kTrThreads, kTrSmem, st>>>(recs, countPtr, maxN, nrc->mlpHalf,
+                                                    reinterpret_cast<const __half2*>(nrc->gridHalf), nrc->geom,
+                                                    nrc->mlpGrad, nrc->gridGrad, nrc->loss, nrc->status);
     SB_CUDA_TRY(cudaGetLastError());
     return STRELKA_OK;
 }

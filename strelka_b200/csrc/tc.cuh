@@ -78,20 +78,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // --- descriptors ---
-// K-major, no swizzle shared-memory matrix descriptor (sm_100 format:
-// start >> 4 in bits 0..13, leading byte offset >> 4 in 16..29, stride byte
-// offset >> 4 in 32..45, version 1 in bits 46..47, layout type 0).
-__device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+// Non-swizzled shared-memory matrix descriptor (sm_100 format: start >> 4
+// in bits 0..13, leading byte offset >> 4 in 16..29, stride byte offset >> 4
+// in 32..45, version 1 in bits 46..47, layout type 0).  K-major operands: LBO
+// = distance between core matrices along K, SBO = along M/N.  MN-major
+// operands (core matrix = 8 K-rows of 8 contiguous M/N elements): LBO =
+// distance along K, SBO = along M/N as well.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
 {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
-// Instruction descriptor of kind::f16 with F16 A and B (both K-major) and an
-// F32 accumulator: D format bits 4..5 = 1, N >> 3 in bits 17..22, M >> 4 in
-// bits 24..28.
-__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N)
+// Instruction descriptor of kind::f16 with F16 A and B and an F32
+// accumulator: D format bits 4..5 = 1, A / B MN-major flags in bits 15 / 16
+// (0 = K-major), N >> 3 in bits 17..22, M >> 4 in bits 24..28.
+__host__ __device__ constexpr uint32_t idesc_f16_f32(int M, int N, bool aMN = false, bool bMN = false)
 {
-    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+    return (1u << 4) | ((aMN ? 1u : 0u) << 15) | ((bMN ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
 }
 
 // --- MMA: D[tmem] (+)= A[tmem] * B[smem]^T, issued by one thread ---
@@ -102,6 +106,16 @@ __device__ __forceinline__ void mma_f16_ts(uint32_t dTmem, uint32_t aTmem, uint6
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(dTmem),
         "r"(aTmem), "l"(bDesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+// --- MMA: D[tmem] (+)= A[smem] * B[smem]^T, issued by one thread ---
+__device__ __forceinline__ void mma_f16_ss(uint32_t dTmem, uint64_t aDesc, uint64_t bDesc, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dTmem),
+        "l"(aDesc), "l"(bDesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
 // the mbarrier completes one phase when every MMA this thread issued so far is done
@@ -119,6 +133,13 @@ __device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4])
 {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t* r)
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                  : "r"(taddr));
 }
 
