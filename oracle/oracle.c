@@ -472,14 +472,11 @@ static int any_hit(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, unsig
 }
 
 /* ------------------------------------------------------------------------- */
-/* The GPU's node-pair traversal, replayed for visit counts and for its exact
- * closest-hit tie order (not a reference algorithm).  For an inner node n the
- * children are L = n+1 and R = escape(L) (the implicit tree of the depth-first
- * layout); one "record" step tests both: a leaf child by Moller-Trumbore, an
- * inner child by its box.  Closest hit descends into the nearer child first
- * with a 32-entry stack and the 2^-12 pruning rule; any hit keeps the
- * depth-first order.  A full stack falls back to the stackless loops. */
-#define PAIR_STACK 32
+/* Helpers of the GPU traversal replay below (not a reference algorithm): for
+ * an inner node n the children are L = n+1 and R = escape(L), the implicit
+ * tree of the depth-first layout.  A full stack falls back to the stackless
+ * loops. */
+#define WIDE_STACK 64
 static int node_is_leaf(const OracleScene* s, uint32_t c) { return (uint32_t)s->nodes[c].instId != INVALID_INDEX; }
 
 static void pair_children(const OracleScene* s, uint32_t n, uint32_t* L, uint32_t* R)
@@ -508,7 +505,7 @@ static int leaf_test(const OracleScene* s, uint32_t leaf, v3 o, v3 d, float* t, 
 }
 
 static void stackless_closest_from(const OracleScene* s, v3 o, float tmax, v3 d, const float inv[3], uint32_t node, float* minHit,
-                                   Hit* hit, int* found, unsigned long long* nI, unsigned long long* nL)
+                                   uint32_t* best, Hit* hit, int* found, unsigned long long* nI, unsigned long long* nL)
 {
     float oo[3] = {o.x, o.y, o.z};
     uint64_t cap = 2ull * s->numNodes + 2, visits = 0;
@@ -519,8 +516,9 @@ static void stackless_closest_from(const OracleScene* s, v3 o, float tmax, v3 d,
             (*nL)++;
             float t, bu = 0, bv = 0;
             uint32_t iid, pid;
-            if (leaf_test(s, node, o, d, &t, &bu, &bv, &iid, &pid) && t < tmax && t < *minHit) {
+            if (leaf_test(s, node, o, d, &t, &bu, &bv, &iid, &pid) && t < tmax && (t < *minHit || (t == *minHit && node < *best))) {
                 *minHit = t;
+                *best = node;
                 hit->t = t; hit->bary[0] = bu; hit->bary[1] = bv; hit->instId = iid; hit->primId = pid;
                 *found = 1;
             }
@@ -538,76 +536,151 @@ static void stackless_closest_from(const OracleScene* s, v3 o, float tmax, v3 d,
     }
 }
 
-static int pair_closest(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, unsigned long long* nI, unsigned long long* nL)
+/* The GPU's 4-wide traversal (csrc/traverse.cuh), replayed over the binary
+ * tree.  A 4-wide node is a binary inner node P at even depth; its entries, in
+ * order, are for each binary child c of P: c itself when it is a leaf
+ * (tested without a box, except at the root, whose box gates it), otherwise
+ * c's two children, an inner one with its
+ * own box and a leaf one gated by c's box.  One step processes a node: all
+ * entry boxes first (pruned against the best hit at the node's entry), then
+ * the leaves that passed in order; closest hit sorts the inner candidates by
+ * entry distance with the GPU's compare-exchange network, continues with the
+ * nearest and pushes the others farthest first; any hit keeps the
+ * depth-first order.  Refs: W_LEAF marks a leaf (W_NOBOX: without a box);
+ * inner refs are binary node indices here. */
+#define W_LEAF 0x80000000u
+#define W_NOBOX 0x40000000u
+
+static void wide_entries(const OracleScene* s, uint32_t P, uint32_t ref[4], uint32_t gate[4])
+{
+    for (int k = 0; k < 4; ++k) {
+        ref[k] = INVALID_INDEX;
+        gate[k] = INVALID_INDEX;
+    }
+    int e = 0;
+    uint32_t child[2];
+    pair_children(s, P, &child[0], &child[1]);
+    for (int k = 0; k < 2; ++k) {
+        uint32_t c = child[k];
+        if (c == INVALID_INDEX) continue;
+        if (node_is_leaf(s, c)) {
+            /* at the root, gated by the root's box (the reference tests it first) */
+            if (P == 0) {
+                ref[e] = c | W_LEAF;
+                gate[e++] = 0;
+            } else {
+                ref[e++] = c | W_LEAF | W_NOBOX;
+            }
+            continue;
+        }
+        uint32_t g[2];
+        pair_children(s, c, &g[0], &g[1]);
+        for (int j = 0; j < 2; ++j) {
+            if (g[j] == INVALID_INDEX) continue;
+            if (node_is_leaf(s, g[j])) {
+                ref[e] = g[j] | W_LEAF;
+                gate[e] = c;
+            } else {
+                ref[e] = g[j];
+                gate[e] = g[j];
+            }
+            ++e;
+        }
+    }
+}
+
+static void wide_cswap(float* t, uint32_t* r, int a, int b)
+{
+    if (t[b] < t[a]) {
+        float x = t[a]; t[a] = t[b]; t[b] = x;
+        uint32_t y = r[a]; r[a] = r[b]; r[b] = y;
+    }
+}
+
+static int wide_closest(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, unsigned long long* nI, unsigned long long* nL)
 {
     float inv[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
     float oo[3] = {o.x, o.y, o.z};
     float minHit = 1e9f;
+    uint32_t best = INVALID_INDEX; /* node index of the best hit's leaf: ties go to the first in depth-first order */
     int found = 0;
     if (s->numNodes == 0) return 0;
-    uint32_t stackN[PAIR_STACK];
-    float stackT[PAIR_STACK];
+    uint32_t stackN[WIDE_STACK];
+    float stackT[WIDE_STACK];
     int sp = 0;
-    uint32_t cur = 0, steps = 0;
+    uint32_t cur = node_is_leaf(s, 0) ? (W_LEAF | W_NOBOX) : 0, steps = 0;
     for (;;) {
         if (cur != INVALID_INDEX) {
-            if (cur >= s->numNodes || ++steps > s->numNodes + 1u) break;
-            if (cur == 0 && node_is_leaf(s, 0)) {
+            if (++steps > s->numNodes + 1u) break;
+            if (cur & W_LEAF) {
                 (*nL)++;
                 float t, bu = 0, bv = 0;
-                uint32_t iid, pid;
-                if (leaf_test(s, 0, o, d, &t, &bu, &bv, &iid, &pid) && t < tmax && t < minHit) {
+                uint32_t iid, pid, leaf = cur & ~(W_LEAF | W_NOBOX);
+                if (leaf_test(s, leaf, o, d, &t, &bu, &bv, &iid, &pid) && t < tmax && (t < minHit || (t == minHit && leaf < best))) {
                     minHit = t;
+                    best = leaf;
                     hit->t = t; hit->bary[0] = bu; hit->bary[1] = bv; hit->instId = iid; hit->primId = pid;
                     found = 1;
                 }
                 cur = INVALID_INDEX;
             } else {
+                if (cur >= s->numNodes) break;
                 (*nI)++;
-                uint32_t L, R;
-                pair_children(s, cur, &L, &R);
-                int goL = 0, goR = 0;
-                float tL = 0.0f, tR = 0.0f;
-                for (int k = 0; k < 2; ++k) {
-                    uint32_t c = k == 0 ? L : R;
-                    if (c == INVALID_INDEX) continue;
-                    if (node_is_leaf(s, c)) {
+                uint32_t ref[4], gate[4];
+                wide_entries(s, cur, ref, gate);
+                float bt[4];
+                int pass[4];
+                float lim0 = minHit * PRUNE_SCALE;
+                for (int k = 0; k < 4; ++k) {
+                    bt[k] = 0.0f;
+                    pass[k] = 0;
+                    if (ref[k] == INVALID_INDEX) continue;
+                    if (ref[k] & W_NOBOX) {
+                        pass[k] = 1;
+                        continue;
+                    }
+                    const BVHNode* b = &s->nodes[gate[k]];
+                    pass[k] = oracle_intersect_ray_box(oo, inv, b->minBounds, b->maxBounds, &bt[k]) && !(bt[k] > tmax) &&
+                              !(bt[k] > lim0);
+                }
+                float ct[4];
+                uint32_t cr[4];
+                for (int k = 0; k < 4; ++k) {
+                    ct[k] = INFINITY;
+                    cr[k] = INVALID_INDEX;
+                    if (!pass[k]) continue;
+                    if (ref[k] & W_LEAF) {
                         (*nL)++;
                         float t, bu = 0, bv = 0;
-                        uint32_t iid, pid;
-                        if (leaf_test(s, c, o, d, &t, &bu, &bv, &iid, &pid) && t < tmax && t < minHit) {
+                        uint32_t iid, pid, leaf = ref[k] & ~(W_LEAF | W_NOBOX);
+                        if (leaf_test(s, leaf, o, d, &t, &bu, &bv, &iid, &pid) && t < tmax && (t < minHit || (t == minHit && leaf < best))) {
                             minHit = t;
+                            best = leaf;
                             hit->t = t; hit->bary[0] = bu; hit->bary[1] = bv; hit->instId = iid; hit->primId = pid;
                             found = 1;
                         }
                     } else {
-                        float bt;
-                        int h = oracle_intersect_ray_box(oo, inv, s->nodes[c].minBounds, s->nodes[c].maxBounds, &bt);
-                        if (k == 0) { goL = h; tL = bt; } else { goR = h; tR = bt; }
+                        ct[k] = bt[k];
+                        cr[k] = ref[k];
                     }
                 }
+                wide_cswap(ct, cr, 0, 1);
+                wide_cswap(ct, cr, 2, 3);
+                wide_cswap(ct, cr, 0, 2);
+                wide_cswap(ct, cr, 1, 3);
+                wide_cswap(ct, cr, 1, 2);
                 float lim = minHit * PRUNE_SCALE;
-                goL = goL && !(tL > tmax) && !(tL > lim);
-                goR = goR && !(tR > tmax) && !(tR > lim);
-                if (goL && goR) {
-                    int leftNear = tL <= tR;
-                    uint32_t nearC = leftNear ? L : R, farC = leftNear ? R : L;
-                    float farT = leftNear ? tR : tL;
-                    if (sp < PAIR_STACK) {
-                        stackN[sp] = farC;
-                        stackT[sp] = farT;
+                cur = (cr[0] != INVALID_INDEX && !(ct[0] > lim)) ? cr[0] : INVALID_INDEX;
+                for (int k = 3; k >= 1; --k) {
+                    if (cr[k] == INVALID_INDEX || ct[k] > lim) continue;
+                    if (sp < WIDE_STACK) {
+                        stackN[sp] = cr[k];
+                        stackT[sp] = ct[k];
                         ++sp;
-                        cur = nearC;
                     } else {
-                        stackless_closest_from(s, o, tmax, d, inv, 0, &minHit, hit, &found, nI, nL);
+                        stackless_closest_from(s, o, tmax, d, inv, 0, &minHit, &best, hit, &found, nI, nL);
                         return found;
                     }
-                } else if (goL) {
-                    cur = L;
-                } else if (goR) {
-                    cur = R;
-                } else {
-                    cur = INVALID_INDEX;
                 }
             }
         }
@@ -626,99 +699,83 @@ static int pair_closest(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, 
     return found;
 }
 
-static int pair_any(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, unsigned long long* nI, unsigned long long* nL)
+static int wide_any(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, unsigned long long* nI, unsigned long long* nL)
 {
     float inv[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
     float oo[3] = {o.x, o.y, o.z};
     if (s->numNodes == 0) return 0;
-    uint32_t stackN[PAIR_STACK];
+    uint32_t stackN[WIDE_STACK];
     int sp = 0;
-    uint32_t cur = 0, steps = 0;
+    uint32_t cur = node_is_leaf(s, 0) ? (W_LEAF | W_NOBOX) : 0, steps = 0;
     for (;;) {
-        if (cur != INVALID_INDEX) {
-            if (cur >= s->numNodes || ++steps > s->numNodes + 1u) return 0;
-            if (cur == 0 && node_is_leaf(s, 0)) {
-                (*nL)++;
-                float t, bu, bv;
-                uint32_t iid, pid;
-                int is = leaf_test(s, 0, o, d, &t, &bu, &bv, &iid, &pid);
-                hit->t = t;
-                if (is && t < tmax) {
-                    hit->instId = iid;
-                    hit->primId = pid;
-                    return 1;
+        if (cur != INVALID_INDEX && !(cur & W_LEAF)) {
+            if (++steps > s->numNodes + 1u || cur >= s->numNodes) return 0;
+            (*nI)++;
+            uint32_t ref[4], gate[4];
+            wide_entries(s, cur, ref, gate);
+            int pass[4];
+            for (int k = 0; k < 4; ++k) {
+                pass[k] = 0;
+                if (ref[k] == INVALID_INDEX) continue;
+                if (ref[k] & W_NOBOX) {
+                    pass[k] = 1;
+                    continue;
                 }
-                cur = INVALID_INDEX;
-            } else {
-                (*nI)++;
-                uint32_t L, R;
-                pair_children(s, cur, &L, &R);
-                int goL = 0, rPending = 0;
-                if (L != INVALID_INDEX) {
-                    float bt;
-                    goL = node_is_leaf(s, L) ||
-                          (oracle_intersect_ray_box(oo, inv, s->nodes[L].minBounds, s->nodes[L].maxBounds, &bt) &&
-                           !(bt > tmax));
-                }
-                if (R != INVALID_INDEX) {
-                    float bt;
-                    rPending = node_is_leaf(s, R) ||
-                               (oracle_intersect_ray_box(oo, inv, s->nodes[R].minBounds, s->nodes[R].maxBounds, &bt) &&
-                                !(bt > tmax));
-                }
-                if (goL) {
-                    if (rPending) {
-                        if (sp < PAIR_STACK) {
-                            stackN[sp++] = R;
-                        } else {
-                            /* stackless loop from L: the rest of the tree in the same order */
-                            uint32_t node = L;
-                            uint64_t cap = 2ull * s->numNodes + 2, visits = 0;
-                            while (node != INVALID_INDEX) {
-                                if (node >= s->numNodes || ++visits > cap) break;
-                                const BVHNode* n = &s->nodes[node];
-                                if ((uint32_t)n->instId != INVALID_INDEX) {
-                                    (*nL)++;
-                                    float t, bu, bv;
-                                    uint32_t iid, pid;
-                                    int is = leaf_test(s, node, o, d, &t, &bu, &bv, &iid, &pid);
-                                    hit->t = t;
-                                    if (is && t < tmax) {
-                                        hit->instId = iid;
-                                        hit->primId = pid;
-                                        return 1;
-                                    }
-                                } else {
-                                    (*nI)++;
-                                    float bt;
-                                    if (oracle_intersect_ray_box(oo, inv, n->minBounds, n->maxBounds, &bt) && !(bt > tmax)) {
-                                        ++node;
-                                        continue;
-                                    }
-                                }
-                                node = (uint32_t)n->nodeOffset;
-                            }
-                            return 0;
-                        }
-                    }
-                    cur = L;
-                } else if (rPending) {
-                    cur = R;
-                } else {
-                    cur = INVALID_INDEX;
-                }
+                const BVHNode* b = &s->nodes[gate[k]];
+                float bt;
+                pass[k] = oracle_intersect_ray_box(oo, inv, b->minBounds, b->maxBounds, &bt) && !(bt > tmax);
             }
+            uint32_t first = INVALID_INDEX;
+            for (int k = 3; k >= 0; --k) {
+                if (!pass[k]) continue;
+                if (first != INVALID_INDEX) {
+                    if (sp < WIDE_STACK) {
+                        stackN[sp++] = first;
+                    } else {
+                        /* the reference's stackless loop from the root */
+                        uint32_t node = 0;
+                        uint64_t cap = 2ull * s->numNodes + 2, visits = 0;
+                        while (node != INVALID_INDEX) {
+                            if (node >= s->numNodes || ++visits > cap) break;
+                            const BVHNode* n = &s->nodes[node];
+                            if ((uint32_t)n->instId != INVALID_INDEX) {
+                                (*nL)++;
+                                float t, bu, bv;
+                                uint32_t iid, pid;
+                                int is = leaf_test(s, node, o, d, &t, &bu, &bv, &iid, &pid);
+                                hit->t = t;
+                                if (is && t < tmax) {
+                                    hit->instId = iid;
+                                    hit->primId = pid;
+                                    return 1;
+                                }
+                            } else {
+                                (*nI)++;
+                                float bt;
+                                if (oracle_intersect_ray_box(oo, inv, n->minBounds, n->maxBounds, &bt) && !(bt > tmax)) {
+                                    ++node;
+                                    continue;
+                                }
+                            }
+                            node = (uint32_t)n->nodeOffset;
+                        }
+                        return 0;
+                    }
+                }
+                first = ref[k];
+            }
+            cur = first;
         }
         for (;;) {
             if (cur == INVALID_INDEX) {
                 if (sp == 0) return 0;
                 cur = stackN[--sp];
             }
-            if (!node_is_leaf(s, cur)) break;
+            if (!(cur & W_LEAF)) break;
             (*nL)++;
             float t, bu, bv;
             uint32_t iid, pid;
-            int is = leaf_test(s, cur, o, d, &t, &bu, &bv, &iid, &pid);
+            int is = leaf_test(s, cur & ~(W_LEAF | W_NOBOX), o, d, &t, &bu, &bv, &iid, &pid);
             hit->t = t;
             if (is && t < tmax) {
                 hit->instId = iid;
@@ -747,7 +804,7 @@ int oracle_trace(const OracleScene* s, const Ray* rays, uint32_t n, Hit* hits, u
         h.primId = INVALID_INDEX;
         unsigned long long ni = 0, nl = 0;
         int f;
-        if (prune == 2) f = mode == 1 ? pair_any(s, o, r->o.w, d, &h, &ni, &nl) : pair_closest(s, o, r->o.w, d, &h, &ni, &nl);
+        if (prune == 2) f = mode == 1 ? wide_any(s, o, r->o.w, d, &h, &ni, &nl) : wide_closest(s, o, r->o.w, d, &h, &ni, &nl);
         else f = mode == 1 ? any_hit(s, o, r->o.w, d, &h, &ni, &nl) : closest_hit(s, o, r->o.w, d, &h, prune, &ni, &nl);
         if (!f) {
             h.instId = INVALID_INDEX;

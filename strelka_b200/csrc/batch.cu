@@ -503,7 +503,8 @@ struct SceneRec {
     const uint32_t* ib;
     const InstanceConstants* inst;
     uint64_t version;
-    float4* rec;
+    void* mem;  // derived tables (internal.h SceneTables)
+    SceneTables tables;
 };
 
 }  // namespace
@@ -776,7 +777,7 @@ extern "C" int strelka_batch_destroy(StrelkaBatch* b)
     cudaDeviceSynchronize();
     drop_graphs(b);
     free_wave(b);
-    for (SceneRec& r : b->scenes) cudaFree(r.rec);
+    for (SceneRec& r : b->scenes) cudaFree(r.mem);
     void* ptrs[] = {b->jobsDev, b->prefixDev, b->ctl, b->status, b->srgbLut, b->fetch, b->hist, b->offsets};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -824,21 +825,24 @@ extern "C" int strelka_batch_set_jobs(StrelkaBatch* b, const PathTracerDesc* job
     uint32_t keyBase = 0;
     for (uint32_t j = 0; j < numJobs; ++j) {
         const PathTracerDesc& d = jobs[j];
-        float4* rec = nullptr;
+        const SceneTables* tables = nullptr;
         for (SceneRec& r : b->scenes)
             if (r.nodes == d.bvhNodes && r.numNodes == d.numNodes && r.vb == d.vb && r.ib == d.ib &&
                 r.inst == d.instanceConst && r.version == d.sceneVersion)
-                rec = r.rec;
-        if (!rec) {
-            SB_CUDA_TRY(cudaMalloc(&rec, (size_t)std::max<uint32_t>(d.numNodes, 1) * 4 * sizeof(float4)));
-            b->scenes.push_back(SceneRec{d.bvhNodes, d.numNodes, d.vb, d.ib, d.instanceConst, d.sceneVersion, rec});
-            int rc = launch_prep_records(d.bvhNodes, d.numNodes, d.instanceConst, d.numInstances, d.ib, d.numIndices,
-                                         d.vb, d.numVertices, rec, b->status, b->numSMs, st);
+                tables = &r.tables;
+        if (!tables) {
+            void* mem = nullptr;
+            SB_CUDA_TRY(cudaMalloc(&mem, scene_tables_bytes(d.numNodes)));
+            b->scenes.push_back(SceneRec{d.bvhNodes, d.numNodes, d.vb, d.ib, d.instanceConst, d.sceneVersion, mem,
+                                         scene_tables(mem, d.numNodes)});
+            tables = &b->scenes.back().tables;
+            int rc = launch_prep_tables(d.bvhNodes, d.numNodes, d.instanceConst, d.numInstances, d.ib, d.numIndices,
+                                        d.vb, d.numVertices, *tables, b->status, b->numSMs, st);
             if (rc) return rc;
         }
         BatchJobDev& J = host[j];
         memset(&J, 0, sizeof(J));
-        J.s = scene_from_desc(&d, rec, b->srgbLut, b->status);
+        J.s = scene_from_desc(&d, *tables, b->srgbLut, b->status);
         J.ubo = d.constants;
         J.sampleBuffer = d.sampleBuffer;
         J.numPaths = prefix[j + 1] - prefix[j];

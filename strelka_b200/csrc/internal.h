@@ -13,11 +13,28 @@ namespace sb {
 void srgb_lut_host(float* lut);
 // Argument checks of a scene descriptor shared by every entry point.
 int validate_scene_desc(const PathTracerDesc* d);
-// Builds the node-pair record table (4 float4 per node) of a scene on `st`.
-int launch_prep_records(const BVHNode* nodes, uint32_t numNodes, const InstanceConstants* inst, uint32_t numInstances,
-                        const uint32_t* ib, uint32_t numIndices, const Vertex* vb, uint32_t numVertices, float4* rec,
-                        uint32_t* status, int numSMs, cudaStream_t st);
-// The device view of a descriptor's scene with its record table.
-DevScene scene_from_desc(const PathTracerDesc* d, const float4* rec, const float* srgbLut, uint32_t* status);
+// Device tables derived from a scene's BVH, all in one allocation of
+// scene_tables_bytes(numNodes) bytes: the leaf-triangle records (4 float4 per
+// node slot), the 4-wide BVH (8 float4 per node, at most numNodes/2 + 1
+// nodes) and the scratch of its build.
+struct SceneTables {
+    float4* rec = nullptr;
+    float4* wide = nullptr;
+    uint32_t wideCap = 0;
+    uint32_t* parent = nullptr;
+    uint32_t* flag = nullptr;
+    uint32_t* map = nullptr;
+    void* scan = nullptr;
+    size_t scanBytes = 0;
+};
+size_t scene_tables_bytes(uint32_t numNodes);
+// The tables of a scene of numNodes nodes carved out of `base`.
+SceneTables scene_tables(void* base, uint32_t numNodes);
+// Builds the tables of a scene on `st` (no host synchronisation).
+int launch_prep_tables(const BVHNode* nodes, uint32_t numNodes, const InstanceConstants* inst, uint32_t numInstances,
+                       const uint32_t* ib, uint32_t numIndices, const Vertex* vb, uint32_t numVertices,
+                       const SceneTables& t, uint32_t* status, int numSMs, cudaStream_t st);
+// The device view of a descriptor's scene with its derived tables.
+DevScene scene_from_desc(const PathTracerDesc* d, const SceneTables& t, const float* srgbLut, uint32_t* status);
 
 }  // namespace sb

@@ -15,6 +15,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cub/device/device_scan.cuh>
+
 #include "common.h"
 #include "nrc.h"
 #include "refine.cuh"
@@ -69,10 +71,8 @@ const char* kKernelNames[KC_COUNT] = {"generate",  "extend",    "shade",     "sh
                                       "prep",      "nrc_paths", "nrc_train", "nrc_infer", "sort", "tail"};
 
 // ---------------------------------------------------------------------------
-// Scene preparation: the record table of traverse.cuh, per node slot.
-// Leaf: the triangle exactly as getTriangle computes it (raytracing.h:134-153).
-// Inner: both children of the implicit tree (L = n+1, R = escape(n+1)) with
-// the boxes of inner children copied from their nodes.
+// Scene preparation: the record table of traverse.cuh, per leaf node slot:
+// the triangle exactly as getTriangle computes it (raytracing.h:134-153).
 __global__ void k_prep_rec(const float4* __restrict__ nodes, uint32_t numNodes, const InstanceConstants* __restrict__ inst,
                            uint32_t numInstances, const uint32_t* __restrict__ ib, uint32_t numIndices,
                            const Vertex* __restrict__ vb, uint32_t numVertices, float4* __restrict__ rec, uint32_t* status)
@@ -85,39 +85,7 @@ __global__ void k_prep_rec(const float4* __restrict__ nodes, uint32_t numNodes, 
         float4* out = &rec[4 * (size_t)i];
         const uint32_t esc = __float_as_uint(hi.w);
         if (esc != SB_INVALID && esc >= numNodes) atomicOr(status, STRELKA_DEV_NODE_OOB);
-        if (instId == SB_INVALID) {
-            uint32_t ref[2] = {SB_INVALID, SB_INVALID};
-            float4 box[4] = {make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0),
-                             make_float4(0, 0, 0, 0)};
-            const uint32_t L = i + 1;
-            uint32_t R = SB_INVALID;
-            if (L < numNodes) R = __float_as_uint(nodes[2 * (size_t)L + 1].w);
-            else atomicOr(status, STRELKA_DEV_NODE_OOB);
-            if (R != SB_INVALID && R >= numNodes) {
-                atomicOr(status, STRELKA_DEV_NODE_OOB);
-                R = SB_INVALID;
-            }
-            const uint32_t child[2] = {L < numNodes ? L : SB_INVALID, R};
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const uint32_t c = child[k];
-                if (c == SB_INVALID) continue;
-                const float4 clo = nodes[2 * (size_t)c];
-                const float4 chi = nodes[2 * (size_t)c + 1];
-                if (__float_as_uint(clo.w) != SB_INVALID) {
-                    ref[k] = c | SB_LEAF_BIT;
-                } else {
-                    ref[k] = c;
-                    box[2 * k] = make_float4(clo.x, clo.y, clo.z, 0.0f);
-                    box[2 * k + 1] = make_float4(chi.x, chi.y, chi.z, 0.0f);
-                }
-            }
-            out[0] = make_float4(box[0].x, box[0].y, box[0].z, __uint_as_float(ref[0]));
-            out[1] = make_float4(box[1].x, box[1].y, box[1].z, __uint_as_float(ref[1]));
-            out[2] = box[2];
-            out[3] = box[3];
-            continue;
-        }
+        if (instId == SB_INVALID) continue;  // inner nodes live in the 4-wide BVH
         const float4 bad = make_float4(qnan, qnan, qnan, 0.0f);
         if (instId >= numInstances) {
             atomicOr(status, STRELKA_DEV_INSTANCE_OOB);
@@ -151,6 +119,122 @@ __global__ void k_prep_rec(const float4* __restrict__ nodes, uint32_t numNodes, 
 
 // ---------------------------------------------------------------------------
 // Megakernel: computeMain, one thread per (pixel, sample).
+// ---------------------------------------------------------------------------
+// The 4-wide BVH of traverse.cuh, derived from the reference's binary tree
+// (implicit children: L = n+1, R = escape(n+1), bvh.cpp:182-220).  Its nodes
+// are the binary inner nodes at even depth; each holds the children of its
+// two binary children, in order:
+//   a leaf child       -> an ungated leaf entry (tested whenever the node is;
+//                         at the root, gated by the root's box, which the
+//                         reference tests first);
+//   an inner child c   -> c's two children: an inner one with its own box, a
+//                         leaf one gated by c's box.
+// A node's box test implies its parent's (the slab arithmetic rounds
+// monotonically and a parent box contains its children's), so skipping the
+// odd-depth boxes leaves the set of triangles a query tests unchanged.
+
+// parent of every node (the root keeps SB_INVALID)
+__global__ void k_wide_parent(const float4* __restrict__ nodes, uint32_t numNodes, uint32_t* __restrict__ parent)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x) {
+        if (__float_as_uint(nodes[2 * (size_t)i].w) != SB_INVALID) continue;  // leaf
+        const uint32_t L = i + 1;
+        if (L >= numNodes) continue;
+        parent[L] = i;
+        const uint32_t R = __float_as_uint(nodes[2 * (size_t)L + 1].w);
+        if (R != SB_INVALID && R < numNodes) parent[R] = i;
+    }
+}
+
+// 1 for the inner nodes at even depth
+__global__ void k_wide_flag(const float4* __restrict__ nodes, uint32_t numNodes, const uint32_t* __restrict__ parent,
+                            uint32_t* __restrict__ flag, uint32_t* status)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x) {
+        uint32_t f = 0;
+        if (__float_as_uint(nodes[2 * (size_t)i].w) == SB_INVALID) {
+            uint32_t p = i, depth = 0;
+            bool ok = true;
+            while (p != 0) {
+                p = parent[p];
+                if (p == SB_INVALID || ++depth > numNodes) {
+                    ok = false;
+                    break;
+                }
+            }
+            if (!ok) atomicOr(status, STRELKA_DEV_NODE_OOB);
+            f = ok && (depth & 1u) == 0 ? 1u : 0u;
+        }
+        flag[i] = f;
+    }
+}
+
+__global__ void k_wide_build(const float4* __restrict__ nodes, uint32_t numNodes, const uint32_t* __restrict__ flag,
+                             const uint32_t* __restrict__ map, float4* __restrict__ wide, uint32_t wideCap, uint32_t* status)
+{
+    for (uint32_t P = blockIdx.x * blockDim.x + threadIdx.x; P < numNodes; P += gridDim.x * blockDim.x) {
+        if (!flag[P]) continue;
+        const uint32_t w = map[P];
+        if (w >= wideCap) {
+            atomicOr(status, STRELKA_DEV_NODE_OOB);
+            continue;
+        }
+        float lo[3][4], hi[3][4];
+        uint32_t ref[4] = {SB_INVALID, SB_INVALID, SB_INVALID, SB_INVALID};
+        for (int a = 0; a < 3; ++a)
+            for (int k = 0; k < 4; ++k) lo[a][k] = hi[a][k] = 0.0f;
+        int e = 0;
+        auto right_of = [&](uint32_t left) -> uint32_t {
+            const uint32_t r = __float_as_uint(nodes[2 * (size_t)left + 1].w);
+            return r < numNodes ? r : SB_INVALID;
+        };
+        auto put = [&](uint32_t r, uint32_t boxNode) {
+            ref[e] = r;
+            if (boxNode != SB_INVALID) {
+                const float4 b0 = nodes[2 * (size_t)boxNode], b1 = nodes[2 * (size_t)boxNode + 1];
+                lo[0][e] = b0.x; lo[1][e] = b0.y; lo[2][e] = b0.z;
+                hi[0][e] = b1.x; hi[1][e] = b1.y; hi[2][e] = b1.z;
+            }
+            ++e;
+        };
+        const uint32_t L = P + 1 < numNodes ? P + 1 : SB_INVALID;
+        const uint32_t child[2] = {L, L != SB_INVALID ? right_of(L) : SB_INVALID};
+        bool bad = child[0] == SB_INVALID || child[1] == SB_INVALID;
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t c = child[k];
+            if (c == SB_INVALID) continue;
+            if (__float_as_uint(nodes[2 * (size_t)c].w) != SB_INVALID) {
+                // below the root a node is entered only after its box passed;
+                // the root's own box is tested here, before its leaf children
+                if (P == 0) put(c | SB_LEAF_BIT, P);
+                else put(c | SB_LEAF_BIT | SB_NOBOX_BIT, SB_INVALID);
+                continue;
+            }
+            const uint32_t g0 = c + 1 < numNodes ? c + 1 : SB_INVALID;
+            const uint32_t grand[2] = {g0, g0 != SB_INVALID ? right_of(g0) : SB_INVALID};
+            bad = bad || grand[0] == SB_INVALID || grand[1] == SB_INVALID;
+            for (int j = 0; j < 2; ++j) {
+                const uint32_t g = grand[j];
+                if (g == SB_INVALID) continue;
+                if (__float_as_uint(nodes[2 * (size_t)g].w) != SB_INVALID) put(g | SB_LEAF_BIT, c);
+                else if (flag[g] && map[g] < wideCap) put(map[g], g);
+                else bad = true;
+            }
+        }
+        if (bad) atomicOr(status, STRELKA_DEV_NODE_OOB);
+        float4* out = &wide[8 * (size_t)w];
+        out[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+        out[1] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+        out[2] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+        out[3] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+        out[4] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+        out[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+        out[6] = make_float4(__uint_as_float(ref[0]), __uint_as_float(ref[1]), __uint_as_float(ref[2]),
+                             __uint_as_float(ref[3]));
+        out[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
 __global__ void __launch_bounds__(kExtendBlock) k_megakernel(DevScene s, PathTracerParam ubo, float* __restrict__ sampleBuffer,
                                                              uint64_t first, uint64_t count)
 {
@@ -746,8 +830,9 @@ struct StrelkaPathTracer {
     const void* keyIb = nullptr;
     const void* keyInst = nullptr;
     uint32_t keyNumNodes = 0;
-    float4* rec = nullptr;  // 4 float4 per node (traverse.cuh record table)
-    size_t recCap = 0;      // nodes
+    void* tablesMem = nullptr;  // derived scene tables (internal.h SceneTables)
+    size_t tablesCap = 0;       // nodes they were sized for
+    SceneTables tables;
     float* srgbLut = nullptr;
     uint32_t* status = nullptr;
     // wavefront
@@ -874,19 +959,20 @@ int ensure_scene(StrelkaPathTracer* pt, const BVHNode* nodes, uint32_t numNodes,
                  uint64_t version, cudaStream_t st)
 {
     if (pt->sceneVersion == version && pt->keyNodes == nodes && pt->keyVb == vb && pt->keyIb == ib && pt->keyInst == inst &&
-        pt->keyNumNodes == numNodes && pt->rec)
+        pt->keyNumNodes == numNodes && pt->tablesMem)
         return STRELKA_OK;
-    if (numNodes > pt->recCap || !pt->rec) {
-        if (pt->rec) cudaFree(pt->rec);
-        pt->rec = nullptr;
-        size_t cap = std::max<size_t>(numNodes, 1);
-        SB_CUDA_TRY(cudaMalloc(&pt->rec, cap * 4 * sizeof(float4)));
-        pt->recCap = cap;
+    if (numNodes > pt->tablesCap || !pt->tablesMem) {
+        if (pt->tablesMem) cudaFree(pt->tablesMem);
+        pt->tablesMem = nullptr;
+        const uint32_t cap = std::max<uint32_t>(numNodes, 1);
+        SB_CUDA_TRY(cudaMalloc(&pt->tablesMem, scene_tables_bytes(cap)));
+        pt->tablesCap = cap;
     }
+    pt->tables = scene_tables(pt->tablesMem, numNodes);
     if (numNodes) {
-        Timer t(pt, KC_PREP, st);
-        int rc = launch_prep_records(nodes, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, pt->rec,
-                                     pt->status, pt->numSMs, st);
+        Timer t(pt, KC_PREP, st, 6);
+        int rc = launch_prep_tables(nodes, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, pt->tables,
+                                    pt->status, pt->numSMs, st);
         if (rc) return rc;
     }
     pt->sceneVersion = version;
@@ -900,7 +986,7 @@ int ensure_scene(StrelkaPathTracer* pt, const BVHNode* nodes, uint32_t numNodes,
 
 DevScene make_scene(StrelkaPathTracer* pt, const PathTracerDesc* d)
 {
-    return scene_from_desc(d, pt->rec, pt->srgbLut, pt->status);
+    return scene_from_desc(d, pt->tables, pt->srgbLut, pt->status);
 }
 
 int occupancy_grid(const void* fn, int block, int numSMs)
@@ -924,24 +1010,69 @@ void srgb_lut_host(float* lut)
 
 int validate_scene_desc(const PathTracerDesc* d) { return check_scene_desc(d); }
 
-int launch_prep_records(const BVHNode* nodes, uint32_t numNodes, const InstanceConstants* inst, uint32_t numInstances,
-                        const uint32_t* ib, uint32_t numIndices, const Vertex* vb, uint32_t numVertices, float4* rec,
-                        uint32_t* status, int numSMs, cudaStream_t st)
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+static size_t scan_bytes(uint32_t n)
+{
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)std::max<uint32_t>(n, 1));
+    return bytes;
+}
+
+size_t scene_tables_bytes(uint32_t numNodes)
+{
+    const size_t n = std::max<uint32_t>(numNodes, 1);
+    const size_t wideCap = n / 2 + 1;
+    return align256(n * 4 * sizeof(float4)) + align256(wideCap * 8 * sizeof(float4)) + 3 * align256(n * 4) +
+           align256(scan_bytes(numNodes));
+}
+
+SceneTables scene_tables(void* base, uint32_t numNodes)
+{
+    const size_t n = std::max<uint32_t>(numNodes, 1);
+    SceneTables t;
+    t.wideCap = (uint32_t)(n / 2 + 1);
+    char* p = static_cast<char*>(base);
+    t.rec = reinterpret_cast<float4*>(p);
+    p += align256(n * 4 * sizeof(float4));
+    t.wide = reinterpret_cast<float4*>(p);
+    p += align256((size_t)t.wideCap * 8 * sizeof(float4));
+    t.parent = reinterpret_cast<uint32_t*>(p);
+    p += align256(n * 4);
+    t.flag = reinterpret_cast<uint32_t*>(p);
+    p += align256(n * 4);
+    t.map = reinterpret_cast<uint32_t*>(p);
+    p += align256(n * 4);
+    t.scan = p;
+    t.scanBytes = scan_bytes(numNodes);
+    return t;
+}
+
+int launch_prep_tables(const BVHNode* nodes, uint32_t numNodes, const InstanceConstants* inst, uint32_t numInstances,
+                       const uint32_t* ib, uint32_t numIndices, const Vertex* vb, uint32_t numVertices,
+                       const SceneTables& t, uint32_t* status, int numSMs, cudaStream_t st)
 {
     if (!numNodes) return STRELKA_OK;
-    int grid = std::min<int>((numNodes + 255) / 256, numSMs * 16);
-    k_prep_rec<<<grid, 256, 0, st>>>(reinterpret_cast<const float4*>(nodes), numNodes, inst, numInstances, ib, numIndices,
-                                     vb, numVertices, rec, status);
+    const float4* nd = reinterpret_cast<const float4*>(nodes);
+    const int grid = std::min<int>((numNodes + 255) / 256, numSMs * 16);
+    k_prep_rec<<<grid, 256, 0, st>>>(nd, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, t.rec, status);
+    SB_CUDA_TRY(cudaMemsetAsync(t.parent, 0xFF, (size_t)numNodes * 4, st));
+    k_wide_parent<<<grid, 256, 0, st>>>(nd, numNodes, t.parent);
+    k_wide_flag<<<grid, 256, 0, st>>>(nd, numNodes, t.parent, t.flag, status);
+    size_t bytes = t.scanBytes;
+    SB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(t.scan, bytes, t.flag, t.map, (int)numNodes, st));
+    k_wide_build<<<grid, 256, 0, st>>>(nd, numNodes, t.flag, t.map, t.wide, t.wideCap, status);
     SB_CUDA_TRY(cudaGetLastError());
     return STRELKA_OK;
 }
 
-DevScene scene_from_desc(const PathTracerDesc* d, const float4* rec, const float* srgbLut, uint32_t* status)
+DevScene scene_from_desc(const PathTracerDesc* d, const SceneTables& t, const float* srgbLut, uint32_t* status)
 {
     DevScene s{};
     s.nodes = reinterpret_cast<const float4*>(d->bvhNodes);
     s.tris = nullptr;
-    s.rec = rec;
+    s.rec = t.rec;
+    s.wide = t.wide;
+    s.numWide = t.wideCap;
     s.numNodes = d->numNodes;
     s.numVertices = d->numVertices;
     s.vb = d->vb;
@@ -1022,7 +1153,7 @@ extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
 {
     if (!pt) return STRELKA_OK;
     free_wave(pt->main);
-    if (pt->rec) cudaFree(pt->rec);
+    if (pt->tablesMem) cudaFree(pt->tablesMem);
     if (pt->srgbLut) cudaFree(pt->srgbLut);
     if (pt->status) cudaFree(pt->status);
     if (pt->visitCounters) cudaFree(pt->visitCounters);

@@ -23,7 +23,9 @@ namespace sb {
 struct DevScene {
     const float4* nodes;  // 2 float4 per BVHNode
     const float4* tris;   // 3 float4 per node (leaf slots only)
-    const float4* rec;    // 4 float4 per node: node-pair records / leaf triangles
+    const float4* rec;    // 4 float4 per node: leaf triangles (at leaf slots)
+    const float4* wide;   // 8 float4 per 4-wide node (see below)
+    uint32_t numWide;     // capacity of `wide` in nodes
     uint32_t numNodes;
     uint32_t numVertices;
     const Vertex* vb;
@@ -219,9 +221,10 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, v3 o, float tmax, v
 namespace sb {
 
 #ifndef SB_STACK
-#define SB_STACK 32
+#define SB_STACK 64
 #endif
-#define SB_LEAF_BIT 0x80000000u
+#define SB_LEAF_BIT 0x80000000u   // a ref to a leaf triangle (its node slot in the record table)
+#define SB_NOBOX_BIT 0x40000000u  // a leaf tested without a box (a leaf child of the node itself)
 
 struct RayQ {
     v3 o, d, inv;
@@ -254,6 +257,7 @@ __device__ __forceinline__ bool rec_triangle(const DevScene& s, const RayQ& r, u
 struct Fallback {
     HitRec hit;
     float minHit;
+    uint32_t leaf;  // node index of the best hit's leaf
     uint32_t nInner, nLeaf;
     bool found;
 };
@@ -262,7 +266,8 @@ struct Fallback {
 // leaf triangles from the record table; runs from the root with the best hit
 // so far (used when the stack overflows).
 template <bool COUNT>
-__device__ __noinline__ Fallback closest_stackless_rec(const DevScene s, const RayQ r, float minHit, HitRec hit, bool found)
+__device__ __noinline__ Fallback closest_stackless_rec(const DevScene s, const RayQ r, float minHit, uint32_t best, HitRec hit,
+                                                       bool found)
 {
     Fallback f;
     f.nInner = 0;
@@ -279,8 +284,10 @@ __device__ __noinline__ Fallback closest_stackless_rec(const DevScene s, const R
             if (COUNT) ++f.nLeaf;
             float t, bu, bv;
             uint32_t iid, pid;
-            if (rec_triangle(s, r, node, t, bu, bv, iid, pid) && (t < r.tmax) && (t < minHit)) {
+            if (rec_triangle(s, r, node, t, bu, bv, iid, pid) && (t < r.tmax) &&
+                (t < minHit || (t == minHit && node < best))) {
                 minHit = t;
+                best = node;
                 hit.t = t;
                 hit.u = bu;
                 hit.v = bv;
@@ -301,6 +308,7 @@ __device__ __noinline__ Fallback closest_stackless_rec(const DevScene s, const R
     }
     f.hit = hit;
     f.minHit = minHit;
+    f.leaf = best;
     f.found = found;
     return f;
 }
@@ -355,7 +363,8 @@ __device__ __noinline__ Fallback any_stackless_rec(const DevScene s, const RayQ 
 struct Trav {
     RayQ r;
     float minHit;
-    uint32_t cur;  // record to process next; SB_INVALID = pop
+    uint32_t leaf;  // closest hit: node index of the best hit's leaf
+    uint32_t cur;  // 4-wide node to process next, a leaf ref (SB_LEAF_BIT), or SB_INVALID = pop
     int sp;
     uint32_t steps;
     bool found;
@@ -366,6 +375,7 @@ __device__ __forceinline__ void trav_init(const DevScene& s, Trav& T, v3 o, floa
 {
     T.r = make_ray(o, tmax, d);
     T.minHit = 1e9f;
+    T.leaf = SB_INVALID;
     T.sp = 0;
     T.steps = 0;
     T.found = false;
@@ -374,86 +384,153 @@ __device__ __forceinline__ void trav_init(const DevScene& s, Trav& T, v3 o, floa
     T.hit.t = any ? 0.0f : 1e9f;
     T.hit.instId = SB_INVALID;
     T.hit.primId = SB_INVALID;
-    T.cur = s.numNodes ? 0u : SB_INVALID;
+    if (!s.numNodes) T.cur = SB_INVALID;
+    else if (__float_as_uint(__ldg(&s.nodes[0]).w) != SB_INVALID) T.cur = SB_LEAF_BIT | SB_NOBOX_BIT;  // the root is a leaf
+    else T.cur = 0u;  // the 4-wide root
 }
 
-// One closest-hit step: processes the record T.cur (or the root leaf), then
-// pops until a record to process is found.  Returns true when finished.
+// The four entries of 4-wide node w.
+struct WideNode {
+    float4 lx, ly, lz, hx, hy, hz;
+    uint32_t ref[4];
+};
+__device__ __forceinline__ WideNode load_wide(const DevScene& s, uint32_t w)
+{
+    const float4* p = &s.wide[8 * (size_t)w];
+    WideNode n;
+    n.lx = __ldg(p);
+    n.ly = __ldg(p + 1);
+    n.lz = __ldg(p + 2);
+    n.hx = __ldg(p + 3);
+    n.hy = __ldg(p + 4);
+    n.hz = __ldg(p + 5);
+    const float4 rf = __ldg(p + 6);
+    n.ref[0] = __float_as_uint(rf.x);
+    n.ref[1] = __float_as_uint(rf.y);
+    n.ref[2] = __float_as_uint(rf.z);
+    n.ref[3] = __float_as_uint(rf.w);
+    return n;
+}
+__device__ __forceinline__ float4 comp4(float4 v, int k)
+{
+    return make_float4(k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w, 0.0f, 0.0f, 0.0f);
+}
+// box of entry k, tested with the reference's slab arithmetic
+__device__ __forceinline__ bool wide_box(const RayQ& r, const WideNode& n, int k, float& t)
+{
+    const float4 lo = make_float4(comp4(n.lx, k).x, comp4(n.ly, k).x, comp4(n.lz, k).x, 0.0f);
+    const float4 hi = make_float4(comp4(n.hx, k).x, comp4(n.hy, k).x, comp4(n.hz, k).x, 0.0f);
+    return ray_box(r.o, r.inv, lo, hi, t);
+}
+__device__ __forceinline__ void cswap(float& ta, uint32_t& ra, float& tb, uint32_t& rb)
+{
+    if (tb < ta) {
+        const float t = ta;
+        ta = tb;
+        tb = t;
+        const uint32_t x = ra;
+        ra = rb;
+        rb = x;
+    }
+}
+
+// Closest-hit test of one leaf triangle.  On a tie in t the leaf with the
+// smaller node index wins: the node array is in depth-first order, so that
+// is the leaf the reference visits first and keeps (its test is the strict
+// t < minHit), whatever order this traversal reaches them in.
+__device__ __forceinline__ void closest_leaf(const DevScene& s, Trav& T, uint32_t leaf)
+{
+    float t, bu, bv;
+    uint32_t iid, pid;
+    if (rec_triangle(s, T.r, leaf, t, bu, bv, iid, pid) && (t < T.r.tmax) &&
+        (t < T.minHit || (t == T.minHit && leaf < T.leaf))) {
+        T.minHit = t;
+        T.leaf = leaf;
+        T.hit.t = t;
+        T.hit.u = bu;
+        T.hit.v = bv;
+        T.hit.instId = iid;
+        T.hit.primId = pid;
+        T.found = true;
+    }
+}
+
+// One closest-hit step: processes the 4-wide node T.cur (or the root leaf),
+// then pops until a node to process is found.  Returns true when finished.
 template <bool COUNT>
 __device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, uint32_t* stackN, float* stackT, uint32_t& nInner,
                                              uint32_t& nLeaf)
 {
     const uint32_t cur = T.cur;
     if (cur != SB_INVALID) {
-        if (cur >= s.numNodes || ++T.steps > s.numNodes + 1u) {
-            raise_status(s, cur >= s.numNodes ? STRELKA_DEV_NODE_OOB : STRELKA_DEV_TRAVERSAL_CAP);
+        if (++T.steps > s.numNodes + 1u) {
+            raise_status(s, STRELKA_DEV_TRAVERSAL_CAP);
             return true;
         }
-        const float4* rp = &s.rec[4 * (size_t)cur];
-        const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
-        const uint32_t L = __float_as_uint(r0.w);
-        if (cur == 0 && __float_as_uint(__ldg(&s.nodes[0]).w) != SB_INVALID) {
-            // the root itself is a leaf
+        if (cur & SB_LEAF_BIT) {
             if (COUNT) ++nLeaf;
-            float t, bu, bv;
-            uint32_t iid, pid;
-            if (rec_triangle(s, T.r, 0, t, bu, bv, iid, pid) && (t < T.r.tmax) && (t < T.minHit)) {
-                T.minHit = t;
-                T.hit.t = t;
-                T.hit.u = bu;
-                T.hit.v = bv;
-                T.hit.instId = iid;
-                T.hit.primId = pid;
-                T.found = true;
-            }
+            closest_leaf(s, T, cur & ~(SB_LEAF_BIT | SB_NOBOX_BIT));
             T.cur = SB_INVALID;
         } else {
+            if (cur >= s.numWide) {
+                raise_status(s, STRELKA_DEV_NODE_OOB);
+                return true;
+            }
             if (COUNT) ++nInner;
-            const float4 r2 = __ldg(rp + 2), r3 = __ldg(rp + 3);
-            const uint32_t R = __float_as_uint(r1.w);
-            bool goL = false, goR = false;
-            float tL = 0.0f, tR = 0.0f;
-            // children in the reference's order: left, then right
+            // boxes first (so that the node's bounds are dead before the
+            // triangle tests), then the leaves hit in the reference's order;
+            // inner children hit within tmax become candidates
+            uint32_t ref[4];
+            float bt[4];
+            bool pass[4];
+            {
+                const WideNode n = load_wide(s, cur);
+                const float lim0 = T.minHit * SB_PRUNE_SCALE;
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const uint32_t c = k == 0 ? L : R;
-                if (c == SB_INVALID) continue;
-                if (c & SB_LEAF_BIT) {
-                    if (COUNT) ++nLeaf;
-                    float t, bu, bv;
-                    uint32_t iid, pid;
-                    if (rec_triangle(s, T.r, c & ~SB_LEAF_BIT, t, bu, bv, iid, pid) && (t < T.r.tmax) && (t < T.minHit)) {
-                        T.minHit = t;
-                        T.hit.t = t;
-                        T.hit.u = bu;
-                        T.hit.v = bv;
-                        T.hit.instId = iid;
-                        T.hit.primId = pid;
-                        T.found = true;
-                    }
-                } else {
-                    float bt;
-                    const bool h = k == 0 ? ray_box(T.r.o, T.r.inv, r0, r1, bt) : ray_box(T.r.o, T.r.inv, r2, r3, bt);
-                    if (k == 0) { goL = h; tL = bt; } else { goR = h; tR = bt; }
+                for (int k = 0; k < 4; ++k) {
+                    ref[k] = n.ref[k];
+                    bt[k] = 0.0f;
+                    pass[k] = ref[k] != SB_INVALID &&
+                              ((ref[k] & SB_NOBOX_BIT) || (wide_box(T.r, n, k, bt[k]) && !(bt[k] > T.r.tmax) && !(bt[k] > lim0)));
                 }
             }
+            float ct[4];
+            uint32_t cr[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                ct[k] = __int_as_float(0x7f800000);  // +inf: no candidate
+                cr[k] = SB_INVALID;
+                if (!pass[k]) continue;
+                if (ref[k] & SB_LEAF_BIT) {
+                    if (COUNT) ++nLeaf;
+                    closest_leaf(s, T, ref[k] & ~(SB_LEAF_BIT | SB_NOBOX_BIT));
+                } else {
+                    ct[k] = bt[k];
+                    cr[k] = ref[k];
+                }
+            }
+            // nearest first: sort the (up to four) candidates by entry distance
+            cswap(ct[0], cr[0], ct[1], cr[1]);
+            cswap(ct[2], cr[2], ct[3], cr[3]);
+            cswap(ct[0], cr[0], ct[2], cr[2]);
+            cswap(ct[1], cr[1], ct[3], cr[3]);
+            cswap(ct[1], cr[1], ct[2], cr[2]);
             const float lim = T.minHit * SB_PRUNE_SCALE;
-            goL = goL && !(tL > T.r.tmax) && !(tL > lim);
-            goR = goR && !(tR > T.r.tmax) && !(tR > lim);
-            if (goL && goR) {
-                const bool leftNear = tL <= tR;
-                const uint32_t nearC = leftNear ? L : R, farC = leftNear ? R : L;
-                const float farT = leftNear ? tR : tL;
+            T.cur = (cr[0] != SB_INVALID && !(ct[0] > lim)) ? cr[0] : SB_INVALID;
+            // the others onto the stack, farthest first
+#pragma unroll
+            for (int k = 3; k >= 1; --k) {
+                if (cr[k] == SB_INVALID || ct[k] > lim) continue;
                 if (T.sp < SB_STACK) {
-                    stackN[T.sp] = farC;
-                    stackT[T.sp] = farT;
+                    stackN[T.sp] = cr[k];
+                    stackT[T.sp] = ct[k];
                     ++T.sp;
-                    T.cur = nearC;
                 } else {
                     // stack full: finish with the stackless loop from the root
-                    const Fallback f = closest_stackless_rec<COUNT>(s, T.r, T.minHit, T.hit, T.found);
+                    const Fallback f = closest_stackless_rec<COUNT>(s, T.r, T.minHit, T.leaf, T.hit, T.found);
                     T.hit = f.hit;
                     T.minHit = f.minHit;
+                    T.leaf = f.leaf;
                     T.found = f.found;
                     if (COUNT) {
                         nInner += f.nInner;
@@ -463,12 +540,6 @@ __device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, uint32_
                     T.sp = 0;
                     return true;
                 }
-            } else if (goL) {
-                T.cur = L;
-            } else if (goR) {
-                T.cur = R;
-            } else {
-                T.cur = SB_INVALID;
             }
         }
     }
@@ -486,74 +557,61 @@ __device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, uint32_
     return false;
 }
 
-// One any-hit step (depth-first order).  Returns true when finished; T.found
-// tells whether a hit with t < tmax was found.
+// One any-hit step (the reference's depth-first order).  Returns true when
+// finished; T.found tells whether a hit with t < tmax was found.
 template <bool COUNT>
 __device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, uint32_t* stackN, uint32_t& nInner, uint32_t& nLeaf)
 {
-    uint32_t cur = T.cur;
-    if (cur != SB_INVALID) {
-        if (cur >= s.numNodes || ++T.steps > s.numNodes + 1u) {
-            raise_status(s, cur >= s.numNodes ? STRELKA_DEV_NODE_OOB : STRELKA_DEV_TRAVERSAL_CAP);
+    const uint32_t cur = T.cur;
+    if (cur != SB_INVALID && !(cur & SB_LEAF_BIT)) {
+        if (++T.steps > s.numNodes + 1u || cur >= s.numWide) {
+            raise_status(s, cur >= s.numWide ? STRELKA_DEV_NODE_OOB : STRELKA_DEV_TRAVERSAL_CAP);
             return true;
         }
-        if (cur == 0 && __float_as_uint(__ldg(&s.nodes[0]).w) != SB_INVALID) {
-            if (COUNT) ++nLeaf;
-            float t, bu, bv;
-            uint32_t iid, pid;
-            bool isect = rec_triangle(s, T.r, 0, t, bu, bv, iid, pid);
-            T.hit.t = t;
-            if (isect && (t < T.r.tmax)) {
-                T.hit.instId = iid;
-                T.hit.primId = pid;
-                T.found = true;
-                return true;
-            }
-            T.cur = SB_INVALID;
-        } else {
-            if (COUNT) ++nInner;
-            const float4* rp = &s.rec[4 * (size_t)cur];
-            const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1), r2 = __ldg(rp + 2), r3 = __ldg(rp + 3);
-            const uint32_t L = __float_as_uint(r0.w), R = __float_as_uint(r1.w);
-            // a leaf child is always visited; an inner child when its box is
-            // hit within tmax (raytracing.h:249-286 reaches the same nodes)
-            bool goL = false, rPending = false;
-            if (L != SB_INVALID) {
-                float bt;
-                goL = (L & SB_LEAF_BIT) || (ray_box(T.r.o, T.r.inv, r0, r1, bt) && !(bt > T.r.tmax));
-            }
-            if (R != SB_INVALID) {
-                float bt;
-                rPending = (R & SB_LEAF_BIT) || (ray_box(T.r.o, T.r.inv, r2, r3, bt) && !(bt > T.r.tmax));
-            }
-            if (goL) {
-                if (rPending) {
-                    if (T.sp < SB_STACK) {
-                        stackN[T.sp++] = R;
-                    } else {
-                        // stack full: the stackless loop from L visits the
-                        // rest of the tree in the same order
-                        const Fallback f = any_stackless_rec<COUNT>(s, T.r, L & ~SB_LEAF_BIT, T.hit);
-                        T.hit = f.hit;
-                        T.found = f.found;
-                        if (COUNT) {
-                            nInner += f.nInner;
-                            nLeaf += f.nLeaf;
-                        }
-                        T.cur = SB_INVALID;
-                        T.sp = 0;
-                        return true;
-                    }
-                }
-                T.cur = L;
-            } else if (rPending) {
-                T.cur = R;
-            } else {
-                T.cur = SB_INVALID;
+        if (COUNT) ++nInner;
+        // the entries visited, in order: an ungated leaf always, a gated leaf
+        // or an inner child when its box is hit within tmax (the reference
+        // reaches the same leaves and nodes, raytracing.h:249-286); the first
+        // is next, the others wait on the stack in order
+        uint32_t ref[4];
+        bool pass[4];
+        {
+            const WideNode n = load_wide(s, cur);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                ref[k] = n.ref[k];
+                float bt = 0.0f;
+                pass[k] = ref[k] != SB_INVALID &&
+                          ((ref[k] & SB_NOBOX_BIT) || (wide_box(T.r, n, k, bt) && !(bt > T.r.tmax)));
             }
         }
+        uint32_t first = SB_INVALID;
+#pragma unroll
+        for (int k = 3; k >= 0; --k) {
+            if (!pass[k]) continue;
+            if (first != SB_INVALID) {
+                if (T.sp < SB_STACK) {
+                    stackN[T.sp++] = first;
+                } else {
+                    // stack full: the reference's stackless loop from the root
+                    // gives the same first hit
+                    const Fallback f = any_stackless_rec<COUNT>(s, T.r, 0u, T.hit);
+                    T.hit = f.hit;
+                    T.found = f.found;
+                    if (COUNT) {
+                        nInner += f.nInner;
+                        nLeaf += f.nLeaf;
+                    }
+                    T.cur = SB_INVALID;
+                    T.sp = 0;
+                    return true;
+                }
+            }
+            first = ref[k];
+        }
+        T.cur = first;
     }
-    // a leaf reached as the next node (a pending right child or a popped one)
+    // leaves reached as the next entry (the first of a node, or popped)
     for (;;) {
         if (T.cur == SB_INVALID) {
             if (T.sp == 0) return true;
@@ -563,7 +621,7 @@ __device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, uint32_t* s
         if (COUNT) ++nLeaf;
         float t, bu, bv;
         uint32_t iid, pid;
-        bool isect = rec_triangle(s, T.r, T.cur & ~SB_LEAF_BIT, t, bu, bv, iid, pid);
+        const bool isect = rec_triangle(s, T.r, T.cur & ~(SB_LEAF_BIT | SB_NOBOX_BIT), t, bu, bv, iid, pid);
         T.hit.t = t;
         if (isect && (t < T.r.tmax)) {
             T.hit.instId = iid;

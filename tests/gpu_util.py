@@ -42,3 +42,33 @@ def compare_closest(gpu_hits, orc_hits):
         assert abs(tg - to) <= 1e-6 * abs(to), f"ray {k}: t {tg} vs {to}"
         ties += 1
     return ties
+
+
+def vertex_edge_rays(seed_origins=None):
+    """Rays from points inside the unit Cornell box aimed at the vertices and
+    edge midpoints of its 16x16 wall grid, where two or more triangles share
+    the hit point and closest-hit ties in t are common."""
+    g = np.concatenate([np.arange(17) / 16.0, (np.arange(16) + 0.5) / 16.0]).astype(F32)
+    a, b = np.meshgrid(g, g)
+    a, b = a.ravel(), b.ravel()
+    targets = []
+    for axis in range(3):
+        others = [k for k in range(3) if k != axis]
+        for val in (0.0, 1.0):
+            t = np.zeros((a.size, 3), F32)
+            t[:, axis] = val
+            t[:, others[0]] = a
+            t[:, others[1]] = b
+            targets.append(t)
+    targets = np.concatenate(targets)
+    origins = np.array(seed_origins or [[0.5, 0.5, 0.5], [0.25, 0.5, 0.5], [0.5, 0.3, 0.7], [0.31, 0.62, 0.44]], F32)
+    rays = []
+    for o in origins:
+        d = targets - o
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        r = np.zeros((targets.shape[0], 8), F32)
+        r[:, :3] = o
+        r[:, 3] = 1e9
+        r[:, 4:7] = d
+        rays.append(r)
+    return np.concatenate(rays)

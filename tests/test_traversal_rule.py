@@ -1,0 +1,59 @@
+"""The GPU's 4-wide traversal rule, replayed by the oracle (prune=2), returns
+the reference's closestHit / anyHit records (shaders/raytracing.h:198-286)
+bit for bit, ties in t included: skipping the odd-depth boxes of the binary
+tree leaves the set of tested triangles unchanged, and closest-hit ties go to
+the leaf first in depth-first order, as in the reference's strict t < minHit
+loop.  The GPU kernels match this replay exactly (tests/test_gpu_trace.py)."""
+import numpy as np
+import pytest
+
+import oracle
+from gpu_util import interior_rays, vertex_edge_rays
+from strelka_b200 import scenes
+
+
+@pytest.fixture(scope="module")
+def cornell():
+    s = scenes.cornell(16, 16, sphere_levels=4)
+    return oracle.SceneView(s)
+
+
+@pytest.mark.parametrize("any_hit", [False, True])
+def test_ties_at_vertices_and_edges(cornell, any_hit):
+    rays = vertex_edge_rays()
+    ref, found, _ = oracle.trace(cornell, rays, any_hit=any_hit)
+    wide, _, _ = oracle.trace(cornell, rays, any_hit=any_hit, prune=2)
+    assert found.mean() > 0.8
+    assert np.array_equal(wide, ref)
+
+
+@pytest.mark.parametrize("tmax", [1e9, 0.4])
+def test_random_interior_rays(cornell, tmax):
+    rays = interior_rays(20_000, 11, tmax=tmax)
+    for any_hit in (False, True):
+        ref, _, _ = oracle.trace(cornell, rays, any_hit=any_hit)
+        wide, _, _ = oracle.trace(cornell, rays, any_hit=any_hit, prune=2)
+        assert np.array_equal(wide, ref)
+
+
+def test_soup():
+    s = scenes.soup(20_000, 3)
+    v = oracle.SceneView(s)
+    for shadow in (False, True):
+        rays = scenes.rays_soup(20_000, 4, shadow=shadow)
+        for any_hit in (False, True):
+            ref, _, _ = oracle.trace(v, rays, any_hit=any_hit)
+            wide, _, _ = oracle.trace(v, rays, any_hit=any_hit, prune=2)
+            assert np.array_equal(wide, ref)
+
+
+@pytest.mark.parametrize("num_tris", [1, 2, 3, 5])
+def test_tiny_trees(num_tris):
+    # a leaf root, a root with two leaves, and odd shapes of the first levels
+    s = scenes.soup(num_tris, 7)
+    v = oracle.SceneView(s)
+    rays = scenes.rays_soup(4000, 8)
+    for any_hit in (False, True):
+        ref, _, _ = oracle.trace(v, rays, any_hit=any_hit)
+        wide, _, _ = oracle.trace(v, rays, any_hit=any_hit, prune=2)
+        assert np.array_equal(wide, ref)
