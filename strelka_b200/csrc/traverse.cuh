@@ -9,11 +9,10 @@
 // each leaf visit reads 32 + 48 bytes instead of an instance record, three
 // indices and three vertices.
 //
-// Closest hit visits nodes in the reference's depth-first order and
-// additionally skips an inner node whose entry distance exceeds the best hit
-// so far by a relative 2^-12 (the reference never prunes); the winner under
-// the strict t < minHit rule is unchanged.  Any hit is the reference
-// traversal verbatim (its result depends on the visit order).
+// trace_closest / trace_any below are the reference's stackless loops over
+// the node array (used by the allocation-free ray query); closest hit adds
+// the 2^-12 relative pruning of subtrees whose entry lies beyond the best
+// hit.  The kernels of the passes use the 4-wide traversal further down.
 #pragma once
 #include "device_math.cuh"
 
@@ -191,31 +190,39 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, v3 o, float tmax, v
 }  // namespace sb
 
 // ===========================================================================
-// Node-pair traversal.
+// 4-wide traversal.
 //
-// A derived table of 4 float4 per node slot is built once per scene version:
-//   inner node n (children L = n+1 and R = escape(n+1), the implicit tree of
-//   the reference's depth-first layout, bvh.cpp:182-220):
-//     [0] = L box min | L ref   [1] = L box max | R ref
-//     [2] = R box min | 0       [3] = R box max | 0
-//   leaf node n:  [0] = v0 | instId  [1] = e0 | primId  [2] = e1 | 0
-// where a child ref is its node index, with bit 31 set for a leaf child and
-// 0xFFFFFFFF for a missing one.  Processing one inner record tests both
-// children with one 64-byte fetch: an inner child's box exactly as the
-// reference tests it when it visits that node, a leaf child's triangle
-// exactly as the reference tests it when it reaches that leaf.  So the set of
-// triangles a query can test is the reference's; only the order differs.
+// Derived tables, built once per scene version on the GPU (pathtracer.cu):
+//   record table, 4 float4 per node slot: leaf node n holds its triangle
+//     [0] = v0 | instId  [1] = e0 | primId  [2] = e1 | 0;
+//   4-wide BVH, 8 float4 per node: the binary inner nodes at even depth of
+//     the reference's tree (children L = n+1 and R = escape(n+1), the
+//     implicit tree of the depth-first layout, bvh.cpp:182-220).  Node w:
+//     [0..2] = min x / y / z of its 4 entries, [3..5] = max x / y / z,
+//     [6] = the 4 entry refs.  The entries, in the reference's order, are for
+//     each binary child c: c itself when it is a leaf (ref | SB_LEAF_BIT |
+//     SB_NOBOX_BIT: tested without a box, as the reference does, except at
+//     the root, where the root's box gates it), otherwise c's two children:
+//     an inner one with its own box (ref = its 4-wide index), a leaf one
+//     gated by c's box (ref = its node slot | SB_LEAF_BIT).
+// A child's box test passing implies its parent's (the slab arithmetic
+// rounds monotonically and a parent box contains its children's), so testing
+// only the even-depth boxes leaves the set of triangles a query tests
+// exactly the reference's.  One step reads one 4-wide node (112 bytes) and
+// tests four boxes: half the dependent fetches of a binary traversal.
 //
-// Closest hit visits the nearer child first, keeps the farther on a
-// per-thread stack with its entry distance, and drops any subtree whose entry
-// exceeds the best hit by more than a relative 2^-12; the closest t is the
-// reference's, and on exact ties in t the winning primitive may differ.
-// Any hit keeps the reference's depth-first order exactly: the right child
-// (an inner node whose box was hit, or a leaf) is pushed until the left
-// subtree is done.  A full stack falls back to the stackless reference loop
-// (closest: restart from the root with the best hit so far; any: continue
-// from the child being entered, which visits the rest of the tree in the
-// same depth-first order).
+// Closest hit tests all entry boxes, then the leaves that passed, continues
+// with the nearest passing inner entry and keeps the others on a per-thread
+// stack with their entry distances (sorted, farthest first), dropping any
+// subtree whose entry exceeds the best hit by more than a relative 2^-12.  A
+// tie in t goes to the leaf with the smaller node index, the first in
+// depth-first order: the reference's winner under its strict t < minHit rule.
+// Any hit keeps the reference's depth-first order exactly: a node's passing
+// entries go onto the stack in reverse order, and leaves are tested when
+// reached.  A full stack falls back to the reference's stackless loop from
+// the root (closest: with the best hit so far).  tests/test_traversal_rule.py
+// checks the rule, replayed by the oracle, against the reference loop bit for
+// bit; tests/test_gpu_trace.py checks the kernels against both.
 // ===========================================================================
 
 namespace sb {
