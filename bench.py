@@ -42,11 +42,11 @@ METRIC = "Mpaths/s at 1080p"
 UNIT = "Mpaths/s"
 
 # DRAM bytes (read + write) per closest-hit query of the extend kernel on this
-# workload, from one ncu capture of a full frame's 8 extend launches
-# (dram__bytes_read.sum + dram__bytes_write.sum = 17.87 GB for 68.89M rays;
+# workload, from one ncu capture of a full frame's 5 extend launches
+# (dram__bytes_read.sum + dram__bytes_write.sum = 18.40 GB for 68.87M rays;
 # profiles/extend_large_1080p16_dram.md).  bench.py cannot run ncu itself, so
 # roofline.traffic is this figure times the rays of an average launch.
-EXTEND_DRAM_BYTES_PER_RAY = 259.4
+EXTEND_DRAM_BYTES_PER_RAY = 267.2
 
 # Bytes a traversal reads per 4-wide node it processes: the bounds of its four
 # entries (6 float4) and their refs (1 float4).

@@ -192,9 +192,9 @@ __global__ void __launch_bounds__(kSmallBlock) k_batch_generate(JobTable jt, Wav
     }
 }
 
-// Resident threads per SM asked of the traversal kernels: 9 x 128 for
-// closest hit and 8 x 128 for any hit, as in the single-job pass.
-constexpr int kExtendThreadsPerSM = 9 * 128;
+// Resident threads per SM asked of the traversal kernels: 8 x 128 for
+// closest hit and for any hit, as in the single-job pass.
+constexpr int kExtendThreadsPerSM = 8 * 128;
 constexpr int kShadowThreadsPerSM = 8 * 128;
 
 template <int BLOCK>

@@ -42,14 +42,14 @@ constexpr uint32_t kDefaultTailDepth = 5;  // first bounce finished by k_tail
 #ifndef SB_SHADOW_MINBLOCKS
 #define SB_SHADOW_MINBLOCKS 8
 #endif
-// The closest-hit kernel is latency-bound: 9 resident blocks (56 registers,
-// a few spilled) hide more of its dependent fetches than 8 without spills.
+// The closest-hit kernel is latency-bound: 8 resident blocks (64 registers,
+// 8 bytes spilled) beat 9 (56 registers, 110 bytes spilled) and 7.
 // Shadow queries of bounce k overlap the closest-hit queries of bounce k+1.
 #ifndef SB_OVERLAP_SHADOW
 #define SB_OVERLAP_SHADOW 1
 #endif
 #ifndef SB_EXTEND_MINBLOCKS
-#define SB_EXTEND_MINBLOCKS 9
+#define SB_EXTEND_MINBLOCKS 8
 #endif
 
 enum KernelClass {
