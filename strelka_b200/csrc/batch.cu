@@ -192,6 +192,14 @@ __global__ void __launch_bounds__(kSmallBlock) k_batch_generate(JobTable jt, Wav
     }
 }
 
+// Shadow-request count of a bounce: counters[2] on even bounces, [6] on odd
+// ones, so that shadow(k) can read its count while extend(k+1) resets the
+// one shade(k+1) fills.
+__host__ __device__ __forceinline__ int batch_shadow_count(int qin) { return qin ? 6 : 2; }
+
+// Bounces from this one on are finished by k_batch_tail.
+constexpr int kBatchTailDepth = 5;
+
 // Resident threads per SM asked of the traversal kernels: 8 x 128 for
 // closest hit and for any hit, as in the single-job pass.
 constexpr int kExtendThreadsPerSM = 8 * 128;
@@ -205,8 +213,8 @@ __global__ void __launch_bounds__(BLOCK, kExtendThreadsPerSM / BLOCK) k_batch_ex
     load_prefix(jt, sp);
     const uint32_t count = w.counters[qin];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        w.counters[qin ^ 1] = 0;  // refilled by this bounce's shade
-        w.counters[2] = 0;        // refilled by this bounce's shade
+        w.counters[qin ^ 1] = 0;                // refilled by this bounce's shade
+        w.counters[batch_shadow_count(qin)] = 0;  // refilled by this bounce's shade
     }
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
     uint32_t stackN[SB_STACK];
@@ -412,7 +420,7 @@ __global__ void __launch_bounds__(BLOCK) k_batch_shade(JobTable jt, Wave w, int 
         const uint32_t qpos = warp_push(&w.counters[qin ^ 1], cont);
         if (cont) qout[qpos] = slot;
         const bool hasShadow = sr.kind != 0;
-        const uint32_t spos = warp_push(&w.counters[2], hasShadow);
+        const uint32_t spos = warp_push(&w.counters[batch_shadow_count(qin)], hasShadow);
         if (hasShadow) {
             w.sh_o[spos] = f4(sr.o, sr.tmax);
             w.sh_d[spos] = f4(sr.d, __uint_as_float(slot));
@@ -423,12 +431,12 @@ __global__ void __launch_bounds__(BLOCK) k_batch_shade(JobTable jt, Wave w, int 
 }
 
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, kShadowThreadsPerSM / BLOCK) k_batch_shadow(JobTable jt, Wave w, uint32_t first, uint32_t chunk,
-                                                        uint32_t* fetch)
+__global__ void __launch_bounds__(BLOCK, kShadowThreadsPerSM / BLOCK) k_batch_shadow(JobTable jt, Wave w, int qin, uint32_t first,
+                                                        uint32_t chunk, uint32_t* fetch)
 {
     __shared__ uint32_t sp[kMaxJobs + 1];
     load_prefix(jt, sp);
-    const uint32_t count = w.counters[2];
+    const uint32_t count = w.counters[batch_shadow_count(qin)];
     uint32_t stackN[SB_STACK];
     uint32_t nI = 0, nL = 0;
     WarpPool pool{0, 0, 0};
@@ -460,6 +468,60 @@ __global__ void __launch_bounds__(BLOCK, kShadowThreadsPerSM / BLOCK) k_batch_sh
             apply_shadow(c, xyz(cd), xyz(cg));
             w.col[slot] = f4(c, 0.0f);
         }
+        have = false;
+    }
+}
+
+// Finishes every path queued for bounce `depth` (queue qin) with the
+// persistent loop (closest hit, shade, shadow inline), each with its job's
+// scene; one launch replaces the last bounces' launch sequences, where few
+// paths remain.  Same device code and order of additions as the wavefront.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_batch_tail(JobTable jt, Wave w, int qin, uint32_t first, uint32_t chunk,
+                                                      uint32_t* fetch)
+{
+    __shared__ uint32_t sp[kMaxJobs + 1];
+    load_prefix(jt, sp);
+    const uint32_t count = w.counters[qin];
+    const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
+    WarpPool pool{0, 0, 0};
+    PathState ps;
+    uint32_t slot = 0;
+    int job = 0;
+    bool have = false;
+    while (true) {
+        const uint32_t got = pool_take(pool, fetch, count, chunk, !have);
+        if (!have && got != SB_INVALID) {
+            slot = q[got];
+            job = find_job(sp, jt.numJobs, first + slot);
+            const float4 o = w.ray_o[slot];
+            const float4 d = w.ray_d[slot];
+            const float4 t4 = w.thr[slot];
+            ps.ro = xyz(o);
+            ps.tmax = o.w;
+            ps.rd = xyz(d);
+            ps.lastPdf = d.w;
+            ps.throughput = xyz(t4);
+            const uint32_t fl = __float_as_uint(t4.w);
+            ps.depth = (int)(fl & 0xffffu);
+            ps.specular = (fl >> 16) & 1u;
+            ps.inside = (fl >> 17) & 1u;
+            ps.nrcReady = (fl >> 18) & 1u;
+            ps.color = xyz(w.col[slot]);
+            ps.rng = w.rng[slot];
+            have = true;
+        }
+        if (!__any_sync(kFull, have)) break;
+        if (!have) continue;
+        const BatchJobDev& J = jt.jobs[job];
+        HitRec h;
+        uint32_t a = 0, b = 0;
+        const bool found = J.s.numNodes != 0 && trace_closest_rec<false>(J.s, ps.ro, ps.tmax, ps.rd, h, a, b);
+        ShadowReq sr;
+        const bool cont = shade(J.s, J.ubo, ps, found, h, sr);
+        if (sr.kind != 0 && shadow_visible(J.s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
+        if (cont && ++ps.depth < (int)J.ubo.maxDepth) continue;
+        w.col[slot] = f4(ps.color, 0.0f);
         have = false;
     }
 }
@@ -536,6 +598,8 @@ struct StrelkaBatch {
     // captured launch sequences
     std::map<uint64_t, cudaGraphExec_t> graphs;
     cudaStream_t capture = nullptr;
+    cudaStream_t aux = nullptr;  // shadow queries beside the next bounce
+    cudaEvent_t shadeDone = nullptr, shadowDone = nullptr;
     StrelkaBatchConfig tuned{};
     bool haveTuned = false;
 };
@@ -632,13 +696,19 @@ int launch_wavefront(StrelkaBatch* b, const JobTable& jt, const StrelkaBatchConf
     const int gridE = occupancy_grid((const void*)k_batch_extend<BLOCK>, BLOCK, b->numSMs);
     const int gridS = occupancy_grid((const void*)k_batch_shade<BLOCK>, BLOCK, b->numSMs);
     const int gridW = occupancy_grid((const void*)k_batch_shadow<BLOCK>, BLOCK, b->numSMs);
+    const int gridL = occupancy_grid((const void*)k_batch_tail<BLOCK>, BLOCK, b->numSMs);
     uint32_t f = 0;
     for (uint64_t first = 0; first < b->total; first += chunkPaths) {
         const uint32_t n = (uint32_t)std::min<uint64_t>(chunkPaths, b->total - first);
         SB_CUDA_TRY(cudaMemsetAsync(b->w.counters, 0, kWaveCounters * sizeof(uint32_t), st));
         const int gridG = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, b->numSMs * 8);
         k_batch_generate<<<gridG, kSmallBlock, 0, st>>>(jt, b->w, (uint32_t)first, n);
-        for (int depth = 0; depth < b->maxDepth; ++depth) {
+        // shadow(k) runs on the auxiliary stream beside extend(k+1) and the
+        // sort of bounce k+1 (it reads only shade(k)'s outputs); shade(k+1)
+        // waits for it, so contributions reach each path in the same order
+        const int tailDepth = std::min(b->maxDepth, kBatchTailDepth);
+        bool pendingShadow = false;
+        for (int depth = 0; depth < tailDepth; ++depth) {
             const int qin = depth & 1;
             k_batch_extend<BLOCK><<<gridE, BLOCK, 0, st>>>(jt, b->w, qin, (uint32_t)first, c.queueChunk, b->fetch + f++);
             const uint32_t* order = nullptr;
@@ -652,10 +722,20 @@ int launch_wavefront(StrelkaBatch* b, const JobTable& jt, const StrelkaBatchConf
                                                                     b->sorted);
                 order = b->sorted;
             }
+            if (pendingShadow) SB_CUDA_TRY(cudaStreamWaitEvent(st, b->shadowDone, 0));
             k_batch_shade<BLOCK><<<gridS, BLOCK, 0, st>>>(jt, b->w, qin, order, (uint32_t)first, c.queueChunk,
                                                          b->fetch + f++);
-            k_batch_shadow<BLOCK><<<gridW, BLOCK, 0, st>>>(jt, b->w, (uint32_t)first, c.queueChunk, b->fetch + f++);
+            SB_CUDA_TRY(cudaEventRecord(b->shadeDone, st));
+            SB_CUDA_TRY(cudaStreamWaitEvent(b->aux, b->shadeDone, 0));
+            k_batch_shadow<BLOCK><<<gridW, BLOCK, 0, b->aux>>>(jt, b->w, qin, (uint32_t)first, c.queueChunk,
+                                                              b->fetch + f++);
+            SB_CUDA_TRY(cudaEventRecord(b->shadowDone, b->aux));
+            pendingShadow = true;
         }
+        if (pendingShadow) SB_CUDA_TRY(cudaStreamWaitEvent(st, b->shadowDone, 0));
+        if (tailDepth < b->maxDepth)
+            k_batch_tail<BLOCK><<<gridL, BLOCK, 0, st>>>(jt, b->w, tailDepth & 1, (uint32_t)first, c.queueChunk,
+                                                        b->fetch + f++);
         k_batch_finalize<<<gridG, kSmallBlock, 0, st>>>(jt, b->w, (uint32_t)first, n, b->ctl);
     }
     SB_CUDA_TRY(cudaGetLastError());
@@ -759,7 +839,10 @@ extern "C" int strelka_batch_create(StrelkaBatch** out)
     srgb_lut_host(lut);
     bool ok = cudaMalloc(&b->srgbLut, sizeof(lut)) == cudaSuccess && cudaMalloc(&b->status, sizeof(uint32_t)) == cudaSuccess &&
               cudaMalloc(&b->ctl, sizeof(BatchCtl)) == cudaSuccess &&
-              cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking) == cudaSuccess;
+              cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->shadeDone, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->shadowDone, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         strelka_batch_destroy(b);
         return fail(STRELKA_ERR_OUT_OF_MEMORY, "batch allocation failed");
@@ -782,6 +865,9 @@ extern "C" int strelka_batch_destroy(StrelkaBatch* b)
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (b->capture) cudaStreamDestroy(b->capture);
+    if (b->aux) cudaStreamDestroy(b->aux);
+    if (b->shadeDone) cudaEventDestroy(b->shadeDone);
+    if (b->shadowDone) cudaEventDestroy(b->shadowDone);
     delete b;
     return STRELKA_OK;
 }
