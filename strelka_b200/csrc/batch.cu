@@ -201,9 +201,9 @@ __host__ __device__ __forceinline__ int batch_shadow_count(int qin) { return qin
 constexpr int kBatchTailDepth = 5;
 
 // Resident threads per SM asked of the traversal kernels: 8 x 128 for
-// closest hit and for any hit, as in the single-job pass.
+// closest hit and 9 x 128 for any hit, as in the single-job pass.
 constexpr int kExtendThreadsPerSM = 8 * 128;
-constexpr int kShadowThreadsPerSM = 8 * 128;
+constexpr int kShadowThreadsPerSM = 9 * 128;
 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, kExtendThreadsPerSM / BLOCK) k_batch_extend(JobTable jt, Wave w, int qin, uint32_t first, uint32_t chunk,
