@@ -511,6 +511,13 @@ int strelka_nrc_gradients(StrelkaNrc* nrc, const StrelkaNrcRecord* samples, uint
 int strelka_nrc_get_params(StrelkaNrc* nrc, float* mlp, float* grid);
 int strelka_nrc_set_params(StrelkaNrc* nrc, const float* mlp, const float* grid);
 /* Sizes and the per-level grid resolution (negative when the level is hashed). */
+/* Self-test of the bounded wait that guards every tensor-core completion wait
+ * of the cache's kernels (no counterpart in the reference: test support).  One
+ * thread waits for the first phase of an mbarrier, which nothing completes
+ * unless `arrive` is nonzero; after limitNs nanoseconds (at most 1 s) it gives
+ * up and sets STRELKA_DEV_MMA_TIMEOUT in *deviceStatus (a device pointer).
+ * Asynchronous on `stream`. */
+int strelka_selftest_wait_timeout(uint64_t limitNs, int arrive, uint32_t* deviceStatus, void* stream);
 /* Reads and clears the cache's device status word (STRELKA_DEV_* bits);
  * synchronises the stream. */
 int strelka_nrc_get_device_status(StrelkaNrc* nrc, void* stream, uint32_t* status);

@@ -307,6 +307,7 @@ SIGNATURES = {
     "strelka_nrc_set_params": (C.c_int, [vp, vp, vp]),
     "strelka_nrc_info": (C.c_int, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), vp]),
     "strelka_nrc_get_device_status": (C.c_int, [vp, vp, C.POINTER(C.c_uint32)]),
+    "strelka_selftest_wait_timeout": (C.c_int, [C.c_uint64, C.c_int, vp, vp]),
     "strelka_batch_create": (C.c_int, [C.POINTER(vp)]),
     "strelka_batch_destroy": (C.c_int, [vp]),
     "strelka_batch_set_jobs": (C.c_int, [vp, vp, C.c_uint32, vp]),

@@ -893,6 +893,29 @@ extern "C" int strelka_nrc_set_params(StrelkaNrc* nrc, const float* mlp, const f
     return STRELKA_OK;
 }
 
+namespace {
+// One thread waits, with the bounded wait of the tensor-core kernels, for the
+// first phase of an mbarrier; unless `arrive`, nothing completes that phase.
+__global__ void k_selftest_wait(uint64_t limitNs, int arrive, uint32_t* status)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar, 1);
+        if (arrive) tc::mbar_arrive(&bar);
+        if (!tc::mbar_wait_bounded(&bar, 0, limitNs)) atomicOr(status, STRELKA_DEV_MMA_TIMEOUT);
+    }
+}
+}  // namespace
+
+extern "C" int strelka_selftest_wait_timeout(uint64_t limitNs, int arrive, uint32_t* deviceStatus, void* stream)
+{
+    if (!deviceStatus) return fail(STRELKA_ERR_INVALID_ARGUMENT, "deviceStatus is NULL");
+    if (limitNs > 1000000000ull) return fail(STRELKA_ERR_INVALID_ARGUMENT, "limitNs above 1 s");
+    k_selftest_wait<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(limitNs, arrive, deviceStatus);
+    SB_CUDA_TRY(cudaGetLastError());
+    return STRELKA_OK;
+}
+
 extern "C" int strelka_nrc_get_device_status(StrelkaNrc* nrc, void* stream, uint32_t* status)
 {
     if (!nrc || !status) return fail(STRELKA_ERR_INVALID_ARGUMENT, "NULL argument");

@@ -109,3 +109,26 @@ def test_bad_execute_arguments(cuda, base):
     d = ds.desc(p, None)
     with pytest.raises(abi.StrelkaError):
         pt.execute(d, 16 * 16 * 2, 1, 0)
+
+
+@pytest.mark.parametrize("arrive", [0, 1])
+def test_bounded_wait_gives_up(cuda, arrive):
+    # The wait that guards every tensor-core completion in the radiance-cache
+    # kernels, on an mbarrier phase that nothing completes: it gives up after
+    # its limit and sets the status bit, and the context stays usable.  With
+    # the phase completed first, it passes without a bit.
+    import time
+    lib = abi.load()
+    status = cuda.zeros(1, dtype=cuda.int32, device="cuda")
+    t0 = time.perf_counter()
+    abi.check(lib.strelka_selftest_wait_timeout(2_000_000, arrive, status.data_ptr(), None))
+    cuda.cuda.synchronize()
+    elapsed = time.perf_counter() - t0
+    if arrive:
+        assert int(status.item()) == 0
+    else:
+        assert int(status.item()) == abi.DEV_MMA_TIMEOUT
+        assert elapsed >= 2e-3
+    assert int((cuda.ones(4, device="cuda") * 2).sum().item()) == 8
+    with pytest.raises(abi.StrelkaError):
+        abi.check(lib.strelka_selftest_wait_timeout(2_000_000_000, 0, status.data_ptr(), None))
