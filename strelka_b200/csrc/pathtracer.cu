@@ -691,57 +691,19 @@ __global__ void __launch_bounds__(kSmallBlock) k_finalize(Wave w, float* __restr
 // are few and long, so they run in small blocks spread over many SMs.
 constexpr int kNrcPathBlock = 32;
 
-__global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, PathTracerParam ubo, uint32_t pathsPerBatch,
-                                                                   uint32_t batches, float diffuseRoughness,
-                                                                   StrelkaNrcRecord* __restrict__ out, uint32_t* count,
-                                                                   uint32_t capPerBatch)
+// Writes the training records of a finished path: every recorded vertex k
+// with target (C_end - C_k) / T_k.
+__device__ __forceinline__ void nrc_emit_records(const float4 (&vrec)[kNrcMaxVerts][3], const v3 (&cIn)[kNrcMaxVerts],
+                                                 const v3 (&tIn)[kNrcMaxVerts], int nv, v3 cEnd, StrelkaNrcRecord* dst,
+                                                 uint32_t* count, uint32_t cap)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= pathsPerBatch * batches) return;
-    const uint32_t batch = i / pathsPerBatch;
-    const uint64_t total = (uint64_t)ubo.dimension[0] * (uint64_t)ubo.dimension[1] * (uint64_t)ubo.spp;
-    const uint32_t fseed = jenkins_hash((ubo.frameNumber + batch * 0x2545F491u) ^ 0x5bd1e995u);
-    const uint32_t h = jenkins_hash(i * 0x9E3779B9u ^ fseed);
-    PathTracerParam u = ubo;
-    u.frameNumber = (ubo.frameNumber + batch * 0x2545F491u) ^ 0x3c6ef372u;
-    PathState ps;
-    init_path(u, (uint64_t)h % total, ps);
-    float4 vrec[kNrcMaxVerts][3];
-    v3 cIn[kNrcMaxVerts], tIn[kNrcMaxVerts];
-    int nv = 0;
-    const int maxDepth = (int)ubo.maxDepth;
-    while (ps.depth < maxDepth) {
-        HitRec hit;
-        uint32_t a = 0, b = 0;
-        bool found = s.numNodes != 0 && trace_closest_rec<false>(s, ps.ro, ps.tmax, ps.rd, hit, a, b);
-        const v3 c0 = ps.color, t0 = ps.throughput, dOut = vneg(ps.rd);
-        NrcShade nq;
-        nq.mode = 1;
-        nq.diffuseRoughness = diffuseRoughness;
-        nq.has = false;
-        nq.terminate = false;
-        ShadowReq sr;
-        bool cont = shade(s, u, ps, found, hit, sr, &nq);
-        if (sr.kind != 0 && shadow_visible(s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
-        if (nq.has && nv < kNrcMaxVerts) {
-            vrec[nv][0] = f4(nq.pos, nq.rough);
-            vrec[nv][1] = f4(dOut, nq.normal.x);
-            vrec[nv][2] = make_float4(nq.normal.y, nq.normal.z, 0.0f, 0.0f);
-            cIn[nv] = c0;
-            tIn[nv] = t0;
-            ++nv;
-        }
-        if (!cont) break;
-        ++ps.depth;
-    }
-    StrelkaNrcRecord* dst = out + (size_t)batch * capPerBatch;
     for (int k = 0; k < nv; ++k) {
         const v3 t = tIn[k];
         if (!(t.x > 0.0f && t.y > 0.0f && t.z > 0.0f)) continue;
-        const v3 L = V((ps.color.x - cIn[k].x) / t.x, (ps.color.y - cIn[k].y) / t.y, (ps.color.z - cIn[k].z) / t.z);
+        const v3 L = V((cEnd.x - cIn[k].x) / t.x, (cEnd.y - cIn[k].y) / t.y, (cEnd.z - cIn[k].z) / t.z);
         if (!all_finite(L)) continue;
-        const uint32_t pos = atomicAdd(&count[batch], 1u);
-        if (pos >= capPerBatch) continue;
+        const uint32_t pos = atomicAdd(count, 1u);
+        if (pos >= cap) continue;
         StrelkaNrcRecord r;
         r.pos[0] = vrec[k][0].x; r.pos[1] = vrec[k][0].y; r.pos[2] = vrec[k][0].z;
         r.dir[0] = vrec[k][1].x; r.dir[1] = vrec[k][1].y; r.dir[2] = vrec[k][1].z;
@@ -754,6 +716,68 @@ __global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, P
         r.pad[0] = 0;
         r.pad[1] = 0;
         dst[pos] = r;
+    }
+}
+
+// Training paths of the radiance cache: path i of batch i / pathsPerBatch
+// starts at a hashed sample of the frame and is traced to its end; every
+// vertex becomes a record (nrc_emit_records).  Persistent lanes: a lane takes
+// path indices from an atomic head (*head, zero at launch) and, when its path
+// ends, takes the next one, bounce by bounce, so no warp waits for its
+// longest path.
+__global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, PathTracerParam ubo, uint32_t pathsPerBatch,
+                                                                   uint32_t batches, float diffuseRoughness,
+                                                                   StrelkaNrcRecord* __restrict__ out, uint32_t* count,
+                                                                   uint32_t capPerBatch, uint32_t* head)
+{
+    const uint32_t n = pathsPerBatch * batches;
+    const uint64_t total = (uint64_t)ubo.dimension[0] * (uint64_t)ubo.dimension[1] * (uint64_t)ubo.spp;
+    const int maxDepth = (int)ubo.maxDepth;
+    WarpPool pool{0, 0, 0};
+    bool have = false;
+    uint32_t batch = 0;
+    PathTracerParam u = ubo;
+    PathState ps;
+    float4 vrec[kNrcMaxVerts][3];
+    v3 cIn[kNrcMaxVerts], tIn[kNrcMaxVerts];
+    int nv = 0;
+    while (true) {
+        const uint32_t i = pool_take(pool, head, n, 32, !have);
+        if (!have && i != SB_INVALID) {
+            batch = i / pathsPerBatch;
+            const uint32_t fseed = jenkins_hash((ubo.frameNumber + batch * 0x2545F491u) ^ 0x5bd1e995u);
+            const uint32_t h = jenkins_hash(i * 0x9E3779B9u ^ fseed);
+            u.frameNumber = (ubo.frameNumber + batch * 0x2545F491u) ^ 0x3c6ef372u;
+            init_path(u, (uint64_t)h % total, ps);
+            nv = 0;
+            have = ps.depth < maxDepth;  // else nothing to trace and no vertex to record
+        }
+        // (every lane reaches the vote: pool_take and __any_sync are warp-collective)
+        if (!__any_sync(0xffffffffu, have)) break;
+        if (!have) continue;
+        HitRec hit;
+        uint32_t a = 0, b = 0;
+        const bool found = s.numNodes != 0 && trace_closest_rec<false>(s, ps.ro, ps.tmax, ps.rd, hit, a, b);
+        const v3 c0 = ps.color, t0 = ps.throughput, dOut = vneg(ps.rd);
+        NrcShade nq;
+        nq.mode = 1;
+        nq.diffuseRoughness = diffuseRoughness;
+        nq.has = false;
+        nq.terminate = false;
+        ShadowReq sr;
+        const bool cont = shade(s, u, ps, found, hit, sr, &nq);
+        if (sr.kind != 0 && shadow_visible(s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
+        if (nq.has && nv < kNrcMaxVerts) {
+            vrec[nv][0] = f4(nq.pos, nq.rough);
+            vrec[nv][1] = f4(dOut, nq.normal.x);
+            vrec[nv][2] = make_float4(nq.normal.y, nq.normal.z, 0.0f, 0.0f);
+            cIn[nv] = c0;
+            tIn[nv] = t0;
+            ++nv;
+        }
+        if (cont && ++ps.depth < maxDepth) continue;
+        nrc_emit_records(vrec, cIn, tIn, nv, ps.color, out + (size_t)batch * capPerBatch, &count[batch], capPerBatch);
+        have = false;
     }
 }
 
@@ -844,6 +868,7 @@ struct StrelkaPathTracer {
     std::vector<Rec> recs;
     std::vector<cudaEvent_t> eventPool;
     size_t eventsUsed = 0;
+    int nrcPathGrid = 0;
     int extendGrid = 0, shadowGrid = 0, tailGrid = 0, traceGrid = 0, traceGridAny = 0, shadeGrid = 0, shadeGridNrc = 0, smallGrid = 0;
     unsigned long long* visitCounters = nullptr;  // 6 entries (STRELKA_PT_COUNT)
     // radiance cache
@@ -1139,6 +1164,7 @@ extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, 
     pt->extendGrid = occupancy_grid((const void*)k_extend<false>, kExtendBlock, pt->numSMs);
     pt->shadowGrid = occupancy_grid((const void*)k_shadow<false>, kExtendBlock, pt->numSMs);
     pt->tailGrid = occupancy_grid((const void*)k_tail, kExtendBlock, pt->numSMs);
+    pt->nrcPathGrid = occupancy_grid((const void*)k_nrc_train_paths, kNrcPathBlock, pt->numSMs);
     pt->traceGrid = occupancy_grid((const void*)k_trace<false, false, false>, kExtendBlock, pt->numSMs);
     pt->traceGridAny = occupancy_grid((const void*)k_trace<true, false, false>, kExtendBlock, pt->numSMs);
     pt->shadeGrid = occupancy_grid((const void*)k_shade<false>, kShadeBlock, pt->numSMs);
@@ -1183,12 +1209,14 @@ static int nrc_train_frame(StrelkaPathTracer* pt, const DevScene& s, const PathT
     if (nTrain == 0 || batches == 0) return STRELKA_OK;
     if ((uint64_t)nTrain * batches > (1ull << 26))
         return fail(STRELKA_ERR_INVALID_ARGUMENT, "trainPaths x batches exceeds 2^26");
-    if (batches + 1 > pt->nrcCountCap) {
+    // counters: [0] queries, [1 + b] records of batch b, [1 + batches] the
+    // training kernel's work head
+    if (batches + 2 > pt->nrcCountCap) {
         if (pt->nrcCounts) cudaFree(pt->nrcCounts);
         pt->nrcCounts = nullptr;
         pt->nrcCountCap = 0;
-        SB_CUDA_TRY(cudaMalloc(&pt->nrcCounts, (size_t)(batches + 1) * sizeof(uint32_t)));
-        pt->nrcCountCap = batches + 1;
+        SB_CUDA_TRY(cudaMalloc(&pt->nrcCounts, (size_t)(batches + 2) * sizeof(uint32_t)));
+        pt->nrcCountCap = batches + 2;
     }
     const size_t capPerBatch =
         (size_t)nTrain * std::min<uint32_t>(std::max<uint32_t>(ubo.maxDepth, 1u), (uint32_t)kNrcMaxVerts);
@@ -1201,11 +1229,12 @@ static int nrc_train_frame(StrelkaPathTracer* pt, const DevScene& s, const PathT
     }
     {
         Timer t(pt, KC_NRC_PATHS, st);
-        SB_CUDA_TRY(cudaMemsetAsync(pt->nrcCounts + 1, 0, batches * sizeof(uint32_t), st));
+        SB_CUDA_TRY(cudaMemsetAsync(pt->nrcCounts + 1, 0, (batches + 1) * sizeof(uint32_t), st));
         const uint32_t n = nTrain * batches;
-        k_nrc_train_paths<<<(n + kNrcPathBlock - 1) / kNrcPathBlock, kNrcPathBlock, 0, st>>>(
-            s, ubo, nTrain, batches, pt->nrcCfg.diffuseRoughness, pt->nrcTrain, pt->nrcCounts + 1,
-            (uint32_t)capPerBatch);
+        const int grid = std::min<int>((int)((n + kNrcPathBlock - 1) / kNrcPathBlock), pt->nrcPathGrid);
+        k_nrc_train_paths<<<grid, kNrcPathBlock, 0, st>>>(s, ubo, nTrain, batches, pt->nrcCfg.diffuseRoughness,
+                                                          pt->nrcTrain, pt->nrcCounts + 1, (uint32_t)capPerBatch,
+                                                          pt->nrcCounts + 1 + batches);
         SB_CUDA_TRY(cudaGetLastError());
     }
     Timer t(pt, KC_NRC_TRAIN, st);
