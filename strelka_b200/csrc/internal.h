@@ -16,7 +16,7 @@ int validate_scene_desc(const PathTracerDesc* d);
 // Device tables derived from a scene's BVH, all in one allocation of
 // scene_tables_bytes(numNodes) bytes: the leaf-triangle records (4 float4 per
 // node slot), the 4-wide BVH (8 float4 per node, at most numNodes/2 + 1
-// nodes) and the scratch of its build.
+// nodes) and the scratch of its build (16 B per node).
 struct SceneTables {
     float4* rec = nullptr;
     float4* wide = nullptr;
@@ -24,6 +24,8 @@ struct SceneTables {
     uint32_t* parent = nullptr;
     uint32_t* flag = nullptr;
     uint32_t* map = nullptr;
+    uint32_t* extra = nullptr;  // pointer-jumping parities
+    uint32_t* deep = nullptr;   // set when the tree is too deep for the walk-up
     void* scan = nullptr;
     size_t scanBytes = 0;
 };

@@ -145,9 +145,16 @@ __global__ void k_wide_parent(const float4* __restrict__ nodes, uint32_t numNode
     }
 }
 
-// 1 for the inner nodes at even depth
+// Steps a thread walks up towards the root in k_wide_flag before leaving
+// the node to the pointer-jumping pass (deep trees, chains).
+constexpr uint32_t kWideWalkCap = 1024;
+
+// 1 for the inner nodes at even depth, by walking up to the root.  A walk
+// longer than kWideWalkCap sets *deep instead, and the pointer-jumping pass
+// below recomputes every node's parity, so a chain-shaped tree costs
+// O(n log n), not O(n^2).
 __global__ void k_wide_flag(const float4* __restrict__ nodes, uint32_t numNodes, const uint32_t* __restrict__ parent,
-                            uint32_t* __restrict__ flag, uint32_t* status)
+                            uint32_t* __restrict__ flag, uint32_t* deep, uint32_t* status)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x) {
         uint32_t f = 0;
@@ -156,13 +163,58 @@ __global__ void k_wide_flag(const float4* __restrict__ nodes, uint32_t numNodes,
             bool ok = true;
             while (p != 0) {
                 p = parent[p];
-                if (p == SB_INVALID || ++depth > numNodes) {
+                if (p == SB_INVALID) {
                     ok = false;
+                    break;
+                }
+                if (++depth > kWideWalkCap) {
+                    atomicOr(deep, 1u);
                     break;
                 }
             }
             if (!ok) atomicOr(status, STRELKA_DEV_NODE_OOB);
             f = ok && (depth & 1u) == 0 ? 1u : 0u;
+        }
+        flag[i] = f;
+    }
+}
+
+// Pointer jumping (only when *deep): anc[i] is the ancestor 2^r levels up and
+// par[i] the parity of that distance; after ceil(log2 n) + 1 rounds every
+// ancestor is past the root and par[i] is the parity of the depth.
+__global__ void k_wide_jump_init(uint32_t numNodes, const uint32_t* __restrict__ parent, uint32_t* __restrict__ par,
+                                 const uint32_t* deep)
+{
+    if (!*deep) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x)
+        par[i] = parent[i] != SB_INVALID ? 1u : 0u;
+}
+__global__ void k_wide_jump(uint32_t numNodes, const uint32_t* __restrict__ ancIn, const uint32_t* __restrict__ parIn,
+                            uint32_t* __restrict__ ancOut, uint32_t* __restrict__ parOut, const uint32_t* deep)
+{
+    if (!*deep) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x) {
+        const uint32_t a = ancIn[i];
+        if (a == SB_INVALID || a >= numNodes) {
+            ancOut[i] = a;
+            parOut[i] = parIn[i];
+        } else {
+            ancOut[i] = ancIn[a];
+            parOut[i] = parIn[i] ^ parIn[a];
+        }
+    }
+}
+__global__ void k_wide_jump_finish(const float4* __restrict__ nodes, uint32_t numNodes, const uint32_t* __restrict__ anc,
+                                   const uint32_t* __restrict__ par, uint32_t* __restrict__ flag, const uint32_t* deep,
+                                   uint32_t* status)
+{
+    if (!*deep) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x) {
+        uint32_t f = 0;
+        if (__float_as_uint(nodes[2 * (size_t)i].w) == SB_INVALID) {
+            // an ancestor left means the parents form a cycle
+            if (anc[i] != SB_INVALID) atomicOr(status, STRELKA_DEV_NODE_OOB);
+            else f = par[i] == 0 ? 1u : 0u;
         }
         flag[i] = f;
     }
@@ -1046,7 +1098,7 @@ size_t scene_tables_bytes(uint32_t numNodes)
 {
     const size_t n = std::max<uint32_t>(numNodes, 1);
     const size_t wideCap = n / 2 + 1;
-    return align256(n * 4 * sizeof(float4)) + align256(wideCap * 8 * sizeof(float4)) + 3 * align256(n * 4) +
+    return align256(n * 4 * sizeof(float4)) + align256(wideCap * 8 * sizeof(float4)) + 4 * align256(n * 4) + 256 +
            align256(scan_bytes(numNodes));
 }
 
@@ -1066,6 +1118,10 @@ SceneTables scene_tables(void* base, uint32_t numNodes)
     p += align256(n * 4);
     t.map = reinterpret_cast<uint32_t*>(p);
     p += align256(n * 4);
+    t.extra = reinterpret_cast<uint32_t*>(p);
+    p += align256(n * 4);
+    t.deep = reinterpret_cast<uint32_t*>(p);
+    p += 256;
     t.scan = p;
     t.scanBytes = scan_bytes(numNodes);
     return t;
@@ -1081,7 +1137,23 @@ int launch_prep_tables(const BVHNode* nodes, uint32_t numNodes, const InstanceCo
     k_prep_rec<<<grid, 256, 0, st>>>(nd, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, t.rec, status);
     SB_CUDA_TRY(cudaMemsetAsync(t.parent, 0xFF, (size_t)numNodes * 4, st));
     k_wide_parent<<<grid, 256, 0, st>>>(nd, numNodes, t.parent);
-    k_wide_flag<<<grid, 256, 0, st>>>(nd, numNodes, t.parent, t.flag, status);
+    SB_CUDA_TRY(cudaMemsetAsync(t.deep, 0, sizeof(uint32_t), st));
+    k_wide_flag<<<grid, 256, 0, st>>>(nd, numNodes, t.parent, t.flag, t.deep, status);
+    {
+        // deep trees only (the kernels return at once unless *deep): ancestors
+        // ping-pong between parent and map (map is free until the scan),
+        // parities between extra and flag
+        int rounds = 1;
+        while (rounds < 32 && (1ull << (rounds - 1)) < (uint64_t)numNodes) ++rounds;
+        k_wide_jump_init<<<grid, 256, 0, st>>>(numNodes, t.parent, t.extra, t.deep);
+        uint32_t *ancIn = t.parent, *ancOut = t.map, *parIn = t.extra, *parOut = t.flag;
+        for (int r = 0; r < rounds; ++r) {
+            k_wide_jump<<<grid, 256, 0, st>>>(numNodes, ancIn, parIn, ancOut, parOut, t.deep);
+            std::swap(ancIn, ancOut);
+            std::swap(parIn, parOut);
+        }
+        k_wide_jump_finish<<<grid, 256, 0, st>>>(nd, numNodes, ancIn, parIn, t.flag, t.deep, status);
+    }
     size_t bytes = t.scanBytes;
     SB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(t.scan, bytes, t.flag, t.map, (int)numNodes, st));
     k_wide_build<<<grid, 256, 0, st>>>(nd, numNodes, t.flag, t.map, t.wide, t.wideCap, status);

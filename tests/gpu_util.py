@@ -72,3 +72,41 @@ def vertex_edge_rays(seed_origins=None):
         r[:, 4:7] = d
         rays.append(r)
     return np.concatenate(rays)
+
+
+def chain_bvh(scene):
+    """A chain-shaped BVH over the triangles of a one-instance identity scene
+    (scenes.soup): inner node k has leaf k as its left child and inner node
+    k + 1 as its right child, in the reference's flattened depth-first layout
+    (inner k at index 2k, leaf k at 2k + 1, the last leaf at 2(n - 1)).  Its
+    depth is n - 1; boxes enclose their subtrees, padded +1e-6 on the max
+    corner like the builders."""
+    import copy
+    n = scene.num_triangles
+    pos = scene.vb.view(F32).reshape(-1, 8)[:, :3]
+    tri = pos[scene.ib.reshape(-1, 3)]  # (n, 3, 3)
+    lo_t, hi_t = tri.min(1), tri.max(1) + F32(1e-6)
+    N = 2 * n - 1
+    f = np.zeros((N, 8), F32)
+    u = f.view(np.int32)
+    # suffix bounds: box of triangles k .. n-1
+    slo = np.minimum.accumulate(lo_t[::-1], axis=0)[::-1]
+    shi = np.maximum.accumulate(hi_t[::-1], axis=0)[::-1]
+    for k in range(n - 1):
+        i = 2 * k
+        f[i, 0:3], f[i, 4:7] = slo[k], shi[k]
+        u[i, 3] = -1
+        u[i, 7] = -1                       # escape of every inner node: the end
+        leaf = 2 * k + 1
+        f[leaf, 0:3], f[leaf, 4:7] = lo_t[k], hi_t[k]
+        u[leaf, 0] = k                     # minBounds[0] holds the triangle index bits
+        u[leaf, 3] = 0                     # instance 0
+        u[leaf, 7] = 2 * k + 2             # escape: the right sibling
+    last = 2 * (n - 1)
+    f[last, 0:3], f[last, 4:7] = lo_t[n - 1], hi_t[n - 1]
+    u[last, 0] = n - 1
+    u[last, 3] = 0
+    u[last, 7] = -1
+    c = copy.copy(scene)
+    c.nodes = f.view(np.uint8).reshape(-1).copy()
+    return c

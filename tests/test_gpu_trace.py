@@ -118,3 +118,18 @@ def test_host_buffers_entry(cuda, cornell_setup):
     abi.check(abi.load().strelka_trace_host(pt.handle, C.byref(desc), rays.ctypes.data, hits.ctypes.data, None))
     o, _, _ = oracle.trace(view, rays)
     assert np.array_equal(hits, o)
+
+
+def test_chain_tree_deeper_than_the_walk_cap(cuda):
+    # depth 2999 > the 1024-step walk-up of the 4-wide build: its parities
+    # come from the pointer-jumping pass; hits equal the reference's
+    from gpu_util import chain_bvh
+    s = chain_bvh(scenes.soup(3000, 21))
+    view, ds, pt = oracle.SceneView(s), DeviceScene(s), PathTracer()
+    rays = scenes.rays_soup(20_000, 22)
+    for flags in (abi.TRACE_CLOSEST, abi.TRACE_ANY):
+        g, _ = run_trace(cuda, pt, ds, rays, flags)
+        o, found, _ = oracle.trace(view, rays, any_hit=flags == abi.TRACE_ANY)
+        assert found.sum() > 50
+        assert np.array_equal(g, o)
+    assert pt.device_status() == 0

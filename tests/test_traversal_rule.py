@@ -57,3 +57,20 @@ def test_tiny_trees(num_tris):
         ref, _, _ = oracle.trace(v, rays, any_hit=any_hit)
         wide, _, _ = oracle.trace(v, rays, any_hit=any_hit, prune=2)
         assert np.array_equal(wide, ref)
+
+
+def test_chain_tree():
+    # a BVH of depth n - 1 (much deeper than any builder makes)
+    from gpu_util import chain_bvh
+    s = chain_bvh(scenes.soup(600, 12))
+    v = oracle.SceneView(s)
+    rays = scenes.rays_soup(3000, 13)
+    for any_hit in (False, True):
+        ref, found, _ = oracle.trace(v, rays, any_hit=any_hit)
+        wide, _, _ = oracle.trace(v, rays, any_hit=any_hit, prune=2)
+        assert np.array_equal(wide, ref)
+    # the chain is a valid tree: the reference finds the same hits over it as
+    # over the builder's tree
+    base, _, _ = oracle.trace(oracle.SceneView(scenes.soup(600, 12)), rays)
+    ref, _, _ = oracle.trace(v, rays)
+    assert np.array_equal(ref[:, 3:], base[:, 3:]) and found.sum() > 0
