@@ -301,8 +301,9 @@ typedef struct UpscaleDesc {
 /* ------------------------------------------------------------------------- */
 /* Path tracer pass object (replaces PathTracer : ComputePass<PathTracerParam>,
  * include/render/pathtracer.h:33-50, src/render/pathtracer.cpp:1-94).  The
- * object caches scene-derived device data (a leaf triangle table and a 4-wide
- * BVH derived from bvhNodes, about 88 bytes per BVH node in all) keyed by
+ * object caches scene-derived device data (a leaf triangle table, a 4-wide
+ * BVH derived from bvhNodes and its build scratch: 144 bytes per BVH node
+ * allocated) keyed by
  * PathTracerDesc.sceneVersion and the buffer pointers, and owns the
  * wavefront path queues. */
 
