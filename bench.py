@@ -48,6 +48,12 @@ UNIT = "Mpaths/s"
 # roofline.traffic is this figure times the rays of an average launch.
 EXTEND_DRAM_BYTES_PER_RAY = 267.2
 
+# DRAM bytes (read + write) per closest-hit query of the ray-query kernel on
+# the 1M-triangle soup with 4M rays, from one ncu capture of a timed launch
+# (dram__bytes_read.sum + dram__bytes_write.sum = 2.160 + 0.165 GB;
+# profiles/trace_soup_1M_4M.md).
+TRACE_SOUP_DRAM_BYTES_PER_RAY = 581.4
+
 # Bytes a traversal reads per 4-wide node it processes: the bounds of its four
 # entries (6 float4) and their refs (1 float4).
 WIDE_NODE_BYTES = 112
@@ -221,7 +227,10 @@ def run_traversal(args):
             "config": {"workload": f"traversal microbenchmark: {args.tris} soup triangles (log-normal size, mu=ln 0.003, "
                                    f"sigma=0.5), {n} rays, closest + any hit", "l2": "inputs larger than L2"},
             "roofline": {"bound": "hbm", "achieved": res["closest"]["achieved_gbs"], "peak": peak, "unit": "GB/s",
-                         "frac": res["closest"]["frac"], "traffic": None},
+                         "frac": res["closest"]["frac"],
+                         "traffic": (TRACE_SOUP_DRAM_BYTES_PER_RAY * n
+                                     if (args.tris, args.rays) == (1_000_000, 4_000_000) else None),
+                         "traffic_source": "ncu DRAM bytes of one closest-hit launch on the default soup"},
             "detail": res}
     print(json.dumps(line), flush=True)
 
