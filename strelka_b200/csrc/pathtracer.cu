@@ -507,6 +507,12 @@ __global__ void __launch_bounds__(kSmallBlock) k_sort_scatter(Wave w, int qin, u
 // paths to the other queue and next-event requests to the shadow queue.
 // Shading is latency-bound at the 128 registers it would take; 5 resident
 // blocks (a few spills) hide more of its gathers than 4.
+// First bounce whose shade queue is sorted by material: camera rays (bounce
+// 0) arrive in pixel order and hit coherent materials already, so sorting
+// them costs more than it saves (52.6 -> 52.2 ms per large frame without).
+#ifndef SB_SORT_FROM_DEPTH
+#define SB_SORT_FROM_DEPTH 1
+#endif
 #ifndef SB_SHADE_MINBLOCKS
 #define SB_SHADE_MINBLOCKS 5
 #endif
@@ -1440,7 +1446,7 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
                 else k_extend<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, qchunk, nullptr);
             }
             const uint32_t* order = nullptr;
-            if (sortKeys) {
+            if (sortKeys && depth >= SB_SORT_FROM_DEPTH) {
                 Timer t(pt, KC_SORT, st, 3);
                 const int gridK = std::min<int>((n + kSmallBlock - 1) / kSmallBlock, pt->numSMs * 4);
                 k_sort_count<<<gridK, kSmallBlock, 0, st>>>(s, pt->main.w, qin, sortKeys, pt->sortHist, pt->main.keys);
