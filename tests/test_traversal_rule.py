@@ -74,3 +74,24 @@ def test_chain_tree():
     base, _, _ = oracle.trace(oracle.SceneView(scenes.soup(600, 12)), rays)
     ref, _, _ = oracle.trace(v, rays)
     assert np.array_equal(ref[:, 3:], base[:, 3:]) and found.sum() > 0
+
+
+def test_instanced_scene():
+    # the large-render generator at toy size: several instances, leaves of
+    # different instance ids, an environment-lit open scene
+    s = scenes.large(width=16, height=8, instances=5, frequency=8, num_textures=1, tex_size=16, env_width=16,
+                     env_height=8, max_depth=4, spp=1, seed=9)
+    v = oracle.SceneView(s)
+    lo, hi = s.bounds()
+    rng = np.random.default_rng(14)
+    n = 6000
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, :3] = rng.uniform(lo, hi, (n, 3))
+    d = rng.normal(size=(n, 3))
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 3] = np.where(np.arange(n) % 2 == 0, 1e9, rng.uniform(0.1, 3.0, n))
+    for any_hit in (False, True):
+        ref, found, _ = oracle.trace(v, rays, any_hit=any_hit)
+        wide, _, _ = oracle.trace(v, rays, any_hit=any_hit, prune=2)
+        assert found.sum() > 100
+        assert np.array_equal(wide, ref)
