@@ -124,3 +124,29 @@ def test_training_fits_a_radiance_field(cuda):
     assert np.mean(losses[-20:]) < 0.05 * np.mean(losses[:5]), (losses[:5], losses[-5:])
     assert rel < 0.02, rel
     lib.strelka_nrc_destroy(h)
+
+
+@pytest.mark.parametrize("n", [200, 1])
+def test_gradients_partial_tile(cuda, n):
+    # a batch that fills no whole 128-record tile: the padded rows of the last
+    # tile contribute nothing
+    lib, h, nm, ng = make_nrc(seed=4)
+    rng = np.random.default_rng(6)
+    mlp, _ = params(lib, h, nm, ng)
+    grid = rng.normal(0, 0.3, ng).astype(np.float32)
+    abi.check(lib.strelka_nrc_set_params(h, None, grid.ctypes.data))
+    rec = records(n, 8)
+    gm = np.zeros(nm, np.float32)
+    gg = np.zeros(ng, np.float32)
+    loss = C.c_float()
+    abi.check(lib.strelka_nrc_gradients(h, to_device(rec).data_ptr(), n, gm.ctypes.data, gg.ctypes.data,
+                                        C.byref(loss), None))
+    rm, rg, rloss = nrc_ref.gradients(rec, mlp, grid, BMIN, BMAX, LOG2_T)
+    assert abs(loss.value - rloss) <= 1e-3 * abs(rloss)
+    a, b = gm.astype(np.float64), rm
+    assert np.linalg.norm(a - b) <= 3e-2 * np.linalg.norm(b)
+    assert np.linalg.norm(gg - rg) <= 3e-2 * np.linalg.norm(rg)
+    status = C.c_uint32(1)
+    abi.check(lib.strelka_nrc_get_device_status(h, None, C.byref(status)))
+    assert status.value == 0
+    lib.strelka_nrc_destroy(h)
