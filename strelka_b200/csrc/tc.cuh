@@ -1,10 +1,12 @@
 // tc.cuh — sm_100a tensor-core primitives (tcgen05 + TMEM) as inline PTX.
 //
-// Used by the radiance cache's fused MLP: one CTA of 128 threads owns a
-// 128-row tile, TMEM lane i holds row i, activations live in TMEM as the A
-// operand of `tcgen05.mma ... kind::f16` (the "A from tensor memory" form)
-// and the layer weights sit in shared memory as the B operand, described by
-// a K-major, non-swizzled matrix descriptor.
+// Used by the radiance cache's fused MLP (nrc.cu).  A CTA owns 128-row tiles
+// with row i in TMEM lane i; every warpgroup of the CTA reaches all 128 lanes
+// and the warpgroups split the columns.  Inference keeps the activations in
+// TMEM as the A operand of `tcgen05.mma ... kind::f16` (the "A from tensor
+// memory" form); training keeps them in shared memory (both operands from
+// shared memory).  Operands in shared memory are described by non-swizzled
+// matrix descriptors, K-major or MN-major.
 //
 // Shared-memory operand layout (K-major, no swizzle): the matrix is cut into
 // core matrices of 8 rows x 16 bytes (8 x 8 halves), each stored as 128
