@@ -43,15 +43,14 @@ UNIT = "Mpaths/s"
 
 # DRAM bytes (read + write) per closest-hit query of the extend kernel on this
 # workload, from one ncu capture of a full frame's 5 extend launches
-# (dram__bytes_read.sum + dram__bytes_write.sum = 18.40 GB for 68.87M rays;
-# profiles/extend_large_1080p16_dram.md).  bench.py cannot run ncu itself, so
+# (dram__bytes_read.sum + dram__bytes_write.sum = 18.40 GB for 68.87M rays).
+# bench.py cannot run ncu itself, so
 # roofline.traffic is this figure times the rays of an average launch.
 EXTEND_DRAM_BYTES_PER_RAY = 267.2
 
 # DRAM bytes (read + write) per closest-hit query of the ray-query kernel on
 # the 1M-triangle soup with 4M rays, from one ncu capture of a timed launch
-# (dram__bytes_read.sum + dram__bytes_write.sum = 2.160 + 0.165 GB;
-# profiles/trace_soup_1M_4M.md).
+# (dram__bytes_read.sum + dram__bytes_write.sum = 2.160 + 0.165 GB).
 TRACE_SOUP_DRAM_BYTES_PER_RAY = 581.4
 
 # Bytes a traversal reads per 4-wide node it processes: the bounds of its four

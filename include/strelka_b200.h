@@ -461,14 +461,18 @@ int strelka_trace_host(StrelkaPathTracer* pt, const TraceDesc* desc, const Ray* 
  * allocate device memory (an engine whose allocator owns the whole heap, a
  * real-time loop that cannot afford cudaMalloc's implicit synchronisation):
  * it needs no pass object and keeps its scratch (the derived leaf-triangle
- * table) in a fixed 12 MiB __device__ array that every GPU loading the
- * library holds until exit.  Scenes above 262,144 BVH nodes (131,072
- * triangles) are rejected with STRELKA_ERR_INVALID_ARGUMENT; flags other
- * than STRELKA_TRACE_ANY are rejected with STRELKA_ERR_UNSUPPORTED.  The
- * first call on a device looks up the scratch address for that device, so
- * make it before starting any stream capture.  All calls share the scratch:
- * calls that overlap on the GPU race.  deviceStatus (a device word, may be
- * NULL) receives this call's STRELKA_DEV_* bits. */
+ * table) in a fixed 12 MiB __device__ array.  Under CUDA's lazy module
+ * loading (the default since 12.2) the runtime reserves that array on a
+ * device at the first call there and holds it until exit, so a caller whose
+ * allocator takes the whole heap should make one call per device first
+ * (numNodes = 0 and numRays = 0 does only this set-up).  Scenes above
+ * 262,144 BVH nodes (131,072 triangles) are rejected with
+ * STRELKA_ERR_INVALID_ARGUMENT; flags other than STRELKA_TRACE_ANY are
+ * rejected with STRELKA_ERR_UNSUPPORTED.  The first call on a device looks
+ * up the scratch address for that device, so make it before starting any
+ * stream capture.  All calls share the scratch: calls that overlap on the
+ * GPU race.  deviceStatus (a device word, may be NULL) receives this call's
+ * STRELKA_DEV_* bits. */
 int strelka_trace_execute_noalloc(const TraceDesc* desc, uint32_t* deviceStatus, void* stream);
 
 /* ------------------------------------------------------------------------- */
@@ -520,7 +524,12 @@ int strelka_nrc_set_params(StrelkaNrc* nrc, const float* mlp, const float* grid)
  * Asynchronous on `stream`. */
 int strelka_selftest_wait_timeout(uint64_t limitNs, int arrive, uint32_t* deviceStatus, void* stream);
 /* Reads and clears the cache's device status word (STRELKA_DEV_* bits);
- * synchronises the stream. */
+ * synchronises the stream.  When STRELKA_DEV_MMA_TIMEOUT is set, every
+ * output of the launches since the previous read (predictions, gradients,
+ * the weights and grid after an Adam step) is undefined: a CTA that gave up
+ * freed its tensor memory while its matrix multiply may still have been
+ * writing it, which can corrupt another CTA's tile.  Discard them and
+ * re-create the cache. */
 int strelka_nrc_get_device_status(StrelkaNrc* nrc, void* stream, uint32_t* status);
 int strelka_nrc_info(StrelkaNrc* nrc, uint32_t* numMlpParams, uint64_t* numGridParams, int32_t* levelRes);
 

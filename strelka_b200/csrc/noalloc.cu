@@ -9,13 +9,18 @@
 // them the same closest/any-hit queries with the scratch table in a
 // file-scope __device__ array of fixed size instead.
 //
-// The array costs 12 MiB (+256 B) on every GPU that loads this library, held
-// until the process exits; scenes with more than kNoAllocMaxNodes BVH nodes
-// are rejected.  Every call shares the array, so two calls whose work
-// overlaps on the GPU (for example on two streams of the same device) race
-// on it; serialise such calls.  Each call rebuilds the table and clears the
-// status word before using them, so nothing depends on what the previous
-// call left behind.
+// The array costs 12 MiB (+256 B) of device memory.  With CUDA's lazy module
+// loading (the default since CUDA 12.2) the runtime reserves it when this
+// file's module first loads on a device, which is the first call of this
+// entry point there (its set-up asks for the array's address), and holds it
+// until the process exits.  A caller whose allocator takes the whole heap
+// should therefore make one call per device before reserving its heap; a
+// call with numNodes = 0 and numRays = 0 does only that set-up.  Scenes with
+// more than kNoAllocMaxNodes BVH nodes are rejected.  Every call shares the
+// array, so two calls whose work overlaps on the GPU (for example on two
+// streams of the same device) race on it; serialise such calls.  Each call
+// rebuilds the table and clears the status word before using them, so
+// nothing depends on what the previous call left behind.
 #include <algorithm>
 #include <mutex>
 
