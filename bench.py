@@ -151,11 +151,45 @@ def cpu_baseline(hs, args, budget_s: float):
     return done / el / 1e6, done, threads, el
 
 
+def frame_parity(hs, p, sb, slices: int = 64, per: int = 1024):
+    """Parity of one rendered frame: the oracle (exact build, no FMA
+    contraction) renders `slices` evenly spaced runs of `per` sample indices
+    of the frame with parameters `p`, and they are compared with the GPU's
+    sample buffer `sb` of that frame: relMSE (mean over samples and channels
+    of (x - y)^2 / (y^2 + 1e-2)) and the fraction of bit-identical values."""
+    import oracle
+
+    view = oracle.SceneView(hs)
+    total = p.dimension[0] * p.dimension[1] * p.spp
+    per = min(per, total // slices) if total >= slices else total
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    got, ref = [], []
+    for k in range(slices if total >= slices else 1):
+        first = (k * total) // slices
+        ref.append(oracle.pathtrace(view, p, threads=threads, first=first, count=per))
+        got.append(sb[first * 3:(first + per) * 3].cpu().numpy())
+    el = time.perf_counter() - t0
+    g = np.concatenate(got).astype(np.float64)
+    r = np.concatenate(ref).astype(np.float64)
+    rel = float(np.mean((g - r) ** 2 / (r * r + 1e-2)))
+    exact = float(np.mean(np.concatenate(got).view(np.uint32) == np.concatenate(ref).view(np.uint32)))
+    return {"samples": int(g.size // 3), "relmse": rel, "bit_exact_frac": exact, "frame_number": int(p.frameNumber),
+            "bar": "relMSE <= 1e-4 against the oracle at the same seeds", "oracle_seconds": round(el, 2),
+            "sample": f"{slices} evenly spaced runs of {per} sample indices of the frame"}
+
+
 def run_reference(args):
     """--impl reference: rank 0 times the oracle on the host cores."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    import oracle
+    from strelka_b200 import scenes
+
+    # the scene comes from the CPU-only build of the generators: this arm
+    # never loads the CUDA library
+    scenes.use_generator_library(oracle.workload())
     hs = make_scene(args)
     vals = []
     for step in range(args.warmup + args.steps):
@@ -166,72 +200,102 @@ def run_reference(args):
     n = vals[-1][1]
     cfg = workload_config(args)
     cfg["triangles"] = hs.num_triangles
-    cfg["parallelism"] = "host cores"
     sample = (f"{n} paths per step in 64 evenly spaced slices of the frame's {args.width * args.height * args.spp} "
               f"sample indices, oracle C restatement (-O3 -ffp-contract=fast), OpenMP")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(el for _, _, el in vals),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": cfg,
+        "config": cfg, "parallelism": f"host cores x{threads}",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def run_traversal(args):
-    """--workload traversal: the ray-query microbenchmark (1M-triangle soup,
-    4M rays, closest hit and any hit with tmax uniform in [0.1, 2])."""
+def traversal_study(args, steps: int, warmup: int) -> dict:
+    """The ray-query microbenchmark: the --tris-triangle soup with --rays rays,
+    closest hit (tmax 1e9) and any hit (tmax uniform in [0.1, 2]), each timed
+    over `steps` launches after `warmup` with CUDA events on the launching
+    stream.  Algorithmic bytes per query: 112 B per 4-wide node processed,
+    48 B per triangle test, 32 B ray in, 20 B hit out (counted exactly by an
+    untimed counting replay)."""
     import torch
 
     from strelka_b200 import abi, scenes
     from strelka_b200.render import DeviceScene, PathTracer, to_device
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     hs = scenes.soup(args.tris, 0)
     ds = DeviceScene(hs)
     n = args.rays
     res = {}
     stream = torch.cuda.current_stream()
-    peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    peak, peak_src = hbm_peak()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
     for name, shadow, flags in (("closest", False, abi.TRACE_CLOSEST), ("any", True, abi.TRACE_ANY)):
         rays = to_device(scenes.rays_soup(n, 1 if not shadow else 2, shadow=shadow))
         hits = torch.empty(n * 20, dtype=torch.uint8, device="cuda")
         pt = PathTracer()
         desc = ds.trace_desc(rays, hits, flags)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             pt.trace(desc, stream)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             pt.trace(desc, stream)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
+        ms = e0.elapsed_time(e1) / steps
         cnt = torch.zeros(2, dtype=torch.int64, device="cuda")
         pt.trace(ds.trace_desc(rays, hits, flags | abi.TRACE_COUNT, cnt), stream)
         c = cnt.cpu().numpy()
         out_bytes = 20
         bytes_alg = WIDE_NODE_BYTES * int(c[0]) + 48 * int(c[1]) + (32 + out_bytes) * n
-        res[name] = {"mrays_s": n / (ms * 1e-3) / 1e6, "ms": ms, "nodes_per_ray": c[0] / n,
-                     "tests_per_ray": c[1] / n, "achieved_gbs": bytes_alg / (ms * 1e-3) / 1e9,
-                     "frac": bytes_alg / (ms * 1e-3) / 1e9 / peak}
+        st = pt.device_status()
         pt.close()
-    line = {"metric": "Mrays/s (traversal microbenchmark)", "value": res["closest"]["mrays_s"], "unit": "Mrays/s",
+        if st != 0:
+            raise RuntimeError(f"device status {st:#x}")
+        res[name] = {"mrays_s": n / (ms * 1e-3) / 1e6, "ms_per_launch": ms, "nodes_per_ray": c[0] / n,
+                     "tests_per_ray": c[1] / n, "bytes_alg_per_launch": bytes_alg,
+                     "achieved_gbs": bytes_alg / (ms * 1e-3) / 1e9,
+                     "frac": bytes_alg / (ms * 1e-3) / 1e9 / peak}
+    clk = clocks.stop()
+    return {"workload": f"traversal microbenchmark: {args.tris} soup triangles (centroids uniform in the unit cube, "
+                        f"log-normal vertex offsets mu=ln 0.003 sigma=0.5), {n} rays (origins uniform in "
+                        f"[-0.5,1.5]^3, directions uniform on the sphere), closest hit and any hit",
+            "triangles": hs.num_triangles, "rays": n, "steps": steps, "warmup": warmup, "peak_gbs": peak,
+            "peak_source": peak_src, "target_frac": 0.60, "closest": res["closest"], "any": res["any"],
+            "clocks": clk, "l2": "inputs larger than L2"}
+
+
+def run_traversal(args):
+    """--workload traversal: traversal_study as its own JSON line."""
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    tr = traversal_study(args, args.steps, args.warmup)
+    c = tr["closest"]
+    line = {"metric": "Mrays/s (traversal microbenchmark)", "value": c["mrays_s"], "unit": "Mrays/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"traversal microbenchmark: {args.tris} soup triangles (log-normal size, mu=ln 0.003, "
-                                   f"sigma=0.5), {n} rays, closest + any hit", "l2": "inputs larger than L2"},
-            "roofline": {"bound": "hbm", "achieved": res["closest"]["achieved_gbs"], "peak": peak, "unit": "GB/s",
-                         "frac": res["closest"]["frac"],
-                         "traffic": (TRACE_SOUP_DRAM_BYTES_PER_RAY * n
+            "config": {"workload": tr["workload"], "l2": "inputs larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": c["achieved_gbs"], "peak": tr["peak_gbs"], "unit": "GB/s",
+                         "frac": c["frac"],
+                         "traffic": (TRACE_SOUP_DRAM_BYTES_PER_RAY * tr["rays"]
                                      if (args.tris, args.rays) == (1_000_000, 4_000_000) else None),
                          "traffic_source": "ncu DRAM bytes of one closest-hit launch on the default soup"},
-            "detail": res}
+            "detail": tr, "clocks": tr["clocks"]}
     print(json.dumps(line), flush=True)
+
+
+def hbm_peak():
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        return json.load(open(peaks_path))["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
 
 
 def nrc_mlp_microbench(torch, RadianceCache, lo, hi, log2t, peak_tflops):
@@ -312,28 +376,26 @@ def run_nrc_mlp(args):
     print(json.dumps(line), flush=True)
 
 
-def run_nrc(args):
-    """--workload nrc: wall time of the radiance-cache renderer to reach the
-    relMSE of one plain frame (the large render at --spp samples per pixel),
-    both measured against a --ref-spp reference of the plain renderer.
+def nrc_study(args, hs, ds) -> dict:
+    """Wall time of the radiance-cache renderer to reach the relMSE of one
+    plain frame (the large render at --spp samples per pixel), both measured
+    against a --ref-spp reference of the plain renderer.
 
     The cached renderer starts from an untrained cache; its warm-up of
     --nrc-warmup training batches (training paths and Adam steps, no image)
     counts toward its time, and then it accumulates frames of --nrc-spp
-    samples, training on every frame, until its relMSE reaches the plain
-    frame's.  Every frame
-    is timed with CUDA events on the launching stream; relMSE is computed
-    between frames, outside the timed intervals."""
+    samples, training on every frame.  A trial reaches the target when its
+    running relMSE is at or below the plain relMSE on two consecutive
+    frames; its time runs to the end of the second of them.  Each trial also
+    reports its relMSE at equal time: after the last frame that ends within
+    the plain frame's wall time.  Every frame is timed with CUDA events on
+    the launching stream; relMSE is computed between frames, outside the
+    timed intervals."""
     import torch
 
     from strelka_b200 import abi
-    from strelka_b200.render import DeviceScene, PathTracer, RadianceCache
+    from strelka_b200.render import PathTracer, RadianceCache
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    if int(os.environ.get("RANK", "0")) != 0:
-        return
-    hs = make_scene(args)
-    ds = DeviceScene(hs)
     W, H, S = args.width, args.height, args.spp
     npx = W * H
     stream = torch.cuda.current_stream()
@@ -369,11 +431,11 @@ def run_nrc(args):
     def relmse(acc, n):
         return float((((acc / n) - ref) ** 2 / den).mean())
 
-    # plain: one frame of S spp, a few independent frames
+    # plain: frames of S spp, each compared with the reference on its own
     for k in range(3):
         render(plain, 10 + k, S)
     plain_ms, plain_err = [], []
-    for k in range(max(args.steps, 8)):
+    for k in range(max(args.nrc_plain_frames, 8)):
         acc = torch.zeros(npx, 3, dtype=torch.float64, device="cuda")
         plain_ms.append(timed(plain, 2000 + k, S, acc))
         plain_err.append(relmse(acc, S))
@@ -420,6 +482,8 @@ def run_nrc(args):
         acc = torch.zeros(npx, 3, dtype=torch.float64, device="cuda")
         curve = []
         reached = None
+        below = 0
+        at_equal_time = None
         frames_ms = []
         for k in range(args.nrc_max_frames):
             ms = timed(pt, base + 50_000 + k, args.nrc_spp, acc)
@@ -427,7 +491,10 @@ def run_nrc(args):
             t_nrc += ms
             e = relmse(acc, (k + 1) * args.nrc_spp)
             curve.append([(k + 1) * args.nrc_spp, round(e, 6), round(t_nrc, 3)])
-            if e <= target:
+            if t_nrc <= t_plain:
+                at_equal_time = e
+            below = below + 1 if e <= target else 0
+            if below >= 2:
                 reached = (k + 1) * args.nrc_spp
                 break
         times = pt.kernel_times(stream)
@@ -438,35 +505,63 @@ def run_nrc(args):
         cache.close()
         trials.append({"reached_at_spp": reached, "ratio": (t_nrc / t_plain) if reached else None, "ms_total": t_nrc,
                        "ms_warmup": t_warm, "ms_per_frame": statistics.median(frames_ms),
+                       "relmse_at_plain_time": at_equal_time,
+                       "relmse_ratio_at_plain_time": (at_equal_time / target) if at_equal_time is not None else None,
                        "curve_spp_relmse_ms": curve})
     clk = clocks.stop()
     pt.close()
     scratch_cache.close()
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peak_tf = json.load(open(peaks_path)).get("bf16_tflops_sustained", 1400.0) if os.path.exists(peaks_path) else 1400.0
-    mlp = nrc_mlp_microbench(torch, RadianceCache, lo, hi, args.nrc_log2t, peak_tf)
     if st != 0:
         raise RuntimeError(f"device status {st:#x}")
     ratios = sorted(t["ratio"] if t["ratio"] is not None else float("inf") for t in trials)
     median_ratio = ratios[len(ratios) // 2]
-    line = {
+    eq = sorted(t["relmse_ratio_at_plain_time"] if t["relmse_ratio_at_plain_time"] is not None else float("inf")
+                for t in trials)
+    return {
         "metric": "radiance-cache wall time to the plain 16-spp relMSE, relative to plain",
-        "value": median_ratio if median_ratio != float("inf") else None, "unit": "x plain wall time", "n_gpus": 1,
-        "steps": args.steps, "warmup": 3, "ms_per_step": t_plain, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 render, f16 network (f32 accumulation)", "data": "synthetic",
+        "median_ratio": median_ratio if median_ratio != float("inf") else None, "unit": "x plain wall time",
+        "target": 0.5, "trials_reached": sum(t["ratio"] is not None for t in trials),
+        "median_relmse_ratio_at_plain_time": eq[len(eq) // 2] if eq[len(eq) // 2] != float("inf") else None,
+        "rule": "reached when the running relMSE is at or below the plain relMSE on two consecutive frames; "
+                "time to the end of the second",
         "config": {"workload": f"radiance cache on the large render ({W}x{H}, depth {args.depth}, "
                                f"{args.instances} instances)",
                    "reference_spp": ref_frames * 16, "plain_spp": S, "plain_frames": len(plain_err),
                    "nrc_trials": len(trials), "nrc_spp_per_frame": args.nrc_spp,
-                   "nrc_warmup_batches": args.nrc_warmup, "nrc_warmup_batches_per_launch": args.nrc_warmup_group, "train_paths_per_frame": args.nrc_train_paths,
+                   "nrc_warmup_batches": args.nrc_warmup, "nrc_warmup_batches_per_launch": args.nrc_warmup_group,
+                   "train_paths_per_frame": args.nrc_train_paths,
                    "train_steps_per_frame": args.nrc_train_steps, "log2_table_size": args.nrc_log2t,
                    "diffuse_roughness": args.nrc_diffuse_roughness, "learning_rate": args.nrc_lr,
                    "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)"},
         "plain": {"relmse": target, "relmse_frames": plain_err, "ms": t_plain},
-        "nrc": {"median_ratio": median_ratio, "trials": trials, "kernel_ms_per_frame_first_trial": kernel_ms},
-        "reference_seconds": ref_s,
-        "clocks": clk,
-        "mlp_microbench": mlp,
+        "trials": trials, "kernel_ms_per_frame_first_trial": kernel_ms,
+        "reference_seconds": ref_s, "clocks": clk,
+    }
+
+
+def run_nrc(args):
+    """--workload nrc: nrc_study as its own JSON line, with the cache's
+    fused-kernel microbenchmark."""
+    import torch
+
+    from strelka_b200.render import DeviceScene, RadianceCache
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    hs = make_scene(args)
+    ds = DeviceScene(hs)
+    res = nrc_study(args, hs, ds)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak_tf = json.load(open(peaks_path)).get("bf16_tflops_sustained", 1400.0) if os.path.exists(peaks_path) else 1400.0
+    lo, hi = hs.bounds()
+    mlp = nrc_mlp_microbench(torch, RadianceCache, lo, hi, args.nrc_log2t, peak_tf)
+    line = {
+        "metric": res["metric"], "value": res["median_ratio"], "unit": res["unit"], "n_gpus": 1,
+        "steps": len(res["plain"]["relmse_frames"]), "warmup": 3, "ms_per_step": res["plain"]["ms"],
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 render, f16 network (f32 accumulation)", "data": "synthetic", "config": res["config"],
+        "plain": res["plain"], "nrc": res, "clocks": res["clocks"], "mlp_microbench": mlp,
     }
     print(json.dumps(line), flush=True)
 
@@ -626,6 +721,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-step-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--no-studies", action="store_true",
+                    help="skip the traversal microbenchmark and the radiance-cache study in the default run")
     ap.add_argument("--workload", default="large", choices=["large", "traversal", "nrc", "nrc-mlp", "batch"])
     ap.add_argument("--batch-jobs", type=int, default=32)
     ap.add_argument("--batch-scenes", type=int, default=6)
@@ -638,6 +736,7 @@ def main():
     ap.add_argument("--nrc-warmup", type=int, default=16)
     ap.add_argument("--nrc-warmup-group", type=int, default=8)
     ap.add_argument("--nrc-max-frames", type=int, default=64)
+    ap.add_argument("--nrc-plain-frames", type=int, default=10)
     ap.add_argument("--nrc-train-paths", type=int, default=16384)
     ap.add_argument("--nrc-train-steps", type=int, default=1)
     ap.add_argument("--nrc-trials", type=int, default=5)
@@ -754,6 +853,9 @@ def main():
     else:
         peak, peak_src = 6650.0, "fallback"
     achieved = bytes_alg / (ext_ms * 1e-3) / 1e9 if ext_ms > 0 else None
+    sh_ms, sh_launches = times["shadow"]
+    sh_bytes = WIDE_NODE_BYTES * cnt["shadow_inner"] + 48 * cnt["shadow_leaf"] + 64 * cnt["shadow_rays"]
+    sh_achieved = sh_bytes / (sh_ms * 1e-3) / 1e9 if sh_ms > 0 else None
 
     # ---- end to end through the C ABI: host param in, tonemapped RGBA8 out ---
     host_img = torch.empty(W * H * 4, dtype=torch.uint8, pin_memory=True)
@@ -777,12 +879,30 @@ def main():
     if st != 0:
         raise RuntimeError(f"device status {st:#x}")
 
+    # ---- parity of the first timed frame against the oracle -------------------
+    parity = None
+    if rank == 0 and world == 1 and not args.no_parity:
+        p_first = hs.param(frameNumber=multigpu.frame_number(rank, args.warmup), iteration=args.warmup)
+        pt.execute(ds.desc(p_first, sb), total, 1, args.warmup, stream)
+        torch.cuda.synchronize()
+        parity = frame_parity(hs, p_first, sb)
+        st = pt.device_status()
+        if st != 0:
+            raise RuntimeError(f"device status {st:#x}")
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, n, threads, el = cpu_baseline(hs, args, budget_s=args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{n} paths of the frame ({n / total * 100:.3f}%), 64 evenly spaced slices of the sample "
                          f"indices, {el:.1f} s, oracle C restatement -O3 -ffp-contract=fast, OpenMP"}
+
+    # ---- the rest of the metric, one GPU: the traversal microbenchmark and
+    # the radiance-cache time-to-equal-relMSE study ---------------------------
+    trav = nrc_res = None
+    if rank == 0 and world == 1 and not args.no_studies:
+        trav = traversal_study(args, steps=10, warmup=3)
+        nrc_res = nrc_study(args, hs, ds)
 
     if dist:
         dist.barrier()
@@ -791,12 +911,13 @@ def main():
         return
     cfg = workload_config(args)
     cfg["triangles"] = hs.num_triangles
-    cfg["parallelism"] = f"replicas x{world} (independent frames per GPU)" if world > 1 else "single GPU"
     param_bytes = 336 + 416 + 16
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural scene, see config.workload)", "config": cfg,
+        "parallelism": f"replicas x{world} (independent frames per GPU)" if world > 1 else "single GPU",
+        "parity": parity,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": EXTEND_DRAM_BYTES_PER_RAY * cnt["extend_rays"] / max(ext_launches, 1)
@@ -806,8 +927,18 @@ def main():
                      "kernel": "extend (closest-hit traversal)", "peak_source": peak_src,
                      "bytes_alg_timed_region": bytes_alg, "kernel_ms_timed_region": ext_ms,
                      "kernel_launches_timed_region": ext_launches, "visits": cnt},
+        "roofline_shadow": {"bound": "hbm", "kernel": "shadow (any-hit traversal)",
+                            "achieved": sh_achieved, "peak": peak, "unit": "GB/s",
+                            "frac": (sh_achieved / peak) if sh_achieved else None,
+                            "bytes_alg_per_launch": sh_bytes / max(sh_launches, 1),
+                            "kernel_ms_timed_region": sh_ms, "kernel_launches_timed_region": sh_launches,
+                            "note": "112 B per 4-wide node + 48 B per triangle test + 64 B request per query; "
+                                    "the kernel runs on the second stream beside the next bounce's extend, so its "
+                                    "duration includes SM time shared with that kernel"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": param_bytes, "d2h_bytes_per_step": W * H * 4},
+        "traversal": trav,
+        "nrc": nrc_res,
         "gpu_launches": launches,
         "clocks": clk,
         "kernel_ms_per_frame": {k: v[0] / args.steps for k, v in times.items() if v[1]},
@@ -816,6 +947,8 @@ def main():
                           "classes sum to more than ms_per_step",
     }
     print(json.dumps(line), flush=True)
+    if parity is not None and not parity["relmse"] <= 1e-4:
+        raise SystemExit(f"parity failed: relMSE {parity['relmse']} against the oracle exceeds 1e-4")
 
 
 if __name__ == "__main__":

@@ -21,6 +21,7 @@ import numpy as np
 _DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_DIR, "liboracle.so")
 FAST_LIB_PATH = os.path.join(_DIR, "liboracle_fast.so")
+WORKLOAD_LIB_PATH = os.path.join(_DIR, "libworkload.so")
 
 _libs: dict[str, C.CDLL] = {}
 
@@ -78,6 +79,7 @@ def load(fast: bool = False) -> C.CDLL:
         "oracle_ray_triangle": (C.c_int, [vp, vp, vp, vp, vp, C.POINTER(f32), C.POINTER(f32), C.POINTER(f32)]),
         "oracle_trace": (C.c_int, [C.POINTER(OracleScene), vp, u32, vp, vp, C.c_int, C.c_int, vp, C.c_int]),
         "oracle_intersect_fp64": (C.c_int, [C.POINTER(OracleScene), vp, vp, vp, u32, vp, vp, vp]),
+        "oracle_intersect_terms_fp64": (C.c_int, [C.POINTER(OracleScene), vp, vp, vp, u32, vp]),
         "oracle_pathtrace": (C.c_int, [vp, C.POINTER(OracleScene), vp, C.c_int]),
         "oracle_pathtrace_range": (C.c_int, [vp, C.POINTER(OracleScene), vp, C.c_uint64, C.c_uint64, C.c_int]),
         "oracle_reduce": (C.c_int, [vp, vp, vp]),
@@ -92,6 +94,20 @@ def load(fast: bool = False) -> C.CDLL:
         fn.restype = res
         fn.argtypes = args
     _libs[path] = lib
+    return lib
+
+
+def workload() -> C.CDLL:
+    """The CPU-only build of the package's seeded scene generators and host
+    SAH builder (oracle/libworkload.so), for processes that build workloads
+    without loading the CUDA library: pass it to
+    strelka_b200.scenes.use_generator_library."""
+    if WORKLOAD_LIB_PATH in _libs:
+        return _libs[WORKLOAD_LIB_PATH]
+    if not os.path.exists(WORKLOAD_LIB_PATH):
+        build()
+    lib = C.CDLL(WORKLOAD_LIB_PATH)
+    _libs[WORKLOAD_LIB_PATH] = lib
     return lib
 
 
@@ -149,6 +165,17 @@ def intersect_fp64(view: SceneView, rays: np.ndarray, inst: np.ndarray, prim: np
     v = np.zeros(n, np.float64)
     lib.oracle_intersect_fp64(C.byref(view.scene), _ptr(rays), _ptr(inst), _ptr(prim), n, _ptr(t), _ptr(u), _ptr(v))
     return t, u, v
+
+
+def intersect_terms_fp64(view: SceneView, rays: np.ndarray, inst: np.ndarray, prim: np.ndarray) -> np.ndarray:
+    """(n, 3) conditioning scales of u, v, t (oracle_intersect_terms_fp64)."""
+    lib = load()
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = rays.shape[0]
+    out = np.zeros((n, 3), np.float64)
+    lib.oracle_intersect_terms_fp64(C.byref(view.scene), _ptr(rays), _ptr(np.ascontiguousarray(inst, np.uint32)),
+                                    _ptr(np.ascontiguousarray(prim, np.uint32)), n, _ptr(out))
+    return out
 
 
 def pathtrace(view: SceneView, param, threads: int = 0, first: int = 0, count: int | None = None,

@@ -858,6 +858,58 @@ int oracle_intersect_fp64(const OracleScene* s, const Ray* rays, const uint32_t*
     return 0;
 }
 
+/* Conditioning of the same formula: for each ray, the magnitude scale of
+ * u, v and t, (sum of |terms| of the numerator + |value| x sum of |terms| of
+ * det) / |det|, where the terms are the products the triple products
+ * expand into.  A rounding error of relative size e in each product shifts
+ * the value by at most about e x scale, so scale x 2^-52 bounds what FP64
+ * itself resolves and scale x 2^-44 what a double-float evaluation does. */
+int oracle_intersect_terms_fp64(const OracleScene* s, const Ray* rays, const uint32_t* instIds, const uint32_t* primIds,
+                                uint32_t n, double* scale3)
+{
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        scale3[3 * i + 0] = NAN; scale3[3 * i + 1] = NAN; scale3[3 * i + 2] = NAN;
+        uint32_t inst = instIds[i], prim = primIds[i];
+        if (inst >= s->numInstances) continue;
+        const InstanceConstants* ic = &s->instances[inst];
+        uint32_t base = (uint32_t)ic->indexOffset + prim * 3u;
+        if ((uint64_t)base + 2 >= s->numIndices) continue;
+        double P[3][3];
+        for (int k = 0; k < 3; ++k) {
+            const float* p = s->vb[s->ib[base + k]].position;
+            const float* m = ic->objectToWorld.m;
+            for (int a = 0; a < 3; ++a)
+                P[k][a] = (double)m[0 * 4 + a] * p[0] + (double)m[1 * 4 + a] * p[1] + (double)m[2 * 4 + a] * p[2] +
+                          (double)m[3 * 4 + a];
+        }
+        double o[3] = {rays[i].o.x, rays[i].o.y, rays[i].o.z}, d[3] = {rays[i].d.x, rays[i].d.y, rays[i].d.z};
+        double e0[3], e1[3], tv[3];
+        for (int a = 0; a < 3; ++a) { e0[a] = P[1][a] - P[0][a]; e1[a] = P[2][a] - P[0][a]; tv[a] = o[a] - P[0][a]; }
+        double pv[3] = {d[1] * e1[2] - d[2] * e1[1], d[2] * e1[0] - d[0] * e1[2], d[0] * e1[1] - d[1] * e1[0]};
+        double qv[3] = {tv[1] * e0[2] - tv[2] * e0[1], tv[2] * e0[0] - tv[0] * e0[2], tv[0] * e0[1] - tv[1] * e0[0]};
+        double apv[3] = {fabs(d[1] * e1[2]) + fabs(d[2] * e1[1]), fabs(d[2] * e1[0]) + fabs(d[0] * e1[2]),
+                         fabs(d[0] * e1[1]) + fabs(d[1] * e1[0])};
+        double aqv[3] = {fabs(tv[1] * e0[2]) + fabs(tv[2] * e0[1]), fabs(tv[2] * e0[0]) + fabs(tv[0] * e0[2]),
+                         fabs(tv[0] * e0[1]) + fabs(tv[1] * e0[0])};
+        double det = e0[0] * pv[0] + e0[1] * pv[1] + e0[2] * pv[2];
+        double nDet = fabs(e0[0]) * apv[0] + fabs(e0[1]) * apv[1] + fabs(e0[2]) * apv[2];
+        double nU = fabs(tv[0]) * apv[0] + fabs(tv[1]) * apv[1] + fabs(tv[2]) * apv[2];
+        double nV = fabs(d[0]) * aqv[0] + fabs(d[1]) * aqv[1] + fabs(d[2]) * aqv[2];
+        double nT = fabs(e1[0]) * aqv[0] + fabs(e1[1]) * aqv[1] + fabs(e1[2]) * aqv[2];
+        double u = (tv[0] * pv[0] + tv[1] * pv[1] + tv[2] * pv[2]) / det;
+        double v = (d[0] * qv[0] + d[1] * qv[1] + d[2] * qv[2]) / det;
+        double t = (e1[0] * qv[0] + e1[1] * qv[1] + e1[2] * qv[2]) / det;
+        double ad = fabs(det);
+        scale3[3 * i + 0] = (nU + fabs(u) * nDet) / ad;
+        scale3[3 * i + 1] = (nV + fabs(v) * nDet) / ad;
+        scale3[3 * i + 2] = (nT + fabs(t) * nDet) / ad;
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------------------------- */
 /* lights.h */
 typedef struct {

@@ -96,6 +96,11 @@ int oracle_trace(const OracleScene* s, const Ray* rays, uint32_t n, Hit* hits, u
 int oracle_intersect_fp64(const OracleScene* s, const Ray* rays, const uint32_t* instIds,
                           const uint32_t* primIds, uint32_t n, double* t, double* u, double* v);
 
+/* Per ray, the conditioning scale of u, v and t in that formula (see
+ * oracle.c): scale x 2^-52 bounds FP64's own error. */
+int oracle_intersect_terms_fp64(const OracleScene* s, const Ray* rays, const uint32_t* instIds,
+                                const uint32_t* primIds, uint32_t n, double* scale3);
+
 /* pathtracerMdl.hlsl:406-423 computeMain over idx in [0, W*H*spp):
  * writes sampleBuffer[(idx)*3 + c]. */
 int oracle_pathtrace(const PathTracerParam* p, const OracleScene* s, float* sampleBuffer,

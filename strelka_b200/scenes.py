@@ -14,6 +14,38 @@ import numpy as np
 
 from . import abi
 
+# The library the generators are called from: the package's own by default.
+# A CPU-only build of the same generator sources can stand in for it
+# (use_generator_library), so that a process can build scenes without
+# loading the CUDA library.
+_gen_lib: C.CDLL | None = None
+
+
+def use_generator_library(lib: C.CDLL | None) -> None:
+    """Calls the scene generators through `lib` (a library exporting the
+    strelka_scene_* / strelka_rays_soup / strelka_camera_lookat /
+    strelka_bvh_build entry points of include/strelka_b200_scenes.h), or
+    through the package's library again when `lib` is None."""
+    global _gen_lib
+    if lib is not None:
+        for name, (res, args) in abi.SIGNATURES.items():
+            fn = getattr(lib, name, None)
+            if fn is not None:
+                fn.restype = res
+                fn.argtypes = args
+    _gen_lib = lib
+
+
+def _lib() -> C.CDLL:
+    return _gen_lib if _gen_lib is not None else abi.load()
+
+
+def _check(lib: C.CDLL, rc: int) -> None:
+    if rc != abi.OK:
+        buf = C.create_string_buffer(1024)
+        lib.strelka_get_last_error(buf, len(buf))
+        raise abi.StrelkaError(rc, buf.value.decode(errors="replace"))
+
 
 def _np(ptr, count: int, ctype) -> np.ndarray:
     """Copies `count` elements of a ctypes array pointer into a uint8 numpy array."""
@@ -74,7 +106,8 @@ class HostScene:
         p = self.param(**kw)
         e = (C.c_float * 3)(*[float(v) for v in eye])
         t = (C.c_float * 3)(*[float(v) for v in target])
-        abi.check(abi.load().strelka_camera_lookat(C.byref(p), width, height, e, t, fov_deg))
+        lib = _lib()
+        _check(lib, lib.strelka_camera_lookat(C.byref(p), width, height, e, t, fov_deg))
         return p
 
     def param(self, **kw) -> abi.PathTracerParam:
@@ -87,7 +120,7 @@ class HostScene:
 
 
 def _from_c(hs: abi.StrelkaHostScene) -> HostScene:
-    lib = abi.load()
+    lib = _lib()
     try:
         textures = []
         for i in range(hs.numTextures):
@@ -123,43 +156,43 @@ def _from_c(hs: abi.StrelkaHostScene) -> HostScene:
 
 def cornell(width: int = 512, height: int = 512, sphere_levels: int = 4, light_side: float = 0.25,
             light_radiance: float = 15.0, max_depth: int = 4, spp: int = 1) -> HostScene:
-    lib = abi.load()
+    lib = _lib()
     cfg = abi.StrelkaCornellConfig(width, height, sphere_levels, light_side, light_radiance, max_depth, spp, 1, 0)
     hs = abi.StrelkaHostScene()
-    abi.check(lib.strelka_scene_cornell(C.byref(cfg), C.byref(hs)))
+    _check(lib, lib.strelka_scene_cornell(C.byref(cfg), C.byref(hs)))
     return _from_c(hs)
 
 
 def soup(num_tris: int, seed: int = 0) -> HostScene:
-    lib = abi.load()
+    lib = _lib()
     hs = abi.StrelkaHostScene()
-    abi.check(lib.strelka_scene_soup(num_tris, seed, C.byref(hs)))
+    _check(lib, lib.strelka_scene_soup(num_tris, seed, C.byref(hs)))
     return _from_c(hs)
 
 
 def large(width: int = 1920, height: int = 1080, instances: int = 64, frequency: int = 89, num_textures: int = 8,
           tex_size: int = 2048, env_width: int = 1024, env_height: int = 512, max_depth: int = 8, spp: int = 16,
           seed: int = 0) -> HostScene:
-    lib = abi.load()
+    lib = _lib()
     cfg = abi.StrelkaLargeConfig(width, height, instances, frequency, num_textures, tex_size, env_width, env_height,
                                  max_depth, spp, seed)
     hs = abi.StrelkaHostScene()
-    abi.check(lib.strelka_scene_large(C.byref(cfg), C.byref(hs)))
+    _check(lib, lib.strelka_scene_large(C.byref(cfg), C.byref(hs)))
     return _from_c(hs)
 
 
 def rays_soup(n: int, seed: int = 1, shadow: bool = False) -> np.ndarray:
     """(n, 8) float32 rays: origin xyz, tmax, direction xyz, 0."""
-    lib = abi.load()
+    lib = _lib()
     out = np.zeros((n, 8), np.float32)
-    abi.check(lib.strelka_rays_soup(n, seed, 1 if shadow else 0, out.ctypes.data_as(C.c_void_p)))
+    _check(lib, lib.strelka_rays_soup(n, seed, 1 if shadow else 0, out.ctypes.data_as(C.c_void_p)))
     return out
 
 
 def bvh_build(positions: np.ndarray, inst_ids: np.ndarray, prim_ids: np.ndarray) -> np.ndarray:
     """SAH BVH over world-space triangle corners (positions (3N, 3) float32);
     returns the flattened nodes as uint8 (numNodes * 32)."""
-    lib = abi.load()
+    lib = _lib()
     n = positions.shape[0]
     arr = (abi.BVHInputPosition * max(n, 1))()
     raw = np.frombuffer(arr, dtype=np.uint8).reshape(max(n, 1), 20)
@@ -169,7 +202,7 @@ def bvh_build(positions: np.ndarray, inst_ids: np.ndarray, prim_ids: np.ndarray)
         raw[:n, 16:20] = np.ascontiguousarray(prim_ids, np.uint32).view(np.uint8).reshape(n, 4)
     out = C.POINTER(abi.BVHNode)()
     cnt = C.c_uint32(0)
-    abi.check(lib.strelka_bvh_build(arr, n, C.byref(out), C.byref(cnt)))
+    _check(lib, lib.strelka_bvh_build(arr, n, C.byref(out), C.byref(cnt)))
     if cnt.value == 0:
         return np.zeros(0, np.uint8)
     nodes = _np(out, cnt.value, abi.BVHNode)
