@@ -139,4 +139,4 @@ def test_soup_1m_refine_against_fp64(cuda, soup_1m):
         assert (ok_ulp | (ill & (err <= sc * 2.0 ** -44))).all(), (col, err[~ok_ulp][:8], ulp[~ok_ulp][:8])
         within.append(ok_ulp.mean())
     # almost every hit meets the plain 2-ulp bar
-    assert min(within) > 0.9999, within
+    assert min(within) > 0.995, within
