@@ -27,7 +27,10 @@ _libs: dict[str, C.CDLL] = {}
 
 
 def build() -> None:
+    """Builds the oracle's libraries, and oracle/_ref from the reference's
+    own shader sources when the reference tree is present."""
     subprocess.run(["sh", os.path.join(_DIR, "build.sh")], check=True)
+    subprocess.run(["sh", os.path.join(_DIR, "build_ref.sh")], check=True)
 
 
 class OracleTexture(C.Structure):
@@ -88,6 +91,8 @@ def load(fast: bool = False) -> C.CDLL:
         "oracle_upscale": (C.c_int, [vp, vp, C.c_uint32, C.c_uint32, vp]),
         "oracle_mdl_read": (None, [vp, C.c_uint64, vp, vp, C.c_uint32, vp]),
         "oracle_tex_lookup": (None, [vp, f32, f32, vp]),
+        "oracle_sample_light": (None, [vp, vp, f32, f32, vp]),
+        "oracle_camera_ray": (None, [vp, u32, u32, C.POINTER(u32), u32, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

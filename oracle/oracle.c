@@ -18,6 +18,7 @@
  *  - sin/cos/acos are the project's own polynomial versions below.
  */
 #include "oracle.h"
+#include "own_math.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -99,69 +100,10 @@ static inline v3 mat_mul_dir3(const StrelkaFloat4x4* M, v3 v)
 }
 
 /* ------------------------------------------------------------------------- */
-/* Own sin/cos/acos.  sin/cos: Cody–Waite reduction by pi/2 (three-part split
- * of pi/2, FMA steps) and the Taylor polynomials of sin (to r^11) and cos (to
- * r^12) on |r| <= pi/4.  acos: the arcsine Maclaurin series to x^23 on
- * |x| <= 1/2 and acos(x) = 2 asin(sqrt((1-x)/2)) outside. */
-static const float PIO2_1 = 0x1.921fb6p+0f;
-static const float PIO2_2 = -0x1.777a5cp-25f;
-static const float PIO2_3 = -0x1.ee59dap-50f;
-static const float TWO_OVER_PI = 0x1.45f306p-1f;
-static const float PI_HI = 0x1.921fb6p+1f;
-static const float PI_LO = -0x1.777a5cp-24f;
-
-static void own_sincos(float x, float* s, float* c)
-{
-    if (!(fabsf(x) <= 1.0e30f)) { *s = NAN; *c = NAN; return; }
-    float k = rintf(x * TWO_OVER_PI);
-    float r = fmaf(-k, PIO2_1, x);
-    r = fmaf(-k, PIO2_2, r);
-    r = fmaf(-k, PIO2_3, r);
-    float r2 = r * r;
-    float ps = fmaf(r2, -2.5052108385441720e-8f, 2.7557319223985893e-6f);
-    ps = fmaf(r2, ps, -1.9841269841269841e-4f);
-    ps = fmaf(r2, ps, 8.3333333333333333e-3f);
-    ps = fmaf(r2, ps, -1.6666666666666667e-1f);
-    float sr = fmaf(r * r2, ps, r);
-    float pc = fmaf(r2, 2.0876756987868099e-9f, -2.7557319223985891e-7f);
-    pc = fmaf(r2, pc, 2.4801587301587302e-5f);
-    pc = fmaf(r2, pc, -1.3888888888888889e-3f);
-    pc = fmaf(r2, pc, 4.1666666666666667e-2f);
-    pc = fmaf(r2, pc, -0.5f);
-    float cr = fmaf(r2, pc, 1.0f);
-    int q = (int)(k - 4.0f * floorf(k * 0.25f));
-    switch (q) {
-    case 0: *s = sr; *c = cr; break;
-    case 1: *s = cr; *c = -sr; break;
-    case 2: *s = -sr; *c = -cr; break;
-    default: *s = -cr; *c = sr; break;
-    }
-}
-float oracle_sinf(float x) { float s, c; own_sincos(x, &s, &c); return s; }
-float oracle_cosf(float x) { float s, c; own_sincos(x, &s, &c); return c; }
-
-static float own_asin_small(float x) /* |x| <= 0.5 */
-{
-    float z = x * x;
-    float p = fmaf(z, 6.4472103118896484e-3f, 7.3125258735988454e-3f);
-    p = fmaf(z, p, 8.3903358096168155e-3f);
-    p = fmaf(z, p, 9.7616095291940789e-3f);
-    p = fmaf(z, p, 1.1551800896139705e-2f);
-    p = fmaf(z, p, 1.3964843750000000e-2f);
-    p = fmaf(z, p, 1.7352764423076924e-2f);
-    p = fmaf(z, p, 2.2372159090909092e-2f);
-    p = fmaf(z, p, 3.0381944444444444e-2f);
-    p = fmaf(z, p, 4.4642857142857144e-2f);
-    p = fmaf(z, p, 7.5000000000000000e-2f);
-    p = fmaf(z, p, 1.6666666666666667e-1f);
-    return fmaf(x * z, p, x);
-}
-float oracle_acosf(float x)
-{
-    if (fabsf(x) <= 0.5f) return PIO2_1 - (own_asin_small(x) - PIO2_2);
-    if (x > 0.5f) return 2.0f * own_asin_small(sqrtf((1.0f - x) * 0.5f));
-    return PI_HI - (2.0f * own_asin_small(sqrtf((1.0f + x) * 0.5f)) - PI_LO);
-}
+/* Own sin/cos/acos (own_math.h), exported for the tests. */
+float oracle_sinf(float x) { return own_sinf(x); }
+float oracle_cosf(float x) { return own_cosf(x); }
+float oracle_acosf(float x) { return own_acosf(x); }
 #define SINF oracle_sinf
 #define COSF oracle_cosf
 #define ACOSF oracle_acosf
@@ -1126,6 +1068,16 @@ static LightSample sample_light(const UniformLight* l, v3 hitPoint, float ux, fl
     return ls;
 }
 
+/* lights.h:284-340 for one light, exported for function-level checks:
+ * out = {pointOnLight[3], pdf, normal[3], area, L[3], distToLight}. */
+void oracle_sample_light(const UniformLight* l, const float hitPoint[3], float u0, float u1, float out[12])
+{
+    LightSample ls = sample_light(l, V(hitPoint[0], hitPoint[1], hitPoint[2]), u0, u1);
+    out[0] = ls.pointOnLight.x; out[1] = ls.pointOnLight.y; out[2] = ls.pointOnLight.z; out[3] = ls.pdf;
+    out[4] = ls.normal.x; out[5] = ls.normal.y; out[6] = ls.normal.z; out[7] = ls.area;
+    out[8] = ls.L.x; out[9] = ls.L.y; out[10] = ls.L.z; out[11] = ls.distToLight;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Native materials (project-defined argument record StrelkaMaterialArgs). */
 typedef struct {
@@ -1194,21 +1146,20 @@ void oracle_tex_lookup(const OracleTexture* t, float u, float v, float out[4])
     }
 }
 
-static int load_material(const OracleScene* s, int32_t materialId, const ShadeState* st, Mat* m)
+/* The native material at argument-block offset argOffset with function id
+ * fn, its base colour textured at the shading state's (u, v). */
+static int load_material_args(const OracleScene* s, int32_t argOffset, int32_t fn, const ShadeState* st, Mat* m)
 {
-    if (materialId < 0 || (uint32_t)materialId >= s->numMaterials) return 0;
-    const MdlMaterial* mm = &s->materials[materialId];
-    if (mm->arg_block_offset < 0 || (uint64_t)mm->arg_block_offset + sizeof(StrelkaMaterialArgs) > s->argBlockBytes)
-        return 0;
-    if (mm->functionId < 0 || mm->functionId >= STRELKA_FN_COUNT) return 0;
+    if (argOffset < 0 || (uint64_t)argOffset + sizeof(StrelkaMaterialArgs) > s->argBlockBytes) return 0;
+    if (fn < 0 || fn >= STRELKA_FN_COUNT) return 0;
     StrelkaMaterialArgs a;
-    memcpy(&a, s->argBlock + mm->arg_block_offset, sizeof(a));
+    memcpy(&a, s->argBlock + argOffset, sizeof(a));
     m->base = V(a.base_color[0], a.base_color[1], a.base_color[2]);
     m->roughness = a.roughness;
     m->emission = V(a.emission[0], a.emission[1], a.emission[2]);
     m->ior = a.ior;
     m->tex = a.base_color_texture;
-    m->fn = mm->functionId;
+    m->fn = fn;
     if (m->tex != 0) {
         if (m->tex - 1 >= s->numResourceInfos) return 0;
         uint32_t slot = s->resourceInfos[m->tex - 1].gpu_resource_array_start;
@@ -1218,6 +1169,12 @@ static int load_material(const OracleScene* s, int32_t materialId, const ShadeSt
         m->base = V(m->base.x * texel[0], m->base.y * texel[1], m->base.z * texel[2]);
     }
     return 1;
+}
+static int load_material(const OracleScene* s, int32_t materialId, const ShadeState* st, Mat* m)
+{
+    if (materialId < 0 || (uint32_t)materialId >= s->numMaterials) return 0;
+    const MdlMaterial* mm = &s->materials[materialId];
+    return load_material_args(s, mm->arg_block_offset, mm->functionId, st, m);
 }
 
 /* GGX helpers (Walter et al. 2007) */
@@ -1363,6 +1320,58 @@ static SampleOut bsdf_sample(const Mat* m, const ShadeState* st, v3 k1, const fl
     so.pdf = (1.0f - F) * D * noh;
     so.event = EV_GLOSSY | EV_TRANSMISSION;
     return so;
+}
+
+/* Exported native materials: the functions the MDL-generated dispatchers
+ * (mdl_bsdf_scattering_sample / _evaluate, mdl_edf_emission_intensity,
+ * src/materialmanager/mdlHlslCodeGen.cpp:32-81) stand for in this project.
+ * state = {normal[3], geom_normal[3], position[3], u, v}. */
+static void state_from(const float* st9uv, ShadeState* st)
+{
+    st->normal = V(st9uv[0], st9uv[1], st9uv[2]);
+    st->geom_normal = V(st9uv[3], st9uv[4], st9uv[5]);
+    st->position = V(st9uv[6], st9uv[7], st9uv[8]);
+    st->u = st9uv[9];
+    st->v = st9uv[10];
+}
+int oracle_material_sample(const OracleScene* s, int32_t argOffset, int32_t fn, const float* state, const float k1[3],
+                           const float xi[4], float ior1, float ior2, float k2[3], float bsdfOverPdf[3], float* pdf,
+                           int* event)
+{
+    ShadeState st;
+    Mat m;
+    state_from(state, &st);
+    if (!load_material_args(s, argOffset, fn, &st, &m)) return 0;
+    SampleOut so = bsdf_sample(&m, &st, V(k1[0], k1[1], k1[2]), xi, ior1, ior2);
+    k2[0] = so.k2.x; k2[1] = so.k2.y; k2[2] = so.k2.z;
+    bsdfOverPdf[0] = so.bsdf_over_pdf.x; bsdfOverPdf[1] = so.bsdf_over_pdf.y; bsdfOverPdf[2] = so.bsdf_over_pdf.z;
+    *pdf = so.pdf;
+    *event = so.event;
+    return 1;
+}
+int oracle_material_evaluate(const OracleScene* s, int32_t argOffset, int32_t fn, const float* state,
+                             const float k1[3], const float k2[3], float ior1, float ior2, float diffuse[3],
+                             float glossy[3], float* pdf)
+{
+    ShadeState st;
+    Mat m;
+    state_from(state, &st);
+    if (!load_material_args(s, argOffset, fn, &st, &m)) return 0;
+    EvalOut e = bsdf_evaluate(&m, &st, V(k1[0], k1[1], k1[2]), V(k2[0], k2[1], k2[2]), ior1, ior2);
+    diffuse[0] = e.bsdf_diffuse.x; diffuse[1] = e.bsdf_diffuse.y; diffuse[2] = e.bsdf_diffuse.z;
+    glossy[0] = e.bsdf_glossy.x; glossy[1] = e.bsdf_glossy.y; glossy[2] = e.bsdf_glossy.z;
+    *pdf = e.pdf;
+    return 1;
+}
+int oracle_material_emission(const OracleScene* s, int32_t argOffset, int32_t fn, const float* state,
+                             float intensity[3])
+{
+    ShadeState st;
+    Mat m;
+    state_from(state, &st);
+    if (!load_material_args(s, argOffset, fn, &st, &m)) return 0;
+    intensity[0] = m.emission.x; intensity[1] = m.emission.y; intensity[2] = m.emission.z;
+    return 1;
 }
 
 /* ------------------------------------------------------------------------- */
@@ -1576,6 +1585,14 @@ static void camera_ray(const PathTracerParam* ubo, uint32_t px, uint32_t py, uin
     mat_mul4(&ubo->viewToWorld, orig, wo);
     *o = V(wo[0], wo[1], wo[2]);
     *d = vnormalize(V(wdir[0], wdir[1], wdir[2]));
+}
+
+/* generateCameraRay exported for function-level checks: out = {o[3], d[3]}. */
+void oracle_camera_ray(const PathTracerParam* p, uint32_t px, uint32_t py, uint32_t* rng, uint32_t s, float out[6])
+{
+    v3 o, d;
+    camera_ray(p, px, py, rng, s, &o, &d);
+    out[0] = o.x; out[1] = o.y; out[2] = o.z; out[3] = d.x; out[4] = d.y; out[5] = d.z;
 }
 
 /* pathtracerMdl.hlsl:204-404 */

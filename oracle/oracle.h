@@ -101,6 +101,12 @@ int oracle_intersect_fp64(const OracleScene* s, const Ray* rays, const uint32_t*
 int oracle_intersect_terms_fp64(const OracleScene* s, const Ray* rays, const uint32_t* instIds,
                                 const uint32_t* primIds, uint32_t n, double* scale3);
 
+/* lights.h:284-340 for one light: out = {pointOnLight[3], pdf, normal[3],
+ * area, L[3], distToLight}. */
+void oracle_sample_light(const UniformLight* l, const float hitPoint[3], float u0, float u1, float out[12]);
+/* pathtracerMdl.hlsl:165-202: out = {origin[3], direction[3]}. */
+void oracle_camera_ray(const PathTracerParam* p, uint32_t px, uint32_t py, uint32_t* rng, uint32_t s, float out[6]);
+
 /* pathtracerMdl.hlsl:406-423 computeMain over idx in [0, W*H*spp):
  * writes sampleBuffer[(idx)*3 + c]. */
 int oracle_pathtrace(const PathTracerParam* p, const OracleScene* s, float* sampleBuffer,
@@ -123,6 +129,20 @@ int oracle_tonemap(const Tonemapparam* p, const float* input, float* output);
 void oracle_mdl_read(const uint8_t* buffer, uint64_t bytes, const uint32_t* offsets, const uint32_t* kinds, uint32_t n,
                      uint64_t* out);
 int oracle_upscale(const Upscalepassparam* p, const float* input, uint32_t inW, uint32_t inH, float* output);
+
+/* The project's native materials behind the MDL dispatch functions
+ * (src/materialmanager/mdlHlslCodeGen.cpp:32-81), by argument-block offset
+ * and function id; state = {normal[3], geom_normal[3], position[3], u, v}.
+ * Return 0 when the material record is out of range.  Used by the HLSL shim
+ * of oracle/ref/ in place of the MDL-generated code. */
+int oracle_material_sample(const OracleScene* s, int32_t argOffset, int32_t fn, const float* state, const float k1[3],
+                           const float xi[4], float ior1, float ior2, float k2[3], float bsdfOverPdf[3], float* pdf,
+                           int* event);
+int oracle_material_evaluate(const OracleScene* s, int32_t argOffset, int32_t fn, const float* state,
+                             const float k1[3], const float k2[3], float ior1, float ior2, float diffuse[3],
+                             float glossy[3], float* pdf);
+int oracle_material_emission(const OracleScene* s, int32_t argOffset, int32_t fn, const float* state,
+                             float intensity[3]);
 
 /* texture lookup, mdl_runtime.hlsl:173-208 (REPEAT, no crop) */
 void oracle_tex_lookup(const OracleTexture* t, float u, float v, float out[4]);
