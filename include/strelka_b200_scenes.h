@@ -52,7 +52,14 @@ typedef struct StrelkaCornellConfig {
     uint32_t maxDepth;      /* 4 */
     uint32_t spp;           /* 1 */
     uint32_t tonemapper;    /* unused by the generator, kept for callers */
-    uint32_t pad;
+    /* Extra lights, a bit mask (0 = the rect light alone):
+     *   1: a disc light (radius 0.12, radiance 10) facing down just under the
+     *      ceiling light, so shadow rays toward the ceiling light often
+     *      reach the disc's emitter first;
+     *   2: a sphere light (radius 0.08, radiance 20) floating in the box.
+     * Each is built as the reference builds it (src/scene/scene.cpp:
+     * 210-361 meshes, 418-510 records) and gets an emitter instance. */
+    uint32_t extraLights;
 } StrelkaCornellConfig;
 int strelka_scene_cornell(const StrelkaCornellConfig* cfg, StrelkaHostScene* out);
 

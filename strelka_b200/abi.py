@@ -268,7 +268,7 @@ class StrelkaHostScene(C.Structure):
 class StrelkaCornellConfig(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("sphereLevels", C.c_uint32),
                 ("lightSide", C.c_float), ("lightRadiance", C.c_float), ("maxDepth", C.c_uint32),
-                ("spp", C.c_uint32), ("tonemapper", C.c_uint32), ("pad", C.c_uint32)]
+                ("spp", C.c_uint32), ("tonemapper", C.c_uint32), ("extraLights", C.c_uint32)]
 
 
 class StrelkaLargeConfig(C.Structure):

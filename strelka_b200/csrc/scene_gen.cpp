@@ -640,6 +640,83 @@ extern "C" int strelka_scene_cornell(const StrelkaCornellConfig* cfg, StrelkaHos
         uint32_t mesh = b.add_mesh(v, idx);
         b.add_instance(mesh, -1, xf, 0);
     }
+    // disc light (scene.cpp:318-361 mesh: a 16-triangle fan of the unit disc
+    // in local z = 0; scene.cpp:480-495 record): its transform carries the
+    // radius as a scale, so, as in the reference, the record's axes and
+    // normal have length r and points[0].x scales the sample by r again
+    if (cfg->extraLights & 1u) {
+        const double r = 0.12, radiance = 10.0;
+        M4 rot = identity();
+        // local z -> world -y (facing down), local x -> world x, local y -> world z
+        rot.m[0] = 1; rot.m[1] = 0; rot.m[2] = 0;
+        rot.m[4] = 0; rot.m[5] = 0; rot.m[6] = 1;
+        rot.m[8] = 0; rot.m[9] = -1; rot.m[10] = 0;
+        M4 xf = mul(mul(translate(0.52, 0.93, 0.47), rot), scale(r, r, r));
+        auto apply = [&](const double p[4], float out[4]) {
+            for (int i = 0; i < 4; ++i) {
+                double acc = 0;
+                for (int j = 0; j < 4; ++j) acc += xf.m[j * 4 + i] * p[j];
+                out[i] = (float)acc;
+            }
+        };
+        UniformLight L{};
+        L.points[0].x = (float)r;
+        const double o[4] = {0, 0, 0, 1}, ex[4] = {1, 0, 0, 0}, ey[4] = {0, 1, 0, 0}, ez[4] = {0, 0, 1, 0};
+        apply(o, &L.points[1].x);
+        apply(ex, &L.points[2].x);
+        apply(ey, &L.points[3].x);
+        apply(ez, &L.normal.x);
+        const float c = (float)(radiance);
+        L.color.x = L.color.y = L.color.z = c;
+        L.color.w = c;
+        L.type = 1;
+        const int32_t lightId = (int32_t)b.lights.size();
+        b.lights.push_back(L);
+        std::vector<Vertex> v;
+        std::vector<uint32_t> idx;
+        const double n[3] = {0.0, 0.0, 1.0};
+        const double centre[3] = {0, 0, 0}, first[3] = {1, 0, 0};
+        v.push_back(make_vertex(centre, n, 0, 0));
+        v.push_back(make_vertex(first, n, 0, 0));
+        const double step = 2.0 * M_PI / 16;
+        double angle = 0;
+        for (int i = 0; i < 16; ++i) {
+            idx.push_back(0);
+            idx.push_back((uint32_t)v.size() - 1);
+            angle += step;
+            const double p[3] = {std::cos(angle), std::sin(angle), 0.0};
+            v.push_back(make_vertex(p, n, 0, 0));
+            idx.push_back((uint32_t)v.size() - 1);
+        }
+        uint32_t mesh = b.add_mesh(v, idx);
+        b.add_instance(mesh, -1, xf, lightId);
+    }
+    // sphere light (scene.cpp:210-316 mesh: an icosphere subdivided 3 times;
+    // scene.cpp:497-508 record: radius and centre)
+    if (cfg->extraLights & 2u) {
+        const double r = 0.08, radiance = 20.0;
+        M4 xf = mul(translate(0.62, 0.55, 0.62), scale(r, r, r));
+        UniformLight L{};
+        L.points[0].x = (float)r;
+        L.points[1].x = 0.62f;
+        L.points[1].y = 0.55f;
+        L.points[1].z = 0.62f;
+        L.points[1].w = 1.0f;
+        const float c = (float)radiance;
+        L.color.x = L.color.y = L.color.z = c;
+        L.color.w = c;
+        L.type = 2;
+        const int32_t lightId = (int32_t)b.lights.size();
+        b.lights.push_back(L);
+        std::vector<std::array<double, 3>> pv;
+        std::vector<uint32_t> f;
+        icosahedron(pv, f);
+        for (int i = 0; i < 3; ++i) subdivide(pv, f);
+        std::vector<Vertex> v;
+        for (auto& p : pv) v.push_back(make_vertex(p.data(), p.data(), 0, 0));
+        uint32_t mesh = b.add_mesh(v, f);
+        b.add_instance(mesh, -1, xf, lightId);
+    }
     int rc = b.finish(out);
     if (rc) return rc;
     const double eye[3] = {0.5, 0.5, 2.35}, target[3] = {0.5, 0.5, 0.0};

@@ -154,10 +154,17 @@ def _from_c(hs: abi.StrelkaHostScene) -> HostScene:
         lib.strelka_scene_free(C.byref(hs))
 
 
+CORNELL_DISC_LIGHT = 1
+CORNELL_SPHERE_LIGHT = 2
+
+
 def cornell(width: int = 512, height: int = 512, sphere_levels: int = 4, light_side: float = 0.25,
-            light_radiance: float = 15.0, max_depth: int = 4, spp: int = 1) -> HostScene:
+            light_radiance: float = 15.0, max_depth: int = 4, spp: int = 1, extra_lights: int = 0) -> HostScene:
+    """The Cornell box; extra_lights adds a disc light under the ceiling light
+    (CORNELL_DISC_LIGHT) and/or a sphere light (CORNELL_SPHERE_LIGHT)."""
     lib = _lib()
-    cfg = abi.StrelkaCornellConfig(width, height, sphere_levels, light_side, light_radiance, max_depth, spp, 1, 0)
+    cfg = abi.StrelkaCornellConfig(width, height, sphere_levels, light_side, light_radiance, max_depth, spp, 1,
+                                   extra_lights)
     hs = abi.StrelkaHostScene()
     _check(lib, lib.strelka_scene_cornell(C.byref(cfg), C.byref(hs)))
     return _from_c(hs)

@@ -256,6 +256,20 @@ def test_cornell_samples(sampling, depth):
     assert undefined < 0.2
 
 
+@pytest.mark.parametrize("extra", [1, 2, 3])
+def test_disc_sphere_and_several_lights(extra):
+    # the light pick over 2-3 lights (pathtracerMdl.hlsl:83-92), the disc and
+    # sphere samplers (lights.h:196-219, 59-89, 300-340, the sphere sampler's
+    # shadowed `u` kept) and shadow rays that reach another light's emitter
+    # first (pathtracerMdl.hlsl:63-74)
+    s = scenes.cornell(48, 40, sphere_levels=3, extra_lights=extra)
+    view = oracle.SceneView(s)
+    for sampling, depth in ((1, 8), (0, 4)):
+        p = s.param(spp=4, maxDepth=depth, frameNumber=5 + depth, stratifiedSamplingType=sampling)
+        assert p.numLights == 1 + bin(extra).count("1")
+        assert _compare_samples(view, p) < 0.2
+
+
 def test_instanced_textured_scene_without_environment():
     # the large-render generator at toy size: 6 instanced displaced spheres,
     # GGX metal / dielectric / textured Lambert; the environment light is an

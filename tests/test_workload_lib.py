@@ -15,7 +15,8 @@ def _fields(hs):
 
 
 def _build_all():
-    return [scenes.cornell(64, 48, sphere_levels=3), scenes.soup(20_000, 3),
+    return [scenes.cornell(64, 48, sphere_levels=3), scenes.cornell(32, 32, sphere_levels=2, extra_lights=3),
+            scenes.soup(20_000, 3),
             scenes.large(width=64, height=32, instances=3, frequency=12, num_textures=2, tex_size=64, env_width=64,
                          env_height=32, max_depth=8, spp=2, seed=0)], scenes.rays_soup(1000, 5, shadow=True)
 
