@@ -6,9 +6,13 @@ this module; the product never does.
 
 The oracle restates the reference's shader math in C (``oracle/oracle.c``,
 each function citing the reference lines it follows).  Parity status: pinned
-by the reference's slab-test known answers (tests/intersection/aabb.cpp), by
-hand-computed RNG states, analytic checks and the golden fixtures under
-``tests/golden/``; the reference's own shaders cannot run here.
+to the reference's own shader source.  oracle/build_ref.sh compiles the
+reference's pathtracerMdl.hlsl (with its includes), reduction, accumulation,
+tonemap and upscale shaders on the host into oracle/_ref/ (``oracle.ref``),
+and tests/test_ref_pin.py checks this restatement against it bit for bit,
+function by function and sample by sample.  Also: the reference's slab-test
+known answers (tests/intersection/aabb.cpp), hand-computed RNG states,
+analytic checks and the golden fixtures under ``tests/golden/``.
 """
 from __future__ import annotations
 

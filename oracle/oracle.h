@@ -5,12 +5,17 @@
  * only the tests, the smoke check and the CPU-baseline leg of the benchmark
  * may load it.  Nothing in the product links or calls it.
  *
- * Parity status: the reference's shaders cannot run on this machine (they
- * need Slang and a Vulkan device) and its tests hold no golden vectors for
- * this path, so the restatement is pinned by the reference's own known-answer
- * cases (the slab tests of tests/intersection/aabb.cpp:16-106), by
- * hand-computed RNG states, by analytic checks (white furnace, tonemap
- * formulas at chosen points) and by golden fixtures generated from this file.
+ * Parity status: pinned to the reference's own shader source.
+ * oracle/build_ref.sh compiles the reference's pathtracerMdl.hlsl (with
+ * raytracing.h, ray.h, random.h, helper.h, pack.h, lights.h), reduction,
+ * accumulation, tonemap and upscale shaders on the host (a syntax-only
+ * rewrite, oracle/hlsl2cpp.py, over the HLSL shim oracle/ref/shim.h) into
+ * oracle/_ref/; tests/test_ref_pin.py checks this file against it bit for
+ * bit, function by function and sample by sample.  The reference's
+ * material code is generated at run time by the MDL SDK, which is absent;
+ * there both sides use the project's native materials below, unpinned.
+ * Further pins: the slab-test known answers of tests/intersection/aabb.cpp,
+ * hand-computed RNG states and analytic checks.
  *
  * Every function cites the reference lines it restates.  Floating-point
  * evaluation follows the source expressions left to right with no fused
