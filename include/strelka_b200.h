@@ -652,7 +652,10 @@ int strelka_batch_destroy(StrelkaBatch* batch);
 /* Copies the job descriptors (at most STRELKA_BATCH_MAX_JOBS, at most 2^31
  * paths in all) and prepares each distinct scene's traversal records on
  * `stream`.  Device buffers stay owned by the caller.  Drops captured graphs
- * and the tuned configuration. */
+ * and the tuned configuration.  The batch runs its jobs smallest first (by
+ * W*H*spp, ties in the given order) so that small jobs finish early; every
+ * job's samples are the same whatever the order, and per-job results
+ * (strelka_batch_job_latency) keep the caller's indexing. */
 int strelka_batch_set_jobs(StrelkaBatch* batch, const PathTracerDesc* jobs, uint32_t numJobs, void* stream);
 /* Sets every job's frameNumber to its descriptor's value + frameOffset
  * (synchronises the stream; captured graphs stay valid). */

@@ -574,7 +574,8 @@ struct SceneRec {
 struct StrelkaBatch {
     int numSMs = 148;
     std::vector<PathTracerDesc> descs;
-    std::vector<BatchJobDev> jobsHost;
+    std::vector<BatchJobDev> jobsHost;  // by slot
+    std::vector<uint32_t> order;        // slot -> the caller's job index
     std::vector<uint32_t> prefix;
     uint32_t total = 0;
     uint32_t numKeys = 0;
@@ -878,11 +879,26 @@ extern "C" int strelka_batch_set_jobs(StrelkaBatch* b, const PathTracerDesc* job
     if (numJobs > (uint32_t)kMaxJobs) return fail(STRELKA_ERR_INVALID_ARGUMENT, "at most %d jobs", kMaxJobs);
     if (numJobs && !jobs) return fail(STRELKA_ERR_INVALID_ARGUMENT, "jobs is NULL");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // Shortest job first: slot k of the batch's path space holds the caller's
+    // job ord[k], in ascending order of path count (ties in the caller's
+    // order), so small jobs finish in the first chunks instead of waiting
+    // behind large ones.  A path's arithmetic depends only on its own job
+    // and its index within that job, so the order changes no result.
+    std::vector<uint32_t> ord(numJobs);
+    for (uint32_t j = 0; j < numJobs; ++j) ord[j] = j;
+    auto paths_of = [&](uint32_t j) {
+        const PathTracerParam& u = jobs[j].constants;
+        return u.dimension[0] <= 0 || u.dimension[1] <= 0 || u.spp <= 0
+                   ? 0ull
+                   : (uint64_t)u.dimension[0] * (uint64_t)u.dimension[1] * (uint64_t)u.spp;
+    };
+    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b2) { return paths_of(a) < paths_of(b2); });
     std::vector<uint32_t> prefix(numJobs + 1, 0);
     uint64_t total = 0;
     uint32_t numKeys = 1;
     int maxDepth = 0;
-    for (uint32_t j = 0; j < numJobs; ++j) {
+    for (uint32_t k = 0; k < numJobs; ++k) {
+        const uint32_t j = ord[k];
         const PathTracerDesc& d = jobs[j];
         int rc = validate_scene_desc(&d);
         if (rc) return fail(rc, "job %u: %s", j, last_error().c_str());
@@ -895,7 +911,7 @@ extern "C" int strelka_batch_set_jobs(StrelkaBatch* b, const PathTracerDesc* job
             if (!e->rgba32f || !e->marginal_cdf || !e->conditional_cdf || e->width == 0 || e->height == 0)
                 return fail(STRELKA_ERR_INVALID_ARGUMENT, "job %u: incomplete environment map", j);
         }
-        prefix[j] = (uint32_t)total;
+        prefix[k] = (uint32_t)total;
         total += (uint64_t)u.dimension[0] * (uint64_t)u.dimension[1] * (uint64_t)u.spp;
         if (total > 0x7FFFFFFFull) return fail(STRELKA_ERR_INVALID_ARGUMENT, "the batch exceeds 2^31 paths");
         maxDepth = std::max(maxDepth, (int)u.maxDepth);
@@ -909,8 +925,8 @@ extern "C" int strelka_batch_set_jobs(StrelkaBatch* b, const PathTracerDesc* job
     // record tables of the distinct scenes (kept across calls)
     std::vector<BatchJobDev> host(numJobs);
     uint32_t keyBase = 0;
-    for (uint32_t j = 0; j < numJobs; ++j) {
-        const PathTracerDesc& d = jobs[j];
+    for (uint32_t k = 0; k < numJobs; ++k) {
+        const PathTracerDesc& d = jobs[ord[k]];
         const SceneTables* tables = nullptr;
         for (SceneRec& r : b->scenes)
             if (r.nodes == d.bvhNodes && r.numNodes == d.numNodes && r.vb == d.vb && r.ib == d.ib &&
@@ -926,12 +942,12 @@ extern "C" int strelka_batch_set_jobs(StrelkaBatch* b, const PathTracerDesc* job
                                         d.vb, d.numVertices, *tables, b->status, b->numSMs, st);
             if (rc) return rc;
         }
-        BatchJobDev& J = host[j];
+        BatchJobDev& J = host[k];
         memset(&J, 0, sizeof(J));
         J.s = scene_from_desc(&d, *tables, b->srgbLut, b->status);
         J.ubo = d.constants;
         J.sampleBuffer = d.sampleBuffer;
-        J.numPaths = prefix[j + 1] - prefix[j];
+        J.numPaths = prefix[k + 1] - prefix[k];
         J.keyBase = keyBase;
         keyBase += (d.mdl_mdlMaterial ? d.numMaterials : 0) + 1;
     }
@@ -944,6 +960,7 @@ extern "C" int strelka_batch_set_jobs(StrelkaBatch* b, const PathTracerDesc* job
     if (numJobs) SB_CUDA_TRY(cudaMemcpy(b->jobsDev, host.data(), numJobs * sizeof(BatchJobDev), cudaMemcpyHostToDevice));
     SB_CUDA_TRY(cudaMemcpy(b->prefixDev, prefix.data(), (numJobs + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice));
     b->descs.assign(jobs, jobs + numJobs);
+    b->order = ord;
     b->jobsHost = host;
     b->prefix = prefix;
     b->total = (uint32_t)total;
@@ -958,7 +975,8 @@ extern "C" int strelka_batch_set_frame(StrelkaBatch* b, uint32_t frameOffset, vo
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // the job table is rewritten in place (the captured graphs keep its address)
     std::vector<BatchJobDev> host = b->jobsHost;
-    for (size_t j = 0; j < host.size(); ++j) host[j].ubo.frameNumber = b->descs[j].constants.frameNumber + frameOffset;
+    for (size_t k = 0; k < host.size(); ++k)
+        host[k].ubo.frameNumber = b->descs[b->order[k]].constants.frameNumber + frameOffset;
     if (host.empty()) return STRELKA_OK;
     SB_CUDA_TRY(cudaStreamSynchronize(st));
     SB_CUDA_TRY(cudaMemcpy(b->jobsDev, host.data(), host.size() * sizeof(BatchJobDev), cudaMemcpyHostToDevice));
@@ -1073,10 +1091,12 @@ extern "C" int strelka_batch_job_latency(StrelkaBatch* b, void* stream, float* m
     BatchCtl c;
     SB_CUDA_TRY(cudaMemcpy(&c, b->ctl, sizeof(c), cudaMemcpyDeviceToHost));
     const uint32_t n = (uint32_t)b->jobsHost.size();
-    for (uint32_t j = 0; j < n && j < capacity; ++j) {
-        if (b->jobsHost[j].numPaths == 0) ms[j] = 0.0f;
-        else if (c.tDone[j] == 0 || c.tDone[j] < c.tStart) ms[j] = -1.0f;
-        else ms[j] = (float)((double)(c.tDone[j] - c.tStart) * 1e-6);
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t j = b->order[k];  // the caller's index of slot k
+        if (j >= capacity) continue;
+        if (b->jobsHost[k].numPaths == 0) ms[j] = 0.0f;
+        else if (c.tDone[k] == 0 || c.tDone[k] < c.tStart) ms[j] = -1.0f;
+        else ms[j] = (float)((double)(c.tDone[k] - c.tStart) * 1e-6);
     }
     return (int)n;
 }
