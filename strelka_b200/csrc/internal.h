@@ -14,11 +14,14 @@ void srgb_lut_host(float* lut);
 // Argument checks of a scene descriptor shared by every entry point.
 int validate_scene_desc(const PathTracerDesc* d);
 // Device tables derived from a scene's BVH, all in one allocation of
-// scene_tables_bytes(numNodes) bytes: the leaf-triangle records (4 float4 per
-// node slot), the 4-wide BVH (8 float4 per node, at most numNodes/2 + 1
+// scene_tables_bytes(numNodes) bytes: the leaf-triangle records (3 float4 per
+// leaf, at most numNodes/2 + 1 leaves), each node's compact leaf index (4 B
+// per node), the 4-wide BVH (8 float4 per node, at most numNodes/2 + 1
 // nodes) and the scratch of its build (16 B per node).
 struct SceneTables {
     float4* rec = nullptr;
+    uint32_t recCap = 0;
+    uint32_t* leafOf = nullptr;
     float4* wide = nullptr;
     uint32_t wideCap = 0;
     uint32_t* parent = nullptr;

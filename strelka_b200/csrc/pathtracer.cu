@@ -70,25 +70,39 @@ const char* kKernelNames[KC_COUNT] = {"generate",  "extend",    "shade",     "sh
                                       "prep",      "nrc_paths", "nrc_train", "nrc_infer", "sort", "tail"};
 
 // ---------------------------------------------------------------------------
-// Scene preparation: the record table of traverse.cuh, per leaf node slot:
-// the triangle exactly as getTriangle computes it (raytracing.h:134-153).
+// Scene preparation: the record table of traverse.cuh, one record per leaf
+// at the leaf's compact index leafOf[i] (its rank among the leaves in the
+// depth-first node order): the triangle exactly as getTriangle computes it
+// (raytracing.h:134-153).
+__global__ void k_leaf_flag(const float4* __restrict__ nodes, uint32_t numNodes, uint32_t* __restrict__ flag)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x)
+        flag[i] = __float_as_uint(nodes[2 * (size_t)i].w) != SB_INVALID ? 1u : 0u;
+}
+
 __global__ void k_prep_rec(const float4* __restrict__ nodes, uint32_t numNodes, const InstanceConstants* __restrict__ inst,
                            uint32_t numInstances, const uint32_t* __restrict__ ib, uint32_t numIndices,
-                           const Vertex* __restrict__ vb, uint32_t numVertices, float4* __restrict__ rec, uint32_t* status)
+                           const Vertex* __restrict__ vb, uint32_t numVertices, const uint32_t* __restrict__ leafOf,
+                           uint32_t recCap, float4* __restrict__ rec, uint32_t* status)
 {
     const float qnan = __int_as_float(0x7fc00000);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x) {
         const float4 lo = nodes[2 * (size_t)i];
         const float4 hi = nodes[2 * (size_t)i + 1];
         const uint32_t instId = __float_as_uint(lo.w);
-        float4* out = &rec[4 * (size_t)i];
         const uint32_t esc = __float_as_uint(hi.w);
         if (esc != SB_INVALID && esc >= numNodes) atomicOr(status, STRELKA_DEV_NODE_OOB);
         if (instId == SB_INVALID) continue;  // inner nodes live in the 4-wide BVH
+        const uint32_t li = leafOf[i];
+        if (li >= recCap) {  // more leaves than a binary tree of numNodes nodes has
+            atomicOr(status, STRELKA_DEV_NODE_OOB);
+            continue;
+        }
+        float4* out = &rec[3 * (size_t)li];
         const float4 bad = make_float4(qnan, qnan, qnan, 0.0f);
         if (instId >= numInstances) {
             atomicOr(status, STRELKA_DEV_INSTANCE_OOB);
-            out[0] = bad; out[1] = bad; out[2] = bad; out[3] = bad;
+            out[0] = bad; out[1] = bad; out[2] = bad;
             continue;
         }
         const InstanceConstants* ic = &inst[instId];
@@ -96,13 +110,13 @@ __global__ void k_prep_rec(const float4* __restrict__ nodes, uint32_t numNodes, 
         const uint32_t base = (uint32_t)ic->indexOffset + prim * 3u;
         if ((uint64_t)base + 2 >= numIndices) {
             atomicOr(status, STRELKA_DEV_INDEX_OOB);
-            out[0] = bad; out[1] = bad; out[2] = bad; out[3] = bad;
+            out[0] = bad; out[1] = bad; out[2] = bad;
             continue;
         }
         const uint32_t i0 = ib[base], i1 = ib[base + 1], i2 = ib[base + 2];
         if (i0 >= numVertices || i1 >= numVertices || i2 >= numVertices) {
             atomicOr(status, STRELKA_DEV_INDEX_OOB);
-            out[0] = bad; out[1] = bad; out[2] = bad; out[3] = bad;
+            out[0] = bad; out[1] = bad; out[2] = bad;
             continue;
         }
         const float* m = ic->objectToWorld.m;
@@ -112,7 +126,6 @@ __global__ void k_prep_rec(const float4* __restrict__ nodes, uint32_t numNodes, 
         out[0] = f4(v0, __uint_as_float(instId));
         out[1] = f4(e0, __uint_as_float(prim));
         out[2] = f4(e1, 0.0f);
-        out[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
 }
 
@@ -221,7 +234,8 @@ __global__ void k_wide_jump_finish(const float4* __restrict__ nodes, uint32_t nu
 }
 
 __global__ void k_wide_build(const float4* __restrict__ nodes, uint32_t numNodes, const uint32_t* __restrict__ flag,
-                             const uint32_t* __restrict__ map, float4* __restrict__ wide, uint32_t wideCap, uint32_t* status)
+                             const uint32_t* __restrict__ map, const uint32_t* __restrict__ leafOf, uint32_t recCap,
+                             float4* __restrict__ wide, uint32_t wideCap, uint32_t* status)
 {
     for (uint32_t P = blockIdx.x * blockDim.x + threadIdx.x; P < numNodes; P += gridDim.x * blockDim.x) {
         if (!flag[P]) continue;
@@ -251,14 +265,25 @@ __global__ void k_wide_build(const float4* __restrict__ nodes, uint32_t numNodes
         const uint32_t L = P + 1 < numNodes ? P + 1 : SB_INVALID;
         const uint32_t child[2] = {L, L != SB_INVALID ? right_of(L) : SB_INVALID};
         bool bad = child[0] == SB_INVALID || child[1] == SB_INVALID;
+        // a leaf's ref is its compact record index
+        auto leaf_ref = [&](uint32_t node) -> uint32_t {
+            const uint32_t li = leafOf[node];
+            if (li >= recCap) {
+                bad = true;
+                return SB_INVALID;
+            }
+            return li;
+        };
         for (int k = 0; k < 2; ++k) {
             const uint32_t c = child[k];
             if (c == SB_INVALID) continue;
             if (__float_as_uint(nodes[2 * (size_t)c].w) != SB_INVALID) {
                 // below the root a node is entered only after its box passed;
                 // the root's own box is tested here, before its leaf children
-                if (P == 0) put(c | SB_LEAF_BIT, P);
-                else put(c | SB_LEAF_BIT | SB_NOBOX_BIT, SB_INVALID);
+                const uint32_t li = leaf_ref(c);
+                if (li == SB_INVALID) put(SB_INVALID, SB_INVALID);
+                else if (P == 0) put(li | SB_LEAF_BIT, P);
+                else put(li | SB_LEAF_BIT | SB_NOBOX_BIT, SB_INVALID);
                 continue;
             }
             const uint32_t g0 = c + 1 < numNodes ? c + 1 : SB_INVALID;
@@ -267,7 +292,10 @@ __global__ void k_wide_build(const float4* __restrict__ nodes, uint32_t numNodes
             for (int j = 0; j < 2; ++j) {
                 const uint32_t g = grand[j];
                 if (g == SB_INVALID) continue;
-                if (__float_as_uint(nodes[2 * (size_t)g].w) != SB_INVALID) put(g | SB_LEAF_BIT, c);
+                if (__float_as_uint(nodes[2 * (size_t)g].w) != SB_INVALID) {
+                    const uint32_t li = leaf_ref(g);
+                    put(li == SB_INVALID ? SB_INVALID : (li | SB_LEAF_BIT), c);
+                }
                 else if (flag[g] && map[g] < wideCap) put(map[g], g);
                 else bad = true;
             }
@@ -1103,8 +1131,8 @@ static size_t scan_bytes(uint32_t n)
 size_t scene_tables_bytes(uint32_t numNodes)
 {
     const size_t n = std::max<uint32_t>(numNodes, 1);
-    const size_t wideCap = n / 2 + 1;
-    return align256(n * 4 * sizeof(float4)) + align256(wideCap * 8 * sizeof(float4)) + 4 * align256(n * 4) + 256 +
+    const size_t wideCap = n / 2 + 1, recCap = n / 2 + 1;
+    return align256(recCap * 3 * sizeof(float4)) + align256(wideCap * 8 * sizeof(float4)) + 5 * align256(n * 4) + 256 +
            align256(scan_bytes(numNodes));
 }
 
@@ -1113,9 +1141,12 @@ SceneTables scene_tables(void* base, uint32_t numNodes)
     const size_t n = std::max<uint32_t>(numNodes, 1);
     SceneTables t;
     t.wideCap = (uint32_t)(n / 2 + 1);
+    t.recCap = (uint32_t)(n / 2 + 1);  // a binary tree of n nodes has (n + 1) / 2 leaves
     char* p = static_cast<char*>(base);
     t.rec = reinterpret_cast<float4*>(p);
-    p += align256(n * 4 * sizeof(float4));
+    p += align256((size_t)t.recCap * 3 * sizeof(float4));
+    t.leafOf = reinterpret_cast<uint32_t*>(p);
+    p += align256(n * 4);
     t.wide = reinterpret_cast<float4*>(p);
     p += align256((size_t)t.wideCap * 8 * sizeof(float4));
     t.parent = reinterpret_cast<uint32_t*>(p);
@@ -1140,7 +1171,13 @@ int launch_prep_tables(const BVHNode* nodes, uint32_t numNodes, const InstanceCo
     if (!numNodes) return STRELKA_OK;
     const float4* nd = reinterpret_cast<const float4*>(nodes);
     const int grid = std::min<int>((numNodes + 255) / 256, numSMs * 16);
-    k_prep_rec<<<grid, 256, 0, st>>>(nd, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, t.rec, status);
+    size_t bytes = t.scanBytes;
+    // compact leaf indices: an exclusive scan of the leaf flags (held in
+    // `parent` until its own use below)
+    k_leaf_flag<<<grid, 256, 0, st>>>(nd, numNodes, t.parent);
+    SB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(t.scan, bytes, t.parent, t.leafOf, (int)numNodes, st));
+    k_prep_rec<<<grid, 256, 0, st>>>(nd, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, t.leafOf,
+                                     t.recCap, t.rec, status);
     SB_CUDA_TRY(cudaMemsetAsync(t.parent, 0xFF, (size_t)numNodes * 4, st));
     k_wide_parent<<<grid, 256, 0, st>>>(nd, numNodes, t.parent);
     SB_CUDA_TRY(cudaMemsetAsync(t.deep, 0, sizeof(uint32_t), st));
@@ -1160,9 +1197,9 @@ int launch_prep_tables(const BVHNode* nodes, uint32_t numNodes, const InstanceCo
         }
         k_wide_jump_finish<<<grid, 256, 0, st>>>(nd, numNodes, ancIn, parIn, t.flag, t.deep, status);
     }
-    size_t bytes = t.scanBytes;
+    bytes = t.scanBytes;
     SB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(t.scan, bytes, t.flag, t.map, (int)numNodes, st));
-    k_wide_build<<<grid, 256, 0, st>>>(nd, numNodes, t.flag, t.map, t.wide, t.wideCap, status);
+    k_wide_build<<<grid, 256, 0, st>>>(nd, numNodes, t.flag, t.map, t.leafOf, t.recCap, t.wide, t.wideCap, status);
     SB_CUDA_TRY(cudaGetLastError());
     return STRELKA_OK;
 }
@@ -1173,6 +1210,8 @@ DevScene scene_from_desc(const PathTracerDesc* d, const SceneTables& t, const fl
     s.nodes = reinterpret_cast<const float4*>(d->bvhNodes);
     s.tris = nullptr;
     s.rec = t.rec;
+    s.leafOf = t.leafOf;
+    s.numRec = t.recCap;
     s.wide = t.wide;
     s.numWide = t.wideCap;
     s.numNodes = d->numNodes;

@@ -22,7 +22,9 @@ namespace sb {
 struct DevScene {
     const float4* nodes;  // 2 float4 per BVHNode
     const float4* tris;   // 3 float4 per node (leaf slots only)
-    const float4* rec;    // 4 float4 per node: leaf triangles (at leaf slots)
+    const float4* rec;    // 3 float4 per leaf, at the leaf's compact index
+    const uint32_t* leafOf;  // per node: its compact leaf index (leaves only)
+    uint32_t numRec;      // capacity of `rec` in leaves
     const float4* wide;   // 8 float4 per 4-wide node (see below)
     uint32_t numWide;     // capacity of `wide` in nodes
     uint32_t numNodes;
@@ -193,7 +195,9 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, v3 o, float tmax, v
 // 4-wide traversal.
 //
 // Derived tables, built once per scene version on the GPU (pathtracer.cu):
-//   record table, 4 float4 per node slot: leaf node n holds its triangle
+//   compact leaf index of every node: a leaf's rank among the leaves in the
+//     depth-first node order (leafOf, an exclusive scan of the leaf flags);
+//   record table, 3 float4 per leaf at its compact index: the triangle
 //     [0] = v0 | instId  [1] = e0 | primId  [2] = e1 | 0;
 //   4-wide BVH, 8 float4 per node: the binary inner nodes at even depth of
 //     the reference's tree (children L = n+1 and R = escape(n+1), the
@@ -204,7 +208,7 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, v3 o, float tmax, v
 //     SB_NOBOX_BIT: tested without a box, as the reference does, except at
 //     the root, where the root's box gates it), otherwise c's two children:
 //     an inner one with its own box (ref = its 4-wide index), a leaf one
-//     gated by c's box (ref = its node slot | SB_LEAF_BIT).
+//     gated by c's box (ref = its compact index | SB_LEAF_BIT).
 // A child's box test passing implies its parent's (the slab arithmetic
 // rounds monotonically and a parent box contains its children's), so testing
 // only the even-depth boxes leaves the set of triangles a query tests
@@ -215,7 +219,7 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, v3 o, float tmax, v
 // with the nearest passing inner entry and keeps the others on a per-thread
 // stack with their entry distances (sorted, farthest first), dropping any
 // subtree whose entry exceeds the best hit by more than a relative 2^-12.  A
-// tie in t goes to the leaf with the smaller node index, the first in
+// tie in t goes to the leaf with the smaller compact index, the first in
 // depth-first order: the reference's winner under its strict t < minHit rule.
 // Any hit keeps the reference's depth-first order exactly: a node's passing
 // entries go onto the stack in reverse order, and leaves are tested when
@@ -230,7 +234,7 @@ namespace sb {
 #ifndef SB_STACK
 #define SB_STACK 64
 #endif
-#define SB_LEAF_BIT 0x80000000u   // a ref to a leaf triangle (its node slot in the record table)
+#define SB_LEAF_BIT 0x80000000u   // a ref to a leaf triangle (its compact index in the record table)
 #define SB_NOBOX_BIT 0x40000000u  // a leaf tested without a box (a leaf child of the node itself)
 
 struct RayQ {
@@ -248,11 +252,12 @@ __device__ __forceinline__ RayQ make_ray(v3 o, float tmax, v3 d)
     return r;
 }
 
-// leaf triangle of node `leaf` in the record table
+// triangle of leaf `leaf` (its compact index: the leaf's rank in the
+// depth-first node order) in the record table
 __device__ __forceinline__ bool rec_triangle(const DevScene& s, const RayQ& r, uint32_t leaf, float& t, float& bu, float& bv,
                                              uint32_t& instId, uint32_t& primId)
 {
-    const float4* tp = &s.rec[4 * (size_t)leaf];
+    const float4* tp = &s.rec[3 * (size_t)leaf];
     const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
     instId = __float_as_uint(a.w);
     primId = __float_as_uint(b.w);
@@ -264,7 +269,7 @@ __device__ __forceinline__ bool rec_triangle(const DevScene& s, const RayQ& r, u
 struct Fallback {
     HitRec hit;
     float minHit;
-    uint32_t leaf;  // node index of the best hit's leaf
+    uint32_t leaf;  // compact index of the best hit's leaf
     uint32_t nInner, nLeaf;
     bool found;
 };
@@ -291,10 +296,15 @@ __device__ __noinline__ Fallback closest_stackless_rec(const DevScene s, const R
             if (COUNT) ++f.nLeaf;
             float t, bu, bv;
             uint32_t iid, pid;
-            if (rec_triangle(s, r, node, t, bu, bv, iid, pid) && (t < r.tmax) &&
-                (t < minHit || (t == minHit && node < best))) {
+            const uint32_t li = __ldg(&s.leafOf[node]);
+            if (li >= s.numRec) {
+                raise_status(s, STRELKA_DEV_NODE_OOB);
+                break;
+            }
+            if (rec_triangle(s, r, li, t, bu, bv, iid, pid) && (t < r.tmax) &&
+                (t < minHit || (t == minHit && li < best))) {
                 minHit = t;
-                best = node;
+                best = li;
                 hit.t = t;
                 hit.u = bu;
                 hit.v = bv;
@@ -340,7 +350,12 @@ __device__ __noinline__ Fallback any_stackless_rec(const DevScene s, const RayQ 
             if (COUNT) ++f.nLeaf;
             float t, bu, bv;
             uint32_t iid, pid;
-            bool isect = rec_triangle(s, r, node, t, bu, bv, iid, pid);
+            const uint32_t li = __ldg(&s.leafOf[node]);
+            if (li >= s.numRec) {
+                raise_status(s, STRELKA_DEV_NODE_OOB);
+                break;
+            }
+            bool isect = rec_triangle(s, r, li, t, bu, bv, iid, pid);
             hit.t = t;
             if (isect && (t < r.tmax)) {
                 hit.instId = iid;
@@ -370,7 +385,7 @@ __device__ __noinline__ Fallback any_stackless_rec(const DevScene s, const RayQ 
 struct Trav {
     RayQ r;
     float minHit;
-    uint32_t leaf;  // closest hit: node index of the best hit's leaf
+    uint32_t leaf;  // closest hit: compact index of the best hit's leaf
     uint32_t cur;  // 4-wide node to process next, a leaf ref (SB_LEAF_BIT), or SB_INVALID = pop
     int sp;
     uint32_t steps;
@@ -442,9 +457,9 @@ __device__ __forceinline__ void cswap(float& ta, uint32_t& ra, float& tb, uint32
 }
 
 // Closest-hit test of one leaf triangle.  On a tie in t the leaf with the
-// smaller node index wins: the node array is in depth-first order, so that
-// is the leaf the reference visits first and keeps (its test is the strict
-// t < minHit), whatever order this traversal reaches them in.
+// smaller compact index wins: compact indices follow the depth-first node
+// order, so that is the leaf the reference visits first and keeps (its test
+// is the strict t < minHit), whatever order this traversal reaches them in.
 __device__ __forceinline__ void closest_leaf(const DevScene& s, Trav& T, uint32_t leaf)
 {
     float t, bu, bv;
