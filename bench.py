@@ -722,6 +722,8 @@ def main():
     ap.add_argument("--ref-step-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--split-frame", action="store_true",
+                    help="N > 1: split every frame over the ranks (strong scaling) instead of independent frames")
     ap.add_argument("--no-studies", action="store_true",
                     help="skip the traversal microbenchmark and the radiance-cache study in the default run")
     ap.add_argument("--workload", default="large", choices=["large", "traversal", "nrc", "nrc-mlp", "batch"])
@@ -765,7 +767,8 @@ def main():
     import torch
 
     from strelka_b200 import abi, multigpu
-    from strelka_b200.render import DeviceScene, PathTracer, accumulation_param, resolve, tonemap_param
+    from strelka_b200.render import (Accumulation, DeviceScene, PathTracer, ReductionPass, Tonemap, accumulation_param,
+                                     ptr, resolve, tonemap_param)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -783,21 +786,40 @@ def main():
     ds = DeviceScene(hs)
     W, H, S = args.width, args.height, args.spp
     total = W * H * S
+    # --split-frame (N > 1): every frame is split over the ranks, spp/N
+    # samples per pixel each, and their reduced images are averaged by one
+    # NCCL all-reduce per frame (strong scaling); otherwise every rank renders
+    # its own frames (weak scaling)
+    split = world > 1 and args.split_frame
+    local_total = total // world if split else total
     mode = abi.MODE_WAVEFRONT if args.mode == "wavefront" else abi.MODE_MEGAKERNEL
     pt = PathTracer(mode=mode, chunk_paths=args.chunk, profile=True)
-    sb = torch.empty(total * 3, dtype=torch.float32, device="cuda")
+    sb = torch.empty(local_total * 3, dtype=torch.float32, device="cuda")
     hist = torch.zeros(W * H * 4, dtype=torch.float32, device="cuda")
     acc = torch.zeros(W * H * 4, dtype=torch.float32, device="cuda")
+    cur = torch.zeros(W * H * 4, dtype=torch.float32, device="cuda")
+    tmimg = torch.zeros(W * H * 4, dtype=torch.float32, device="cuda")
     rgba8 = torch.empty(W * H * 4, dtype=torch.uint8, device="cuda")
     tp = tonemap_param(W, H, 1)
     stream = torch.cuda.current_stream()
 
+    def frame_param(it):
+        if split:
+            return multigpu.split_frame_param(hs.param(frameNumber=it, iteration=it), rank, world)
+        return hs.param(frameNumber=multigpu.frame_number(rank, it), iteration=it)
+
     def frame(it):
         # PtRender::drawFrame (src/render/ptrender.cpp:735-862) for one view
-        p = hs.param(frameNumber=multigpu.frame_number(rank, it), iteration=it)
-        pt.execute(ds.desc(p, sb), total, 1, it, stream)
+        p = frame_param(it)
+        pt.execute(ds.desc(p, sb), local_total, 1, it, stream)
         ap_ = accumulation_param(W, H, it)
-        resolve(p, sb, tp, ap_ if it > 0 else None, hist if it > 0 else None, acc, None, rgba8, stream)
+        if split:
+            ReductionPass().execute(abi.ReductionDesc(p, ptr(sb), ptr(cur)), W * H, 1, it, stream)
+            multigpu.combine_split_frame(cur, dist)
+            Accumulation().execute(abi.AccumulationDesc(ap_, ptr(cur), ptr(hist), ptr(acc)), W, H, it, stream)
+            Tonemap().execute(abi.TonemapDesc(tp, ptr(acc), ptr(tmimg)), W, H, it, stream)
+        else:
+            resolve(p, sb, tp, ap_ if it > 0 else None, hist if it > 0 else None, acc, None, rgba8, stream)
         return p
 
     for it in range(args.warmup):
@@ -831,7 +853,8 @@ def main():
     times = pt.kernel_times(stream)
     el_ms = multigpu.max_over_ranks(el_ms, dist, device="cuda")
 
-    value = world * total * args.steps / (el_ms * 1e-3) / 1e6
+    frame_paths = total if split else world * total  # paths of the whole job per step
+    value = frame_paths * args.steps / (el_ms * 1e-3) / 1e6
 
     # ---- extend-kernel roofline: replay the timed frames with counters -------
     ext_ms = times["extend"][0]
@@ -839,8 +862,7 @@ def main():
     launches = sum(c for _, c in times.values()) + args.steps  # + one resolve per frame
     pt_count = PathTracer(mode=mode, chunk_paths=args.chunk, count=True)
     for k in range(args.steps):
-        pt_count.execute(ds.desc(hs.param(frameNumber=multigpu.frame_number(rank, args.warmup + k)), sb), total, 1, 0,
-                         stream)
+        pt_count.execute(ds.desc(frame_param(args.warmup + k), sb), local_total, 1, 0, stream)
     cnt = pt_count.counters(stream)
     pt_count.close()
     # algorithmic bytes of the closest-hit traversal: 112 B per 4-wide node
@@ -858,7 +880,8 @@ def main():
     sh_achieved = sh_bytes / (sh_ms * 1e-3) / 1e9 if sh_ms > 0 else None
 
     # ---- end to end through the C ABI: host param in, tonemapped RGBA8 out ---
-    host_img = torch.empty(W * H * 4, dtype=torch.uint8, pin_memory=True)
+    out_img = tmimg if split else rgba8
+    host_img = torch.empty(out_img.numel(), dtype=out_img.dtype, pin_memory=True)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -867,13 +890,13 @@ def main():
     f0.record(stream)
     for k in range(args.steps):
         frame(args.warmup + args.steps + k)
-        host_img.copy_(rgba8, non_blocking=True)
+        host_img.copy_(out_img, non_blocking=True)
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = multigpu.max_over_ranks(f0.elapsed_time(f1), dist, device="cuda")
-    e2e = world * total * args.steps / (e2e_ms * 1e-3) / 1e6
+    e2e = frame_paths * args.steps / (e2e_ms * 1e-3) / 1e6
     img = host_img.numpy()
-    if not (img[3::4] == 255).all():
+    if not (img[3::4] == (1.0 if split else 255)).all():
         raise RuntimeError("resolve produced no image")
     st = pt.device_status()
     if st != 0:
@@ -914,9 +937,11 @@ def main():
     param_bytes = 336 + 416 + 16
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": el_ms / args.steps, "higher_is_better": True, "scaling": "strong" if split else "weak",
+        "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural scene, see config.workload)", "config": cfg,
-        "parallelism": f"replicas x{world} (independent frames per GPU)" if world > 1 else "single GPU",
+        "parallelism": (f"one frame split over {world} GPUs (spp/{world} each, NCCL all-reduce of the image per frame)"
+                        if split else f"replicas x{world} (independent frames per GPU)" if world > 1 else "single GPU"),
         "parity": parity,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
@@ -936,7 +961,8 @@ def main():
                                     "the kernel runs on the second stream beside the next bounce's extend, so its "
                                     "duration includes SM time shared with that kernel"},
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": param_bytes, "d2h_bytes_per_step": W * H * 4},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": param_bytes,
+                "d2h_bytes_per_step": out_img.numel() * out_img.element_size()},
         "traversal": trav,
         "nrc": nrc_res,
         "gpu_launches": launches,
