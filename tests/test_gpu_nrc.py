@@ -17,9 +17,9 @@ BMIN = np.array([-1.0, -1.0, -1.0], np.float32)
 BMAX = np.array([2.0, 1.5, 1.0], np.float32)
 
 
-def make_nrc(seed=5, lr=1e-2):
+def make_nrc(seed=5, lr=1e-2, log2_t=LOG2_T):
     lib = abi.load()
-    cfg = abi.StrelkaNrcConfig((C.c_float * 3)(*BMIN), (C.c_float * 3)(*BMAX), lr, seed, LOG2_T, (C.c_uint32 * 3)())
+    cfg = abi.StrelkaNrcConfig((C.c_float * 3)(*BMIN), (C.c_float * 3)(*BMAX), lr, seed, log2_t, (C.c_uint32 * 3)())
     h = C.c_void_p()
     abi.check(lib.strelka_nrc_create(C.byref(cfg), C.byref(h)))
     nm = C.c_uint32()
@@ -73,8 +73,12 @@ def test_forward_matches_reference(cuda):
     lib.strelka_nrc_destroy(h)
 
 
-def test_gradients_match_reference(cuda):
-    lib, h, nm, ng = make_nrc(seed=9)
+@pytest.mark.parametrize("log2_t", [LOG2_T, 19])
+def test_gradients_match_reference(cuda, log2_t):
+    # 2^19 is the table of the radiance-cache workload: levels 0-3 dense,
+    # levels 4-15 hashed into 2^19 entries
+    lib, h, nm, ng = make_nrc(seed=9, log2_t=log2_t)
+    assert ng == 16 * (1 << log2_t) * 2
     rng = np.random.default_rng(1)
     mlp, _ = params(lib, h, nm, ng)
     grid = rng.normal(0, 0.3, ng).astype(np.float32)
@@ -85,7 +89,7 @@ def test_gradients_match_reference(cuda):
     loss = C.c_float()
     abi.check(lib.strelka_nrc_gradients(h, to_device(rec).data_ptr(), 2048, gm.ctypes.data, gg.ctypes.data,
                                         C.byref(loss), None))
-    rm, rg, rloss = nrc_ref.gradients(rec, mlp, grid, BMIN, BMAX, LOG2_T)
+    rm, rg, rloss = nrc_ref.gradients(rec, mlp, grid, BMIN, BMAX, log2_t)
     assert abs(loss.value - rloss) <= 1e-3 * abs(rloss)
     # per weight matrix: relative error of the gradient and its direction
     offs = [0, 4096, 8192, 12288, 16384, nm]
