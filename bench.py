@@ -291,6 +291,77 @@ def run_traversal(args):
     print(json.dumps(line), flush=True)
 
 
+def cornell_study(args, steps: int = 3, warmup: int = 1) -> dict:
+    """The Cornell box at 512x512, 1 spp per iteration x 64 iterations, depth
+    4, frameNumber = iteration, accumulated and tonemapped (ACESFitted) every
+    iteration: PathTracer::execute then the fused reduce + accumulate +
+    tonemap, as PtRender::drawFrame records them (ptrender.cpp:735-862).
+    One step is the whole 64-iteration sequence, timed with CUDA events.
+    The last step's accumulated and tonemapped images are compared with the
+    oracle's same chain."""
+    import torch
+
+    import oracle
+    from strelka_b200 import abi, scenes
+    from strelka_b200.render import DeviceScene, PathTracer, accumulation_param, resolve, tonemap_param
+
+    W = H = 512
+    iters = 64
+    s = scenes.cornell(W, H, sphere_levels=4)
+    ds = DeviceScene(s)
+    pt = PathTracer(mode=abi.MODE_WAVEFRONT)
+    npx = W * H
+    sb = torch.empty(npx * 3, dtype=torch.float32, device="cuda")
+    acc = [torch.zeros(npx * 4, dtype=torch.float32, device="cuda") for _ in range(2)]
+    tm = torch.empty(npx * 4, dtype=torch.float32, device="cuda")
+    tp = tonemap_param(W, H, 1)
+    stream = torch.cuda.current_stream()
+    params = [s.param(spp=1, maxDepth=4, frameNumber=it, iteration=it, stratifiedSamplingType=0) for it in range(iters)]
+    aps = [accumulation_param(W, H, it) for it in range(iters)]
+
+    def sequence():
+        for it in range(iters):
+            pt.execute(ds.desc(params[it], sb), npx, 1, it, stream)
+            resolve(params[it], sb, tp, aps[it], acc[it % 2], acc[(it + 1) % 2], tm, None, stream)
+
+    for _ in range(warmup):
+        sequence()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sequence()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    st = pt.device_status()
+    pt.close()
+    if st != 0:
+        raise RuntimeError(f"device status {st:#x}")
+    ms = statistics.median(times)
+    # the oracle's chain (pathtracerMdl.hlsl, reduction, accumulation, tonemap)
+    t0 = time.perf_counter()
+    view = oracle.SceneView(s)
+    hist = np.zeros(npx * 4, np.float32)
+    threads = os.cpu_count() or 1
+    for it in range(iters):
+        o = oracle.reduce(params[it], oracle.pathtrace(view, params[it], threads=threads))
+        hist = oracle.accumulate(aps[it], o, hist)
+    o_tm = oracle.tonemap(tp, hist)
+    o_s = time.perf_counter() - t0
+    g_acc = acc[iters % 2].cpu().numpy()
+    g_tm = tm.cpu().numpy()
+    rel = float(np.mean((g_acc.astype(np.float64) - hist) ** 2 / (hist.astype(np.float64) ** 2 + 1e-2)))
+    return {"workload": "Cornell box 512x512 (10,252 triangles), 1 spp x 64 iterations, depth 4, frameNumber = "
+                        "iteration, accumulation + ACESFitted every iteration",
+            "mpaths_s": npx * iters / (ms * 1e-3) / 1e6, "ms_per_64_iterations": ms, "steps": steps, "warmup": warmup,
+            "parity": {"relmse_accumulated": rel,
+                       "bit_exact_accumulated": float(np.mean(g_acc.view(np.uint32) == hist.view(np.uint32))),
+                       "bit_exact_tonemapped": float(np.mean(g_tm.view(np.uint32) == o_tm.view(np.uint32))),
+                       "oracle_seconds": round(o_s, 2)}}
+
+
 def hbm_peak():
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
@@ -726,7 +797,7 @@ def main():
                     help="N > 1: split every frame over the ranks (strong scaling) instead of independent frames")
     ap.add_argument("--no-studies", action="store_true",
                     help="skip the traversal microbenchmark and the radiance-cache study in the default run")
-    ap.add_argument("--workload", default="large", choices=["large", "traversal", "nrc", "nrc-mlp", "batch"])
+    ap.add_argument("--workload", default="large", choices=["large", "traversal", "nrc", "nrc-mlp", "batch", "cornell"])
     ap.add_argument("--batch-jobs", type=int, default=32)
     ap.add_argument("--batch-scenes", type=int, default=6)
     ap.add_argument("--batch-seed", type=int, default=0)
@@ -754,6 +825,15 @@ def main():
         return
     if args.workload == "nrc-mlp":
         run_nrc_mlp(args)
+        return
+    if args.workload == "cornell":
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        c = cornell_study(args, steps=args.steps, warmup=args.warmup)
+        print(json.dumps({"metric": "Mpaths/s (Cornell 512^2, 64 accumulated iterations)", "value": c["mpaths_s"],
+                          "unit": "Mpaths/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+                          "data": "synthetic", "config": {"workload": c["workload"]}, "detail": c}), flush=True)
         return
     if args.workload == "batch":
         run_batch(args)
@@ -922,9 +1002,10 @@ def main():
 
     # ---- the rest of the metric, one GPU: the traversal microbenchmark and
     # the radiance-cache time-to-equal-relMSE study ---------------------------
-    trav = nrc_res = None
+    trav = nrc_res = cornell = None
     if rank == 0 and world == 1 and not args.no_studies:
         trav = traversal_study(args, steps=10, warmup=3)
+        cornell = cornell_study(args)
         nrc_res = nrc_study(args, hs, ds)
 
     if dist:
@@ -964,6 +1045,7 @@ def main():
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": param_bytes,
                 "d2h_bytes_per_step": out_img.numel() * out_img.element_size()},
         "traversal": trav,
+        "cornell": cornell,
         "nrc": nrc_res,
         "gpu_launches": launches,
         "clocks": clk,
