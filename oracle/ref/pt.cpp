@@ -159,7 +159,9 @@ int strelka_ref_pathtrace(const ::PathTracerParam* p, const OracleScene* s, floa
 }
 
 /* closestHit / anyHit (raytracing.h:198-286) for n rays: hits[i] as the
- * shader's Hit record, found[i] the return value. */
+ * shader's Hit record, found[i] the return value.  On a miss the ids are
+ * 0xFFFFFFFF; closest hit then reports t = 1e9 and zero barycentrics, any
+ * hit the t its last triangle test wrote. */
 int strelka_ref_trace(const OracleScene* s, const ::Ray* rays, uint32_t n, ::Hit* hits, uint8_t* found, int anyHitMode,
                       int threads)
 {
@@ -175,10 +177,14 @@ int strelka_ref_trace(const OracleScene* s, const ::Ray* rays, uint32_t n, ::Hit
         h.t = 0.0f;
         bool f = anyHitMode ? ref_pt::anyHit(a, r, h) : ref_pt::closestHit(a, r, h);
         if (!f) {
-            h = ref_pt::Hit{};
-            h.t = anyHitMode ? 0.0f : 1e9f;
+            // the shader leaves the ids of a miss unset; any hit's t is the
+            // last triangle test's (its out parameter), closest hit's untouched
             h.instId = 0xFFFFFFFFu;
             h.primId = 0xFFFFFFFFu;
+            if (!anyHitMode) {
+                h.t = 1e9f;
+                h.bary = float2(0.0f);
+            }
         }
         memcpy(&hits[i], &h, sizeof(h));
         found[i] = f ? 1 : 0;

@@ -12,13 +12,12 @@ import pytest
 import oracle
 from gpu_util import bits_equal_fraction, relmse
 from strelka_b200 import abi, scenes
-from strelka_b200.render import DeviceScene, PathTracer
+from strelka_b200.render import DeviceScene, PathTracer, to_device
 
 pytestmark = pytest.mark.gpu
 
 RELMSE_BAR = 1e-4
 EXACT_BAR = 1.0        # every sample bit-identical to the oracle
-GOLDEN_EXACT_BAR = 0.999
 
 
 @pytest.fixture(scope="module")
@@ -124,6 +123,8 @@ def test_large_scene_small(cuda):
 
 
 def test_golden_fixture(cuda):
+    # the fixture is the reference's own shader code compiled on the host
+    # (tests/golden/make_golden.py); samples it leaves undefined are skipped
     import os
     path = os.path.join(os.path.dirname(__file__), "golden", "cornell_64x64.npz")
     gold = np.load(path)
@@ -131,6 +132,30 @@ def test_golden_fixture(cuda):
     ds = DeviceScene(s)
     p = s.param(spp=int(gold["spp"]), maxDepth=int(gold["max_depth"]), frameNumber=int(gold["frame"]),
                 stratifiedSamplingType=int(gold["sst"]))
-    g, _ = render(cuda, s, ds, p, abi.MODE_WAVEFRONT)
-    assert relmse(g, gold["samples"]) <= RELMSE_BAR
-    assert bits_equal_fraction(g, gold["samples"]) >= GOLDEN_EXACT_BAR
+    for mode in (abi.MODE_WAVEFRONT, abi.MODE_MEGAKERNEL):
+        g, _ = render(cuda, s, ds, p, mode)
+        defined = ~gold["undefined"]
+        got, ref = g.reshape(-1, 3)[defined], gold["samples"].reshape(-1, 3)[defined]
+        assert relmse(got, ref) <= RELMSE_BAR
+        assert bits_equal_fraction(got, ref) == EXACT_BAR
+
+
+def test_soup_golden_fixture(cuda):
+    # closest- and any-hit records of the reference's closestHit / anyHit
+    # (compiled on the host, tests/golden/make_golden.py), bit for bit
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_golden
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "soup_trace.npz"))
+    s, rays = make_golden.soup_inputs()
+    ds = DeviceScene(s)
+    pt = PathTracer()
+    n = rays.shape[0]
+    for flags, key in ((abi.TRACE_CLOSEST, "closest"), (abi.TRACE_ANY, "any")):
+        hits = cuda.zeros(n * 20, dtype=cuda.uint8, device="cuda")
+        pt.trace(ds.trace_desc(to_device(rays), hits, flags))
+        cuda.cuda.synchronize()
+        assert np.array_equal(hits.cpu().numpy().view(np.uint32).reshape(n, 5), gold[key]), key
+    assert pt.device_status() == 0
+    pt.close()
