@@ -24,7 +24,7 @@ PY=${PYTHON:-python3}
 mkdir -p _ref/src
 $PY hlsl2cpp.py "$REF/shaders" _ref/src
 FLAGS="-std=c++17 -O2 -ffp-contract=off -fno-fast-math -fwrapv -fopenmp -fPIC -Wall -Wno-unused-function \
-       -Wno-unused-variable -Wno-unused-but-set-variable -Wno-pedantic -I _ref/src -I ref -I ../include"
+       -Wno-unused-variable -Wno-unused-but-set-variable -Wno-pedantic -Wno-sign-compare -I _ref/src -I ref -I ../include"
 $CXX $FLAGS -c ref/pt.cpp -o _ref/pt.o
 $CXX $FLAGS -c ref/post.cpp -o _ref/post.o
 $CXX -shared -fopenmp -o _ref/libstrelka_ref.so _ref/pt.o _ref/post.o -L. -loracle -Wl,-rpath,'$ORIGIN/..' -lm
