@@ -125,29 +125,31 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(hs, args, budget_s: float):
-    """Times the oracle (fast build, all host threads) on evenly spread slices
-    of the frame's sample indices; returns Mpaths/s and the sample size."""
+def cpu_baseline(hs, args, budget_s: float, frame_number: int = 0):
+    """Times the oracle (fast build, all host threads) on 64 evenly spaced,
+    non-overlapping runs of the frame's sample indices.  A first pass of 64
+    paths per run calibrates the rate; the timed pass then renders as many
+    paths per run as fit `budget_s`.  Returns (Mpaths/s, paths, threads,
+    seconds)."""
     import oracle
 
     view = oracle.SceneView(hs)
-    p = hs.param(frameNumber=0)
+    p = hs.param(frameNumber=frame_number)
     total = args.width * args.height * args.spp
     threads = os.cpu_count() or 1
     slices = 64
-    per = 64
-    oracle.pathtrace(view, p, threads=threads, first=0, count=per, fast=True)  # warm-up
-    t0 = time.perf_counter()
-    done = 0
-    while True:
+
+    def run(per):
+        t = time.perf_counter()
         for k in range(slices):
-            first = (k * total) // slices
-            oracle.pathtrace(view, p, threads=threads, first=first, count=per, fast=True)
-            done += per
-        el = time.perf_counter() - t0
-        if el > budget_s or done >= total:
-            break
-        per = min(per * 2, total // slices)
+            oracle.pathtrace(view, p, threads=threads, first=(k * total) // slices, count=per, fast=True)
+        return time.perf_counter() - t
+
+    cal = 64
+    rate = slices * cal / max(run(cal), 1e-6)
+    per = int(min(max(rate * budget_s / slices, cal), total // slices))
+    el = run(per)
+    done = slices * per
     return done / el / 1e6, done, threads, el
 
 
