@@ -311,7 +311,7 @@ def cornell_study(args, steps: int = 3, warmup: int = 1) -> dict:
     iters = 64
     s = scenes.cornell(W, H, sphere_levels=4)
     ds = DeviceScene(s)
-    pt = PathTracer(mode=abi.MODE_WAVEFRONT)
+    pt = PathTracer(mode=abi.MODE_WAVEFRONT if args.mode == "wavefront" else abi.MODE_MEGAKERNEL)
     npx = W * H
     sb = torch.empty(npx * 3, dtype=torch.float32, device="cuda")
     acc = [torch.zeros(npx * 4, dtype=torch.float32, device="cuda") for _ in range(2)]
@@ -356,7 +356,7 @@ def cornell_study(args, steps: int = 3, warmup: int = 1) -> dict:
     g_tm = tm.cpu().numpy()
     rel = float(np.mean((g_acc.astype(np.float64) - hist) ** 2 / (hist.astype(np.float64) ** 2 + 1e-2)))
     return {"workload": "Cornell box 512x512 (10,252 triangles), 1 spp x 64 iterations, depth 4, frameNumber = "
-                        "iteration, accumulation + ACESFitted every iteration",
+                        "iteration, accumulation + ACESFitted every iteration", "mode": args.mode,
             "mpaths_s": npx * iters / (ms * 1e-3) / 1e6, "ms_per_64_iterations": ms, "steps": steps, "warmup": warmup,
             "parity": {"relmse_accumulated": rel,
                        "bit_exact_accumulated": float(np.mean(g_acc.view(np.uint32) == hist.view(np.uint32))),
