@@ -41,17 +41,20 @@ if ROOT not in sys.path:
 METRIC = "Mpaths/s at 1080p"
 UNIT = "Mpaths/s"
 
-# DRAM bytes (read + write) per closest-hit query of the extend kernel on this
-# workload, from one ncu capture of a full frame's 5 extend launches
-# (dram__bytes_read.sum + dram__bytes_write.sum = 18.40 GB for 68.87M rays).
-# bench.py cannot run ncu itself, so
-# roofline.traffic is this figure times the rays of an average launch.
-EXTEND_DRAM_BYTES_PER_RAY = 267.2
+# DRAM bytes (read + write) per closest-hit query of the extend kernel on the
+# large scene, from one ncu capture of the five extend launches of a
+# 960x540 x 4 spp frame (dram__bytes_read.sum + dram__bytes_write.sum =
+# 1693.1 MB for 4,300,568 queries).  The per-query figure falls as the frame
+# grows (481 B per query at 480x270 x 4 spp): more queries share the cached
+# nodes.  bench.py cannot run ncu itself, so roofline.traffic is this figure
+# times the queries of an average launch, an upper bound for the full frame.
+EXTEND_DRAM_BYTES_PER_RAY = 393.7
 
 # DRAM bytes (read + write) per closest-hit query of the ray-query kernel on
-# the 1M-triangle soup with 4M rays, from one ncu capture of a timed launch
-# (dram__bytes_read.sum + dram__bytes_write.sum = 2.160 + 0.165 GB).
-TRACE_SOUP_DRAM_BYTES_PER_RAY = 581.4
+# the 1M-triangle soup, from one ncu capture of a timed launch with 4M rays
+# (1693.7 + 157.9 MB); 458.6 B per query with 1M rays, so the figure scales
+# with the number of rays.
+TRACE_SOUP_DRAM_BYTES_PER_RAY = 462.9
 
 # Bytes a traversal reads per 4-wide node it processes: the bounds of its four
 # entries (6 float4) and their refs (1 float4).
@@ -288,7 +291,7 @@ def run_traversal(args):
                          "frac": c["frac"],
                          "traffic": (TRACE_SOUP_DRAM_BYTES_PER_RAY * tr["rays"]
                                      if (args.tris, args.rays) == (1_000_000, 4_000_000) else None),
-                         "traffic_source": "ncu DRAM bytes of one closest-hit launch on the default soup"},
+                         "traffic_source": "ncu DRAM bytes per query of one closest-hit launch with 4M rays x rays"},
             "detail": tr, "clocks": tr["clocks"]}
     print(json.dumps(line), flush=True)
 
@@ -1030,7 +1033,8 @@ def main():
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": EXTEND_DRAM_BYTES_PER_RAY * cnt["extend_rays"] / max(ext_launches, 1)
                      if args.width == 1920 and args.height == 1080 and args.spp == 16 else None,
-                     "traffic_source": "ncu DRAM bytes per ray of a full-frame capture x rays per launch",
+                     "traffic_source": "ncu DRAM bytes per query of a 960x540x4 frame's extend launches x queries per "
+                                       "launch (an upper bound: the per-query figure falls as the frame grows)",
                      "bytes_alg_per_launch": bytes_alg / max(ext_launches, 1),
                      "kernel": "extend (closest-hit traversal)", "peak_source": peak_src,
                      "bytes_alg_timed_region": bytes_alg, "kernel_ms_timed_region": ext_ms,

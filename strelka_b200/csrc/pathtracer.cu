@@ -405,13 +405,14 @@ __global__ void __launch_bounds__(kExtendBlock, SB_EXTEND_MINBLOCKS) k_extend(De
     WarpPool pool{0, 0, 0};
     uint32_t slot = 0;
     Trav T;
+    const uint32_t root = trav_root(s);
     bool have = false;
     while (true) {
         const uint32_t i = pool_take(pool, &w.counters[3], count, chunk, !have);
         if (!have && i != SB_INVALID) {
             slot = q[i];
             const float4 o = w.ray_o[slot], d = w.ray_d[slot];
-            trav_init(s, T, xyz(o), o.w, xyz(d), false);
+            trav_init_root(T, xyz(o), o.w, xyz(d), false, root);
             have = true;
         }
         if (!__any_sync(0xffffffffu, have)) break;
@@ -672,13 +673,14 @@ __global__ void __launch_bounds__(kExtendBlock, SB_SHADOW_MINBLOCKS) k_shadow(De
     WarpPool pool{0, 0, 0};
     uint32_t item = 0;
     Trav T;
+    const uint32_t root = trav_root(s);
     bool have = false;
     while (true) {
         const uint32_t i = pool_take(pool, &w.counters[5], count, chunk, !have);
         if (!have && i != SB_INVALID) {
             item = i;
             const float4 o = w.sh_o[i], d = w.sh_d[i];
-            trav_init(s, T, xyz(o), o.w, xyz(d), true);
+            trav_init_root(T, xyz(o), o.w, xyz(d), true, root);
             have = true;
         }
         if (!__any_sync(0xffffffffu, have)) break;
@@ -882,13 +884,14 @@ __global__ void __launch_bounds__(kExtendBlock, ANY ? 9 : 8) k_trace(DevScene s,
     WarpPool pool{0, 0, 0};
     uint32_t i = 0;
     Trav T;
+    const uint32_t root = trav_root(s);
     bool have = false;
     while (true) {
         const uint32_t got = pool_take(pool, head, n, chunk, !have);
         if (!have && got != SB_INVALID) {
             i = got;
             const float4 o = __ldg(&rays[2 * (size_t)i]), d = __ldg(&rays[2 * (size_t)i + 1]);
-            trav_init(s, T, xyz(o), o.w, xyz(d), ANY);
+            trav_init_root(T, xyz(o), o.w, xyz(d), ANY, root);
             have = true;
         }
         if (!__any_sync(0xffffffffu, have)) break;

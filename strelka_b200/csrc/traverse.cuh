@@ -212,8 +212,13 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, v3 o, float tmax, v
 // A child's box test passing implies its parent's (the slab arithmetic
 // rounds monotonically and a parent box contains its children's), so testing
 // only the even-depth boxes leaves the set of triangles a query tests
-// exactly the reference's.  One step reads one 4-wide node (112 bytes) and
-// tests four boxes: half the dependent fetches of a binary traversal.
+// exactly the reference's.  One step reads one 4-wide node (112 bytes, with
+// four 256-bit loads of its 128-byte line) and tests four boxes: half the
+// dependent fetches of a binary traversal.  The slab subtractions and
+// products of the four boxes run as packed pairs (sub/mul.rn.f32x2, each
+// half rounded exactly as the scalar instruction), and the ray's reciprocal
+// direction is __frcp_rn, the correctly rounded 1/x, so every value equals
+// the reference's expression evaluated in single precision.
 //
 // Closest hit tests all entry boxes, then the leaves that passed, continues
 // with the nearest passing inner entry and keeps the others on a per-thread
@@ -248,7 +253,9 @@ __device__ __forceinline__ RayQ make_ray(v3 o, float tmax, v3 d)
     r.o = o;
     r.d = d;
     r.tmax = tmax;
-    r.inv = V(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    // __frcp_rn is the reciprocal correctly rounded to nearest: the value of
+    // the IEEE division 1.0f / x for every x (zeros, infinities, subnormals)
+    r.inv = V(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
     return r;
 }
 
@@ -393,6 +400,27 @@ struct Trav {
     HitRec hit;
 };
 
+// The traversal's first entry: the 4-wide root, the root leaf, or nothing.
+__device__ __forceinline__ uint32_t trav_root(const DevScene& s)
+{
+    if (!s.numNodes) return SB_INVALID;
+    return __float_as_uint(__ldg(&s.nodes[0]).w) != SB_INVALID ? (SB_LEAF_BIT | SB_NOBOX_BIT) : 0u;
+}
+__device__ __forceinline__ void trav_init_root(Trav& T, v3 o, float tmax, v3 d, bool any, uint32_t root)
+{
+    T.r = make_ray(o, tmax, d);
+    T.minHit = 1e9f;
+    T.leaf = SB_INVALID;
+    T.sp = 0;
+    T.steps = 0;
+    T.found = false;
+    T.hit.u = 0.0f;
+    T.hit.v = 0.0f;
+    T.hit.t = any ? 0.0f : 1e9f;
+    T.hit.instId = SB_INVALID;
+    T.hit.primId = SB_INVALID;
+    T.cur = root;
+}
 __device__ __forceinline__ void trav_init(const DevScene& s, Trav& T, v3 o, float tmax, v3 d, bool any)
 {
     T.r = make_ray(o, tmax, d);
@@ -416,34 +444,91 @@ struct WideNode {
     float4 lx, ly, lz, hx, hy, hz;
     uint32_t ref[4];
 };
+// Two float4 from one 32-byte-aligned address with one 256-bit read-only load.
+__device__ __forceinline__ void ldg_pair(const float4* p, float4& a, float4& b)
+{
+    const size_t g = __cvta_generic_to_global(p);
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(g));
+}
+// A 4-wide node (128 bytes, 128-byte aligned) in four 256-bit loads.
 __device__ __forceinline__ WideNode load_wide(const DevScene& s, uint32_t w)
 {
     const float4* p = &s.wide[8 * (size_t)w];
     WideNode n;
-    n.lx = __ldg(p);
-    n.ly = __ldg(p + 1);
-    n.lz = __ldg(p + 2);
-    n.hx = __ldg(p + 3);
-    n.hy = __ldg(p + 4);
-    n.hz = __ldg(p + 5);
-    const float4 rf = __ldg(p + 6);
+    float4 rf, pad;
+    ldg_pair(p, n.lx, n.ly);
+    ldg_pair(p + 2, n.lz, n.hx);
+    ldg_pair(p + 4, n.hy, n.hz);
+    ldg_pair(p + 6, rf, pad);
+    (void)pad;
     n.ref[0] = __float_as_uint(rf.x);
     n.ref[1] = __float_as_uint(rf.y);
     n.ref[2] = __float_as_uint(rf.z);
     n.ref[3] = __float_as_uint(rf.w);
     return n;
 }
-__device__ __forceinline__ float4 comp4(float4 v, int k)
+// Packed pairs of floats (sm_100 f32x2 arithmetic: each half rounded as the
+// scalar instruction would round it).
+__device__ __forceinline__ unsigned long long f2pack(float a, float b)
 {
-    return make_float4(k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w, 0.0f, 0.0f, 0.0f);
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
 }
-// box of entry k, tested with the reference's slab arithmetic
-__device__ __forceinline__ bool wide_box(const RayQ& r, const WideNode& n, int k, float& t)
+__device__ __forceinline__ void f2unpack(unsigned long long v, float& a, float& b)
 {
-    const float4 lo = make_float4(comp4(n.lx, k).x, comp4(n.ly, k).x, comp4(n.lz, k).x, 0.0f);
-    const float4 hi = make_float4(comp4(n.hx, k).x, comp4(n.hy, k).x, comp4(n.hz, k).x, 0.0f);
-    return ray_box(r.o, r.inv, lo, hi, t);
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
 }
+__device__ __forceinline__ unsigned long long f2sub(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long f2mul(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+// (b[k] - o) * inv for the four entries k of one bound row
+__device__ __forceinline__ void slab4(float4 b, unsigned long long oo, unsigned long long ii, float t[4])
+{
+    f2unpack(f2mul(f2sub(f2pack(b.x, b.y), oo), ii), t[0], t[1]);
+    f2unpack(f2mul(f2sub(f2pack(b.z, b.w), oo), ii), t[2], t[3]);
+}
+// The four entry boxes of a 4-wide node with the reference's slab arithmetic
+// (ray.h:35-48): t0[k] the entry distance, bit k of the result whether box k is hit.
+__device__ __forceinline__ unsigned wide_boxes(const RayQ& r, const WideNode& n, float t0[4])
+{
+    float fx[4], fy[4], fz[4], nx[4], ny[4], nz[4];
+    {
+        const unsigned long long ox = f2pack(r.o.x, r.o.x), ix = f2pack(r.inv.x, r.inv.x);
+        slab4(n.hx, ox, ix, fx);
+        slab4(n.lx, ox, ix, nx);
+    }
+    {
+        const unsigned long long oy = f2pack(r.o.y, r.o.y), iy = f2pack(r.inv.y, r.inv.y);
+        slab4(n.hy, oy, iy, fy);
+        slab4(n.ly, oy, iy, ny);
+    }
+    {
+        const unsigned long long oz = f2pack(r.o.z, r.o.z), iz = f2pack(r.inv.z, r.inv.z);
+        slab4(n.hz, oz, iz, fz);
+        slab4(n.lz, oz, iz, nz);
+    }
+    unsigned m = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float t1 = fminf(fmaxf(fx[k], nx[k]), fminf(fmaxf(fy[k], ny[k]), fmaxf(fz[k], nz[k])));
+        t0[k] = fmaxf(fmaxf(fminf(fx[k], nx[k]), fmaxf(fminf(fy[k], ny[k]), fminf(fz[k], nz[k]))), 0.0f);
+        if (t1 >= t0[k]) m |= 1u << k;
+    }
+    return m;
+}
+
 __device__ __forceinline__ void cswap(float& ta, uint32_t& ra, float& tb, uint32_t& rb)
 {
     if (tb < ta) {
@@ -508,12 +593,13 @@ __device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, uint32_
             {
                 const WideNode n = load_wide(s, cur);
                 const float lim0 = T.minHit * SB_PRUNE_SCALE;
+                const unsigned hitm = wide_boxes(T.r, n, bt);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     ref[k] = n.ref[k];
-                    bt[k] = 0.0f;
                     pass[k] = ref[k] != SB_INVALID &&
-                              ((ref[k] & SB_NOBOX_BIT) || (wide_box(T.r, n, k, bt[k]) && !(bt[k] > T.r.tmax) && !(bt[k] > lim0)));
+                              ((ref[k] & SB_NOBOX_BIT) || (((hitm >> k) & 1u) && !(bt[k] > T.r.tmax) && !(bt[k] > lim0)));
+                    if (ref[k] & SB_NOBOX_BIT) bt[k] = 0.0f;
                 }
             }
             float ct[4];
@@ -599,12 +685,13 @@ __device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, uint32_t* s
         bool pass[4];
         {
             const WideNode n = load_wide(s, cur);
+            float bt[4];
+            const unsigned hitm = wide_boxes(T.r, n, bt);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 ref[k] = n.ref[k];
-                float bt = 0.0f;
                 pass[k] = ref[k] != SB_INVALID &&
-                          ((ref[k] & SB_NOBOX_BIT) || (wide_box(T.r, n, k, bt) && !(bt > T.r.tmax)));
+                          ((ref[k] & SB_NOBOX_BIT) || (((hitm >> k) & 1u) && !(bt[k] > T.r.tmax)));
             }
         }
         uint32_t first = SB_INVALID;
