@@ -85,6 +85,7 @@ def load(fast: bool = False) -> C.CDLL:
         "oracle_intersect_ray_box": (C.c_int, [vp, vp, vp, vp, C.POINTER(f32)]),
         "oracle_ray_triangle": (C.c_int, [vp, vp, vp, vp, vp, C.POINTER(f32), C.POINTER(f32), C.POINTER(f32)]),
         "oracle_trace": (C.c_int, [C.POINTER(OracleScene), vp, u32, vp, vp, C.c_int, C.c_int, vp, C.c_int]),
+        "oracle_trace_warp": (C.c_int, [C.POINTER(OracleScene), vp, u32, vp, vp, vp]),
         "oracle_intersect_fp64": (C.c_int, [C.POINTER(OracleScene), vp, vp, vp, u32, vp, vp, vp]),
         "oracle_intersect_terms_fp64": (C.c_int, [C.POINTER(OracleScene), vp, vp, vp, u32, vp]),
         "oracle_pathtrace": (C.c_int, [vp, C.POINTER(OracleScene), vp, C.c_int]),
@@ -160,6 +161,21 @@ def trace(view: SceneView, rays: np.ndarray, any_hit: bool = False, prune: bool 
     counters = np.zeros(2, np.uint64)
     lib.oracle_trace(C.byref(view.scene), _ptr(rays), n, _ptr(hits), _ptr(found), 1 if any_hit else 0,
                      int(prune), _ptr(counters), threads)
+    return hits, found.astype(bool), counters
+
+
+def trace_warp(view: SceneView, rays: np.ndarray):
+    """The closest-hit kernels' deferred leaf tests replayed for one warp that
+    takes all n rays from one work chunk: (hits (n,5) uint32, found (n,) bool,
+    counters (2,) uint64 = 4-wide nodes processed, triangle tests)."""
+    lib = load()
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = rays.shape[0]
+    hits = np.zeros((n, 5), np.uint32)
+    found = np.zeros(n, np.uint8)
+    counters = np.zeros(2, np.uint64)
+    if lib.oracle_trace_warp(C.byref(view.scene), _ptr(rays), n, _ptr(hits), _ptr(found), _ptr(counters)) != 0:
+        raise MemoryError("oracle_trace_warp")
     return hits, found.astype(bool), counters
 
 

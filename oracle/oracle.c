@@ -729,6 +729,191 @@ static int wide_any(const OracleScene* s, v3 o, float tmax, v3 d, Hit* hit, unsi
     }
 }
 
+/* The GPU's closest-hit kernels with deferred leaf tests (csrc/traverse.cuh:
+ * closest_defer_*), replayed for ONE warp of 32 lanes that takes every ray of
+ * [0, n) from one work chunk, as the kernels do when the queue chunk is at
+ * least n.  Per warp iteration:
+ *   1. lanes without a query take the next rays in lane order;
+ *   2. when at least DEFER_LANES lanes have pending leaves, or a lane with
+ *      pending leaves has nothing current or fewer than 4 free slots, every
+ *      lane with pending leaves tests its latest one;
+ *   3. each lane with a query processes its current node when it has room
+ *      for four more pending leaves (passing leaves join the list, inner
+ *      candidates as in wide_closest), then pops when nothing is current,
+ *      and finishes when nothing is current and no leaf is pending.
+ * Results equal wide_closest's; the node and test counts are the warp's. */
+#define DEFER_CAP 12
+#define DEFER_LANES 16
+typedef struct {
+    int have, done;
+    uint32_t ray;
+    v3 o, d;
+    float inv[3], oo[3], tmax, minHit;
+    uint32_t best, cur, steps;
+    int sp, np, found;
+    uint32_t stackN[WIDE_STACK];
+    float stackT[WIDE_STACK];
+    uint32_t pend[DEFER_CAP];
+    Hit hit;
+} WarpLane;
+
+static void warp_leaf(const OracleScene* s, WarpLane* L, uint32_t leaf)
+{
+    float t, bu = 0, bv = 0;
+    uint32_t iid, pid;
+    if (leaf_test(s, leaf, L->o, L->d, &t, &bu, &bv, &iid, &pid) && t < L->tmax &&
+        (t < L->minHit || (t == L->minHit && leaf < L->best))) {
+        L->minHit = t;
+        L->best = leaf;
+        L->hit.t = t; L->hit.bary[0] = bu; L->hit.bary[1] = bv; L->hit.instId = iid; L->hit.primId = pid;
+        L->found = 1;
+    }
+}
+
+/* closest_defer_node: returns 1 when the query ended early */
+static int warp_node(const OracleScene* s, WarpLane* L, unsigned long long* nI, unsigned long long* nL)
+{
+    uint32_t cur = L->cur;
+    if (++L->steps > s->numNodes + 1u) return 1;
+    if (cur & W_LEAF) {
+        L->pend[L->np++] = cur & ~(W_LEAF | W_NOBOX);
+        L->cur = INVALID_INDEX;
+        return 0;
+    }
+    if (cur >= s->numNodes) return 1;
+    (*nI)++;
+    uint32_t ref[4], gate[4];
+    wide_entries(s, cur, ref, gate);
+    float lim0 = L->minHit * PRUNE_SCALE, ct[4];
+    uint32_t cr[4];
+    for (int k = 0; k < 4; ++k) {
+        ct[k] = INFINITY;
+        cr[k] = INVALID_INDEX;
+        if (ref[k] == INVALID_INDEX) continue;
+        float bt = 0.0f;
+        int pass = 1;
+        if (!(ref[k] & W_NOBOX)) {
+            const BVHNode* b = &s->nodes[gate[k]];
+            pass = oracle_intersect_ray_box(L->oo, L->inv, b->minBounds, b->maxBounds, &bt) && !(bt > L->tmax) && !(bt > lim0);
+        }
+        if (!pass) continue;
+        if (ref[k] & W_LEAF) {
+            L->pend[L->np++] = ref[k] & ~(W_LEAF | W_NOBOX);
+        } else {
+            ct[k] = bt;
+            cr[k] = ref[k];
+        }
+    }
+    wide_cswap(ct, cr, 0, 1);
+    wide_cswap(ct, cr, 2, 3);
+    wide_cswap(ct, cr, 0, 2);
+    wide_cswap(ct, cr, 1, 3);
+    wide_cswap(ct, cr, 1, 2);
+    L->cur = cr[0];
+    for (int k = 3; k >= 1; --k) {
+        if (cr[k] == INVALID_INDEX) continue;
+        if (L->sp < WIDE_STACK) {
+            L->stackN[L->sp] = cr[k];
+            L->stackT[L->sp] = ct[k];
+            L->sp++;
+        } else {
+            stackless_closest_from(s, L->o, L->tmax, L->d, L->inv, 0, &L->minHit, &L->best, &L->hit, &L->found, nI, nL);
+            L->cur = INVALID_INDEX;
+            L->sp = 0;
+            return 1;
+        }
+    }
+    return 0;
+}
+
+int oracle_trace_warp(const OracleScene* s, const Ray* rays, uint32_t n, Hit* hits, uint8_t* found,
+                      unsigned long long* counters)
+{
+    WarpLane* lane = (WarpLane*)calloc(32, sizeof(WarpLane));
+    if (!lane) return -1;
+    unsigned long long nI = 0, nL = 0;
+    const uint32_t root = s->numNodes == 0 ? INVALID_INDEX : node_is_leaf(s, 0) ? (W_LEAF | W_NOBOX) : 0;
+    uint32_t next = 0;
+    for (;;) {
+        /* 1. new queries, in lane order */
+        for (int l = 0; l < 32; ++l) {
+            WarpLane* L = &lane[l];
+            if (L->have || next >= n) continue;
+            const Ray* r = &rays[next];
+            memset(L, 0, sizeof(*L));
+            L->have = 1;
+            L->ray = next++;
+            L->o = V(r->o.x, r->o.y, r->o.z);
+            L->d = V(r->d.x, r->d.y, r->d.z);
+            L->oo[0] = r->o.x; L->oo[1] = r->o.y; L->oo[2] = r->o.z;
+            L->inv[0] = 1.0f / r->d.x; L->inv[1] = 1.0f / r->d.y; L->inv[2] = 1.0f / r->d.z;
+            L->tmax = r->o.w;
+            L->minHit = 1e9f;
+            L->best = INVALID_INDEX;
+            L->cur = root;
+            L->hit.t = 1e9f;
+            L->hit.instId = INVALID_INDEX;
+            L->hit.primId = INVALID_INDEX;
+        }
+        int any = 0;
+        for (int l = 0; l < 32; ++l) any |= lane[l].have;
+        if (!any) break;
+        /* 2. deferred leaf tests */
+        int waiting = 0, stuck = 0;
+        for (int l = 0; l < 32; ++l) {
+            WarpLane* L = &lane[l];
+            if (!L->have || !L->np) continue;
+            waiting++;
+            if (L->cur == INVALID_INDEX || L->np > DEFER_CAP - 4) stuck = 1;
+        }
+        if (waiting && (waiting >= DEFER_LANES || stuck)) {
+            for (int l = 0; l < 32; ++l) {
+                WarpLane* L = &lane[l];
+                if (!L->have || !L->np) continue;
+                L->np--;
+                nL++;
+                warp_leaf(s, L, L->pend[L->np]);
+            }
+        }
+        /* 3. node step, pop, finish */
+        for (int l = 0; l < 32; ++l) {
+            WarpLane* L = &lane[l];
+            if (!L->have) continue;
+            int fin = 0;
+            if (L->cur != INVALID_INDEX && L->np <= DEFER_CAP - 4) {
+                fin = warp_node(s, L, &nI, &nL);
+                if (fin) L->np = 0;
+            }
+            if (!fin && L->cur == INVALID_INDEX) {
+                float lim = L->minHit * PRUNE_SCALE;
+                while (L->sp > 0) {
+                    --L->sp;
+                    if (!(L->stackT[L->sp] > lim)) {
+                        L->cur = L->stackN[L->sp];
+                        break;
+                    }
+                }
+            }
+            if (!fin && !(L->cur == INVALID_INDEX && L->np == 0)) continue;
+            Hit h = L->hit;
+            if (!L->found) {
+                h.instId = INVALID_INDEX;
+                h.primId = INVALID_INDEX;
+                h.t = 1e9f;
+                h.bary[0] = 0.0f;
+                h.bary[1] = 0.0f;
+            }
+            hits[L->ray] = h;
+            if (found) found[L->ray] = (uint8_t)L->found;
+            L->have = 0;
+        }
+    }
+    free(lane);
+    counters[0] = nI;
+    counters[1] = nL;
+    return 0;
+}
+
 int oracle_trace(const OracleScene* s, const Ray* rays, uint32_t n, Hit* hits, uint8_t* found, int mode,
                  int prune, unsigned long long* counters, int nthreads)
 {

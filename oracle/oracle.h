@@ -96,6 +96,14 @@ int oracle_ray_triangle(const float o[3], const float d[3], const float v0[3], c
 int oracle_trace(const OracleScene* s, const Ray* rays, uint32_t n, Hit* hits, uint8_t* found,
                  int mode, int prune, unsigned long long* counters, int nthreads);
 
+/* The GPU's closest-hit kernels with deferred leaf tests, replayed for one
+ * warp that takes every ray of [0, n) from one work chunk (the kernels run
+ * that way when their queue chunk is at least n).  Hits and found as
+ * oracle_trace (equal to its results); counters gets the warp's {4-wide
+ * nodes processed, triangle tests}. */
+int oracle_trace_warp(const OracleScene* s, const Ray* rays, uint32_t n, Hit* hits, uint8_t* found,
+                      unsigned long long* counters);
+
 /* FP64 Möller–Trumbore of ray i against triangle (instId[i], primId[i]),
  * same formula as raytracing.h:36-88 evaluated in double (no thresholds). */
 int oracle_intersect_fp64(const OracleScene* s, const Ray* rays, const uint32_t* instIds,

@@ -406,6 +406,9 @@ __global__ void __launch_bounds__(kExtendBlock, SB_EXTEND_MINBLOCKS) k_extend(De
     uint32_t slot = 0;
     Trav T;
     const uint32_t root = trav_root(s);
+    __shared__ uint32_t sPend[SB_DEFER_CAP * kExtendBlock];  // deferred leaf tests
+    uint32_t* pend = &sPend[threadIdx.x];
+    uint32_t np = 0;
     bool have = false;
     while (true) {
         const uint32_t i = pool_take(pool, &w.counters[3], count, chunk, !have);
@@ -413,12 +416,13 @@ __global__ void __launch_bounds__(kExtendBlock, SB_EXTEND_MINBLOCKS) k_extend(De
             slot = q[i];
             const float4 o = w.ray_o[slot], d = w.ray_d[slot];
             trav_init_root(T, xyz(o), o.w, xyz(d), false, root);
+            np = 0;
             have = true;
         }
         if (!__any_sync(0xffffffffu, have)) break;
+        closest_defer_leaves<COUNT, kExtendBlock>(s, T, have, pend, np, nL);
         if (!have) continue;
-        const bool done = T.cur == SB_INVALID || closest_step<COUNT>(s, T, stackN, stackT, nI, nL);
-        if (!done) continue;
+        if (!closest_defer_step<COUNT, kExtendBlock>(s, T, stackN, stackT, pend, np, nI, nL)) continue;
         w.hit[slot] = T.found ? make_float4(T.hit.u, T.hit.v, T.hit.t, __uint_as_float(T.hit.instId))
                               : make_float4(0.0f, 0.0f, 1e9f, __uint_as_float(SB_INVALID));
         w.hitPrim[slot] = T.found ? T.hit.primId : SB_INVALID;
@@ -885,6 +889,9 @@ __global__ void __launch_bounds__(kExtendBlock, ANY ? 9 : 8) k_trace(DevScene s,
     uint32_t i = 0;
     Trav T;
     const uint32_t root = trav_root(s);
+    __shared__ uint32_t sPend[ANY ? 1 : SB_DEFER_CAP * kExtendBlock];  // deferred leaf tests (closest hit)
+    uint32_t* pend = &sPend[ANY ? 0 : threadIdx.x];
+    uint32_t np = 0;
     bool have = false;
     while (true) {
         const uint32_t got = pool_take(pool, head, n, chunk, !have);
@@ -892,12 +899,24 @@ __global__ void __launch_bounds__(kExtendBlock, ANY ? 9 : 8) k_trace(DevScene s,
             i = got;
             const float4 o = __ldg(&rays[2 * (size_t)i]), d = __ldg(&rays[2 * (size_t)i + 1]);
             trav_init_root(T, xyz(o), o.w, xyz(d), ANY, root);
+            np = 0;
             have = true;
         }
         if (!__any_sync(0xffffffffu, have)) break;
+        if (!ANY) closest_defer_leaves<COUNT, kExtendBlock>(s, T, have, pend, np, nL);
         if (!have) continue;
-        const bool done = T.cur == SB_INVALID || (ANY ? any_step<COUNT>(s, T, stackN, nI, nL)
-                                                      : closest_step<COUNT>(s, T, stackN, stackT, nI, nL));
+        bool done;
+        if (ANY) {
+            done = T.cur == SB_INVALID || any_step<COUNT>(s, T, stackN, nI, nL);
+        } else {
+            bool fin = false;
+            if (T.cur != SB_INVALID && np <= SB_DEFER_CAP - 4) {
+                fin = closest_defer_node<COUNT, kExtendBlock>(s, T, stackN, stackT, pend, np, nI, nL);
+                if (fin) np = 0;
+            }
+            if (!fin && T.cur == SB_INVALID) closest_pop(T, stackN, stackT);
+            done = fin || (T.cur == SB_INVALID && np == 0);
+        }
         if (!done) continue;
         HitRec h = T.hit;
         if (REFINE && T.found) {

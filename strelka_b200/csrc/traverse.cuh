@@ -665,6 +665,159 @@ __device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, uint32_
     return false;
 }
 
+// ---------------------------------------------------------------------------
+// Closest hit with leaf tests deferred and run together across the warp.
+//
+// A triangle test is about 70 instructions and a node step finds a passing
+// leaf only about once in three, so testing leaves at the node that reaches
+// them runs the test code with a few lanes of the warp active.  Here the
+// passing leaves of a node join the thread's pending list (SB_DEFER_CAP
+// entries in shared memory; entry j of a thread at pend[j * STRIDE]), the
+// traversal goes on with the nearest inner entry, and every lane that waits
+// tests its latest pending leaf when at least SB_DEFER_LANES lanes of the
+// warp wait, or when a waiting lane cannot go on (nothing left to traverse,
+// or no room for another node's leaves).  Pruning uses the best hit known at
+// the time, which is never closer than the one the immediate order would
+// know, so no subtree holding the closest hit is dropped; the tie rule on
+// compact leaf indices makes the result independent of the test order.  The
+// results are the reference's bit for bit; the nodes and tests counted depend
+// on the warp's mix of rays.
+#ifndef SB_DEFER_CAP
+#define SB_DEFER_CAP 12
+#endif
+#ifndef SB_DEFER_LANES
+#define SB_DEFER_LANES 16
+#endif
+
+// Pops until an entry within the best hit is found (T.cur stays SB_INVALID
+// when the stack runs out).
+__device__ __forceinline__ void closest_pop(Trav& T, const uint32_t* stackN, const float* stackT)
+{
+    const float lim = T.minHit * SB_PRUNE_SCALE;
+    while (T.sp > 0) {
+        --T.sp;
+        if (!(stackT[T.sp] > lim)) {
+            T.cur = stackN[T.sp];
+            return;
+        }
+    }
+}
+
+// One node of the deferred traversal (T.cur is a 4-wide node or the root
+// leaf; the caller guarantees room for four more pending leaves): passing
+// leaves join the pending list, the nearest passing inner entry is next and
+// the others go onto the stack, farthest first.  Returns true when the
+// traversal ended early (a fault, the step cap, or the stackless fallback,
+// which tests every leaf itself, pending ones included).
+template <bool COUNT, int STRIDE>
+__device__ __forceinline__ bool closest_defer_node(const DevScene& s, Trav& T, uint32_t* stackN, float* stackT, uint32_t* pend,
+                                                   uint32_t& np, uint32_t& nInner, uint32_t& nLeaf)
+{
+    const uint32_t cur = T.cur;
+    if (++T.steps > s.numNodes + 1u) {
+        raise_status(s, STRELKA_DEV_TRAVERSAL_CAP);
+        return true;
+    }
+    if (cur & SB_LEAF_BIT) {
+        pend[(np++) * STRIDE] = cur & ~(SB_LEAF_BIT | SB_NOBOX_BIT);
+        T.cur = SB_INVALID;
+        return false;
+    }
+    if (cur >= s.numWide) {
+        raise_status(s, STRELKA_DEV_NODE_OOB);
+        return true;
+    }
+    if (COUNT) ++nInner;
+    float ct[4];
+    uint32_t cr[4];
+    {
+        const WideNode n = load_wide(s, cur);
+        const float lim0 = T.minHit * SB_PRUNE_SCALE;
+        float bt[4];
+        const unsigned hitm = wide_boxes(T.r, n, bt);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t ref = n.ref[k];
+            const bool pass = ref != SB_INVALID &&
+                              ((ref & SB_NOBOX_BIT) || (((hitm >> k) & 1u) && !(bt[k] > T.r.tmax) && !(bt[k] > lim0)));
+            ct[k] = __int_as_float(0x7f800000);  // +inf: no candidate
+            cr[k] = SB_INVALID;
+            if (pass && (ref & SB_LEAF_BIT)) {
+                pend[(np++) * STRIDE] = ref & ~(SB_LEAF_BIT | SB_NOBOX_BIT);
+            } else if (pass) {
+                ct[k] = bt[k];
+                cr[k] = ref;
+            }
+        }
+    }
+    // nearest first; every candidate is within the best hit (tested above)
+    cswap(ct[0], cr[0], ct[1], cr[1]);
+    cswap(ct[2], cr[2], ct[3], cr[3]);
+    cswap(ct[0], cr[0], ct[2], cr[2]);
+    cswap(ct[1], cr[1], ct[3], cr[3]);
+    cswap(ct[1], cr[1], ct[2], cr[2]);
+    T.cur = cr[0];
+#pragma unroll
+    for (int k = 3; k >= 1; --k) {
+        if (cr[k] == SB_INVALID) continue;
+        if (T.sp < SB_STACK) {
+            stackN[T.sp] = cr[k];
+            stackT[T.sp] = ct[k];
+            ++T.sp;
+        } else {
+            // stack full: finish with the stackless loop from the root
+            const Fallback f = closest_stackless_rec<COUNT>(s, T.r, T.minHit, T.leaf, T.hit, T.found);
+            T.hit = f.hit;
+            T.minHit = f.minHit;
+            T.leaf = f.leaf;
+            T.found = f.found;
+            if (COUNT) {
+                nInner += f.nInner;
+                nLeaf += f.nLeaf;
+            }
+            T.cur = SB_INVALID;
+            T.sp = 0;
+            return true;
+        }
+    }
+    return false;
+}
+
+// The warp's deferred leaf tests.  All 32 lanes call it; `have` says whether
+// the lane holds a query.
+template <bool COUNT, int STRIDE>
+__device__ __forceinline__ void closest_defer_leaves(const DevScene& s, Trav& T, bool have, const uint32_t* pend, uint32_t& np,
+                                                     uint32_t& nLeaf)
+{
+    const bool wait = have && np != 0;
+    const unsigned waiting = __ballot_sync(0xffffffffu, wait);
+    const bool stuck = wait && (T.cur == SB_INVALID || np > SB_DEFER_CAP - 4);
+    if (waiting && (__popc(waiting) >= SB_DEFER_LANES || __any_sync(0xffffffffu, stuck))) {
+        if (wait) {
+            --np;
+            if (COUNT) ++nLeaf;
+            closest_leaf(s, T, pend[np * STRIDE]);
+        }
+    }
+}
+
+// One iteration of a lane's deferred closest-hit query, after the warp's
+// closest_defer_leaves: a node step when there is room for its leaves, then
+// a pop when nothing is current.  Returns true when the query is finished.
+template <bool COUNT, int STRIDE>
+__device__ __forceinline__ bool closest_defer_step(const DevScene& s, Trav& T, uint32_t* stackN, float* stackT, uint32_t* pend,
+                                                   uint32_t& np, uint32_t& nInner, uint32_t& nLeaf)
+{
+    if (T.cur != SB_INVALID && np <= SB_DEFER_CAP - 4) {
+        if (closest_defer_node<COUNT, STRIDE>(s, T, stackN, stackT, pend, np, nInner, nLeaf)) {
+            np = 0;
+            return true;
+        }
+    }
+    if (T.cur == SB_INVALID) closest_pop(T, stackN, stackT);
+    return T.cur == SB_INVALID && np == 0;
+}
+
 // One any-hit step (the reference's depth-first order).  Returns true when
 // finished; T.found tells whether a hit with t < tmax was found.
 template <bool COUNT>

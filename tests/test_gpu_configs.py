@@ -13,7 +13,8 @@
   reference's stackless loop (raytracing.h:198-247), ties included; any-hit
   records of 4M shadow rays (tmax in [0.1, 2]) bit for bit against the
   reference's depth-first loop (raytracing.h:249-286); visit counts equal to
-  the oracle's replay of the kernels' traversal rule; and the float-float
+  the oracle's replay of the kernels' traversal rule (closest hit: of one
+  warp that takes a 4096-ray batch); and the float-float
   refinement of t and the barycentrics against an FP64 Moller-Trumbore.
 """
 import numpy as np
@@ -88,6 +89,9 @@ def _trace(torch, pt, ds, rays_d, n, flags, counters=None):
 
 
 N_RAYS = 4_000_000
+# the largest queue chunk: one warp takes a batch this size, so closest-hit
+# counts (deferred leaf tests) are deterministic
+WARP_CHUNK = 4096
 
 
 @pytest.mark.parametrize("query", ["closest", "any"])
@@ -102,12 +106,22 @@ def test_soup_1m_tris_4m_rays(cuda, soup_1m, query):
     assert found.sum() > N_RAYS // 20
     assert np.array_equal(g, o)
     # visit counts: the kernels count what they process; the oracle replays
-    # the same rule
+    # the same rule (closest hit: its warp replay, on one warp's batch)
     cnt = cuda.zeros(2, dtype=cuda.int64, device="cuda")
     g2 = _trace(cuda, pt, ds, rd, N_RAYS, flags | abi.TRACE_COUNT, cnt)
-    _, _, co = oracle.trace(view, rays, any_hit=shadow, prune=2)
-    assert np.array_equal(cnt.cpu().numpy().astype(np.uint64), co)
     assert np.array_equal(g2, o)
+    if shadow:
+        _, _, co = oracle.trace(view, rays, any_hit=True, prune=2)
+        assert np.array_equal(cnt.cpu().numpy().astype(np.uint64), co)
+    else:
+        sub = rays[:WARP_CHUNK]
+        ptw = PathTracer(queue_chunk=WARP_CHUNK)
+        cw = cuda.zeros(2, dtype=cuda.int64, device="cuda")
+        gw = _trace(cuda, ptw, ds, to_device(sub), WARP_CHUNK, flags | abi.TRACE_COUNT, cw)
+        ow, _, cow = oracle.trace_warp(view, sub)
+        assert np.array_equal(cw.cpu().numpy().astype(np.uint64), cow)
+        assert np.array_equal(gw, o[:WARP_CHUNK]) and np.array_equal(ow, o[:WARP_CHUNK])
+        assert ptw.device_status() == 0
     assert pt.device_status() == 0
 
 

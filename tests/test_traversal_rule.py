@@ -3,13 +3,22 @@ the reference's closestHit / anyHit records (shaders/raytracing.h:198-286)
 bit for bit, ties in t included: skipping the odd-depth boxes of the binary
 tree leaves the set of tested triangles unchanged, and closest-hit ties go to
 the leaf first in depth-first order, as in the reference's strict t < minHit
-loop.  The GPU kernels match this replay exactly (tests/test_gpu_trace.py)."""
+loop.  The GPU kernels match this replay exactly (tests/test_gpu_trace.py).
+The closest-hit kernels defer leaf tests and run them across the warp; the
+oracle's replay of one such warp (oracle.trace_warp) returns the same records
+too."""
 import numpy as np
 import pytest
 
 import oracle
 from gpu_util import interior_rays, vertex_edge_rays
 from strelka_b200 import scenes
+
+
+def warp_matches(view, rays, ref):
+    """The deferred warp replay's closest hits equal the reference's."""
+    got, _, _ = oracle.trace_warp(view, rays)
+    return np.array_equal(got, ref)
 
 
 @pytest.fixture(scope="module")
@@ -25,6 +34,8 @@ def test_ties_at_vertices_and_edges(cornell, any_hit):
     wide, _, _ = oracle.trace(cornell, rays, any_hit=any_hit, prune=2)
     assert found.mean() > 0.8
     assert np.array_equal(wide, ref)
+    if not any_hit:
+        assert warp_matches(cornell, rays, ref)
 
 
 @pytest.mark.parametrize("tmax", [1e9, 0.4])
@@ -34,6 +45,8 @@ def test_random_interior_rays(cornell, tmax):
         ref, _, _ = oracle.trace(cornell, rays, any_hit=any_hit)
         wide, _, _ = oracle.trace(cornell, rays, any_hit=any_hit, prune=2)
         assert np.array_equal(wide, ref)
+        if not any_hit:
+            assert warp_matches(cornell, rays, ref)
 
 
 def test_soup():
@@ -45,6 +58,8 @@ def test_soup():
             ref, _, _ = oracle.trace(v, rays, any_hit=any_hit)
             wide, _, _ = oracle.trace(v, rays, any_hit=any_hit, prune=2)
             assert np.array_equal(wide, ref)
+            if not any_hit:
+                assert warp_matches(v, rays, ref)
 
 
 @pytest.mark.parametrize("num_tris", [1, 2, 3, 5])
@@ -57,6 +72,8 @@ def test_tiny_trees(num_tris):
         ref, _, _ = oracle.trace(v, rays, any_hit=any_hit)
         wide, _, _ = oracle.trace(v, rays, any_hit=any_hit, prune=2)
         assert np.array_equal(wide, ref)
+        if not any_hit:
+            assert warp_matches(v, rays, ref)
 
 
 def test_chain_tree():
@@ -69,6 +86,8 @@ def test_chain_tree():
         ref, found, _ = oracle.trace(v, rays, any_hit=any_hit)
         wide, _, _ = oracle.trace(v, rays, any_hit=any_hit, prune=2)
         assert np.array_equal(wide, ref)
+        if not any_hit:
+            assert warp_matches(v, rays, ref)
     # the chain is a valid tree: the reference finds the same hits over it as
     # over the builder's tree
     base, _, _ = oracle.trace(oracle.SceneView(scenes.soup(600, 12)), rays)
@@ -95,3 +114,5 @@ def test_instanced_scene():
         wide, _, _ = oracle.trace(v, rays, any_hit=any_hit, prune=2)
         assert found.sum() > 100
         assert np.array_equal(wide, ref)
+        if not any_hit:
+            assert warp_matches(v, rays, ref)
