@@ -326,8 +326,16 @@ typedef struct StrelkaPathTracerConfig {
 enum {
     STRELKA_PT_PROFILE = 1u << 0,       /* record per-kernel CUDA events (strelka_pathtracer_get_kernel_times) */
     STRELKA_PT_COUNT = 1u << 1,         /* count traversal visits (strelka_pathtracer_get_counters) */
-    STRELKA_PT_NO_SHADE_SORT = 1u << 2  /* wavefront: shade paths in queue order, not sorted by material */
+    STRELKA_PT_NO_SHADE_SORT = 1u << 2, /* wavefront: shade paths in queue order, not sorted by material */
+    /* wavefront traversal variants (default: by tree size, STRELKA_LARGE_SCENE_NODES): the large-scene
+       variants keep the top of each traversal stack in shared memory and defer the leaf tests of
+       bounces >= 1 across the warp; the small-scene ones leave L1 to the scene.  Same results. */
+    STRELKA_PT_LARGE_SCENE_KERNELS = 1u << 3, /* always the large-scene variants */
+    STRELKA_PT_SMALL_SCENE_KERNELS = 1u << 4  /* always the small-scene variants */
 };
+
+/* BVH nodes from which the wavefront passes use their large-scene variants. */
+#define STRELKA_LARGE_SCENE_NODES (1u << 21)
 
 typedef struct StrelkaPathTracer StrelkaPathTracer;
 typedef struct StrelkaNrc StrelkaNrc;

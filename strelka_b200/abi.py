@@ -49,6 +49,9 @@ MODE_MEGAKERNEL = 1
 PT_PROFILE = 1
 PT_COUNT = 2
 PT_NO_SHADE_SORT = 4
+PT_LARGE_SCENE_KERNELS = 8
+PT_SMALL_SCENE_KERNELS = 16
+LARGE_SCENE_NODES = 1 << 21
 
 TRACE_CLOSEST = 0
 TRACE_ANY = 1

@@ -217,8 +217,7 @@ __global__ void __launch_bounds__(BLOCK, kExtendThreadsPerSM / BLOCK) k_batch_ex
         w.counters[batch_shadow_count(qin)] = 0;  // refilled by this bounce's shade
     }
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
-    uint32_t stackN[SB_STACK];
-    float stackT[SB_STACK];
+    LocalStack st;
     uint32_t nI = 0, nL = 0;
     WarpPool pool{0, 0, 0};
     bool have = false;
@@ -236,7 +235,7 @@ __global__ void __launch_bounds__(BLOCK, kExtendThreadsPerSM / BLOCK) k_batch_ex
         }
         if (!__any_sync(kFull, have)) break;
         if (!have) continue;
-        const bool done = T.cur == SB_INVALID || closest_step<false>(*sc, T, stackN, stackT, nI, nL);
+        const bool done = T.cur == SB_INVALID || closest_step<false>(*sc, T, st, nI, nL);
         if (!done) continue;
         w.hit[slot] = T.found ? make_float4(T.hit.u, T.hit.v, T.hit.t, __uint_as_float(T.hit.instId))
                               : make_float4(0.0f, 0.0f, 1e9f, __uint_as_float(SB_INVALID));
@@ -437,7 +436,7 @@ __global__ void __launch_bounds__(BLOCK, kShadowThreadsPerSM / BLOCK) k_batch_sh
     __shared__ uint32_t sp[kMaxJobs + 1];
     load_prefix(jt, sp);
     const uint32_t count = w.counters[batch_shadow_count(qin)];
-    uint32_t stackN[SB_STACK];
+    LocalStackN st;
     uint32_t nI = 0, nL = 0;
     WarpPool pool{0, 0, 0};
     bool have = false;
@@ -455,7 +454,7 @@ __global__ void __launch_bounds__(BLOCK, kShadowThreadsPerSM / BLOCK) k_batch_sh
         }
         if (!__any_sync(kFull, have)) break;
         if (!have) continue;
-        const bool done = T.cur == SB_INVALID || any_step<false>(*sc, T, stackN, nI, nL);
+        const bool done = T.cur == SB_INVALID || any_step<false>(*sc, T, st, nI, nL);
         if (!done) continue;
         const float4 cd = w.sh_cd[item];
         const int kind = (int)__float_as_uint(cd.w);

@@ -10,6 +10,7 @@
 //     path state, with the surviving paths compacted by warp ballot into a
 //     queue between bounces.
 // Both forms call the same shade()/apply_shadow() device code.
+#include <type_traits>
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -29,6 +30,12 @@ using namespace sb;
 namespace {
 
 constexpr int kExtendBlock = 128;
+// Traversal stack entries kept in shared memory per thread (deeper ones in
+// local memory), measured fastest per kernel: the wavefront closest-hit pass
+// 8, its any-hit pass and the ray-query kernels 16.
+constexpr int kExtendStackShared = 8;
+constexpr int kShadowStackShared = 16;
+constexpr int kTraceStackShared = 16;
 constexpr int kShadeBlock = 128;
 constexpr int kSmallBlock = 256;
 constexpr uint32_t kMaxSortKeys = 4096;
@@ -388,7 +395,10 @@ __global__ void __launch_bounds__(kSmallBlock) k_generate(PathTracerParam ubo, W
 // queue entries at a time from an atomic head, and a lane takes its next
 // path as soon as its current query ends (the warp keeps stepping while any
 // lane has work), so neither a warp nor a CTA waits for its longest ray.
-template <bool COUNT>
+// DEFER: leaf tests deferred across the warp with the split stack (for
+// incoherent rays); otherwise tested where reached, on a local-memory stack
+// (coherent rays, whose lanes already test the same leaves together).
+template <bool COUNT, bool DEFER>
 __global__ void __launch_bounds__(kExtendBlock, SB_EXTEND_MINBLOCKS) k_extend(DevScene s, Wave w, int qin, uint32_t chunk,
                                                          unsigned long long* visitCounters)
 {
@@ -399,15 +409,17 @@ __global__ void __launch_bounds__(kExtendBlock, SB_EXTEND_MINBLOCKS) k_extend(De
         w.counters[4] = 0;                 // shade's work-queue head
     }
     const uint32_t* __restrict__ q = qin ? w.queue[1] : w.queue[0];
-    uint32_t stackN[SB_STACK];
-    float stackT[SB_STACK];
+    using Stack = std::conditional_t<DEFER, SplitStack<kExtendBlock, kExtendStackShared>, LocalStack>;
+    __shared__ uint2 sStack[DEFER ? kExtendStackShared * kExtendBlock : 1];
+    __shared__ uint32_t sPend[DEFER ? SB_DEFER_CAP * kExtendBlock : 1];  // deferred leaf tests
+    Stack st;
+    if constexpr (DEFER) st.sm = &sStack[threadIdx.x];
+    uint32_t* pend = &sPend[DEFER ? threadIdx.x : 0];
     uint32_t nI = 0, nL = 0, nR = 0;
     WarpPool pool{0, 0, 0};
     uint32_t slot = 0;
     Trav T;
     const uint32_t root = trav_root(s);
-    __shared__ uint32_t sPend[SB_DEFER_CAP * kExtendBlock];  // deferred leaf tests
-    uint32_t* pend = &sPend[threadIdx.x];
     uint32_t np = 0;
     bool have = false;
     while (true) {
@@ -420,9 +432,19 @@ __global__ void __launch_bounds__(kExtendBlock, SB_EXTEND_MINBLOCKS) k_extend(De
             have = true;
         }
         if (!__any_sync(0xffffffffu, have)) break;
-        closest_defer_leaves<COUNT, kExtendBlock>(s, T, have, pend, np, nL);
+        if constexpr (DEFER) closest_defer_leaves<COUNT, kExtendBlock>(s, T, have, pend, np, nL);
         if (!have) continue;
-        if (!closest_defer_step<COUNT, kExtendBlock>(s, T, stackN, stackT, pend, np, nI, nL)) continue;
+        if constexpr (DEFER) {
+            bool fin = false;
+            if (T.cur != SB_INVALID && np <= SB_DEFER_CAP - 4) {
+                fin = closest_defer_node<COUNT, kExtendBlock>(s, T, st, pend, np, nI, nL);
+                if (fin) np = 0;
+            }
+            if (!fin && T.cur == SB_INVALID) closest_pop<true>(T, st);
+            if (!fin && !(T.cur == SB_INVALID && np == 0)) continue;
+        } else {
+            if (!(T.cur == SB_INVALID || closest_step<COUNT>(s, T, st, nI, nL))) continue;
+        }
         w.hit[slot] = T.found ? make_float4(T.hit.u, T.hit.v, T.hit.t, __uint_as_float(T.hit.instId))
                               : make_float4(0.0f, 0.0f, 1e9f, __uint_as_float(SB_INVALID));
         w.hitPrim[slot] = T.found ? T.hit.primId : SB_INVALID;
@@ -667,12 +689,16 @@ __global__ void __launch_bounds__(kShadeBlock, SB_SHADE_MINBLOCKS) k_shade(DevSc
 // shadow: any-hit query for every next-event request (reference depth-first
 // order); adds the visible ones.  Work is taken from an atomic queue in
 // `chunk` units as in k_extend.
-template <bool COUNT>
+// SPLIT: the split stack and the inlined stackless fallback (large scenes).
+template <bool COUNT, bool SPLIT>
 __global__ void __launch_bounds__(kExtendBlock, SB_SHADOW_MINBLOCKS) k_shadow(DevScene s, Wave w, int qin, uint32_t chunk,
                                                                               unsigned long long* visitCounters)
 {
     const uint32_t count = w.counters[shadow_count(qin)];
-    uint32_t stackN[SB_STACK];
+    using Stack = std::conditional_t<SPLIT, SplitStackN<kExtendBlock, kShadowStackShared>, LocalStackN>;
+    __shared__ uint32_t sStack[SPLIT ? kShadowStackShared * kExtendBlock : 1];
+    Stack st;
+    if constexpr (SPLIT) st.sm = &sStack[threadIdx.x];
     uint32_t nI = 0, nL = 0, nR = 0;
     WarpPool pool{0, 0, 0};
     uint32_t item = 0;
@@ -689,7 +715,7 @@ __global__ void __launch_bounds__(kExtendBlock, SB_SHADOW_MINBLOCKS) k_shadow(De
         }
         if (!__any_sync(0xffffffffu, have)) break;
         if (!have) continue;
-        const bool done = T.cur == SB_INVALID || any_step<COUNT>(s, T, stackN, nI, nL);
+        const bool done = T.cur == SB_INVALID || any_step<COUNT, SPLIT>(s, T, st, nI, nL);
         if (!done) continue;
         const float4 cd = w.sh_cd[item];
         const int kind = (int)__float_as_uint(cd.w);
@@ -882,8 +908,11 @@ __global__ void __launch_bounds__(kExtendBlock, ANY ? 9 : 8) k_trace(DevScene s,
                                                         uint32_t n, uint32_t* head, uint32_t chunk,
                                                         unsigned long long* counters)
 {
-    uint32_t stackN[SB_STACK];
-    float stackT[SB_STACK];
+    using Stack = std::conditional_t<ANY, SplitStackN<kExtendBlock, kTraceStackShared>,
+                                     SplitStack<kExtendBlock, kTraceStackShared>>;
+    __shared__ std::conditional_t<ANY, uint32_t, uint2> sStack[kTraceStackShared * kExtendBlock];
+    Stack st;
+    st.sm = &sStack[threadIdx.x];
     uint32_t nI = 0, nL = 0;
     WarpPool pool{0, 0, 0};
     uint32_t i = 0;
@@ -903,18 +932,18 @@ __global__ void __launch_bounds__(kExtendBlock, ANY ? 9 : 8) k_trace(DevScene s,
             have = true;
         }
         if (!__any_sync(0xffffffffu, have)) break;
-        if (!ANY) closest_defer_leaves<COUNT, kExtendBlock>(s, T, have, pend, np, nL);
+        if constexpr (!ANY) closest_defer_leaves<COUNT, kExtendBlock>(s, T, have, pend, np, nL);
         if (!have) continue;
         bool done;
-        if (ANY) {
-            done = T.cur == SB_INVALID || any_step<COUNT>(s, T, stackN, nI, nL);
+        if constexpr (ANY) {
+            done = T.cur == SB_INVALID || any_step<COUNT, true>(s, T, st, nI, nL);
         } else {
             bool fin = false;
             if (T.cur != SB_INVALID && np <= SB_DEFER_CAP - 4) {
-                fin = closest_defer_node<COUNT, kExtendBlock>(s, T, stackN, stackT, pend, np, nI, nL);
+                fin = closest_defer_node<COUNT, kExtendBlock>(s, T, st, pend, np, nI, nL);
                 if (fin) np = 0;
             }
-            if (!fin && T.cur == SB_INVALID) closest_pop(T, stackN, stackT);
+            if (!fin && T.cur == SB_INVALID) closest_pop(T, st);
             done = fin || (T.cur == SB_INVALID && np == 0);
         }
         if (!done) continue;
@@ -977,6 +1006,7 @@ struct StrelkaPathTracer {
     std::vector<cudaEvent_t> eventPool;
     size_t eventsUsed = 0;
     int nrcPathGrid = 0;
+    int extendGridCoherent = 0;
     int extendGrid = 0, shadowGrid = 0, tailGrid = 0, traceGrid = 0, traceGridAny = 0, shadeGrid = 0, shadeGridNrc = 0, smallGrid = 0;
     unsigned long long* visitCounters = nullptr;  // 6 entries (STRELKA_PT_COUNT)
     // radiance cache
@@ -1281,6 +1311,10 @@ extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, 
         delete pt;
         return fail(STRELKA_ERR_INVALID_ARGUMENT, "queueChunk must be 0 or a multiple of 32 up to 4096");
     }
+    if ((pt->cfg.flags & STRELKA_PT_LARGE_SCENE_KERNELS) && (pt->cfg.flags & STRELKA_PT_SMALL_SCENE_KERNELS)) {
+        delete pt;
+        return fail(STRELKA_ERR_INVALID_ARGUMENT, "STRELKA_PT_LARGE_SCENE_KERNELS and STRELKA_PT_SMALL_SCENE_KERNELS together");
+    }
     pt->device = dev;
     cudaDeviceGetAttribute(&pt->numSMs, cudaDevAttrMultiProcessorCount, dev);
     float lut[256];
@@ -1300,8 +1334,9 @@ extern "C" int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, 
         strelka_pathtracer_destroy(pt);
         return fail(STRELKA_ERR_OUT_OF_MEMORY, "cudaMalloc failed");
     }
-    pt->extendGrid = occupancy_grid((const void*)k_extend<false>, kExtendBlock, pt->numSMs);
-    pt->shadowGrid = occupancy_grid((const void*)k_shadow<false>, kExtendBlock, pt->numSMs);
+    pt->extendGrid = occupancy_grid((const void*)k_extend<false, true>, kExtendBlock, pt->numSMs);
+    pt->extendGridCoherent = occupancy_grid((const void*)k_extend<false, false>, kExtendBlock, pt->numSMs);
+    pt->shadowGrid = occupancy_grid((const void*)k_shadow<false, true>, kExtendBlock, pt->numSMs);
     pt->tailGrid = occupancy_grid((const void*)k_tail, kExtendBlock, pt->numSMs);
     pt->nrcPathGrid = occupancy_grid((const void*)k_nrc_train_paths, kNrcPathBlock, pt->numSMs);
     pt->traceGrid = occupancy_grid((const void*)k_trace<false, false, false>, kExtendBlock, pt->numSMs);
@@ -1341,6 +1376,23 @@ extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
 // Radiance-cache training: `batches` batches of trainPaths training paths,
 // traced in one launch, then per batch trainSteps gradient + Adam steps on
 // its vertices (batch sizes read on the device).
+// The wavefront passes' traversal variants.  Shared-memory stacks and
+// deferred leaf tests pay on trees far beyond L1 (10M triangles: +4%); on
+// small trees the shared memory they take from L1 costs more than they save
+// (the 10k-triangle Cornell box: -9%); the measured crossover lies between
+// 1.3M and 5M nodes.  Camera rays (bounce 0) are coherent: their lanes test
+// the same leaves together, so their leaf tests are never deferred.
+static bool large_scene(const StrelkaPathTracer* pt, const DevScene& s)
+{
+    if (pt->cfg.flags & STRELKA_PT_LARGE_SCENE_KERNELS) return true;
+    if (pt->cfg.flags & STRELKA_PT_SMALL_SCENE_KERNELS) return false;
+    return s.numNodes >= STRELKA_LARGE_SCENE_NODES;
+}
+static bool extend_defer(const StrelkaPathTracer* pt, const DevScene& s, int depth)
+{
+    return depth >= 1 && large_scene(pt, s);
+}
+
 static int nrc_train_frame(StrelkaPathTracer* pt, const DevScene& s, const PathTracerParam& ubo, uint32_t batches,
                            cudaStream_t st)
 {
@@ -1503,8 +1555,14 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             const bool count = (pt->cfg.flags & STRELKA_PT_COUNT) != 0;
             {
                 Timer t(pt, KC_EXTEND, st);
-                if (count) k_extend<true><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, qchunk, pt->visitCounters);
-                else k_extend<false><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, qchunk, nullptr);
+                if (extend_defer(pt, s, depth)) {
+                    if (count) k_extend<true, true><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, qchunk, pt->visitCounters);
+                    else k_extend<false, true><<<gridE, kExtendBlock, 0, st>>>(s, pt->main.w, qin, qchunk, nullptr);
+                } else {
+                    const int gridC = std::min<int>((n + kExtendBlock - 1) / kExtendBlock, pt->extendGridCoherent);
+                    if (count) k_extend<true, false><<<gridC, kExtendBlock, 0, st>>>(s, pt->main.w, qin, qchunk, pt->visitCounters);
+                    else k_extend<false, false><<<gridC, kExtendBlock, 0, st>>>(s, pt->main.w, qin, qchunk, nullptr);
+                }
             }
             const uint32_t* order = nullptr;
             if (sortKeys && depth >= SB_SORT_FROM_DEPTH) {
@@ -1537,8 +1595,13 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
 #endif
             {
                 Timer t(pt, KC_SHADOW, sst);
-                if (count) k_shadow<true><<<gridW, kExtendBlock, 0, sst>>>(s, pt->main.w, qin, qchunk, pt->visitCounters);
-                else k_shadow<false><<<gridW, kExtendBlock, 0, sst>>>(s, pt->main.w, qin, qchunk, nullptr);
+                if (large_scene(pt, s)) {
+                    if (count) k_shadow<true, true><<<gridW, kExtendBlock, 0, sst>>>(s, pt->main.w, qin, qchunk, pt->visitCounters);
+                    else k_shadow<false, true><<<gridW, kExtendBlock, 0, sst>>>(s, pt->main.w, qin, qchunk, nullptr);
+                } else {
+                    if (count) k_shadow<true, false><<<gridW, kExtendBlock, 0, sst>>>(s, pt->main.w, qin, qchunk, pt->visitCounters);
+                    else k_shadow<false, false><<<gridW, kExtendBlock, 0, sst>>>(s, pt->main.w, qin, qchunk, nullptr);
+                }
             }
 #if SB_OVERLAP_SHADOW
             SB_CUDA_TRY(cudaEventRecord(pt->shadowDone, pt->aux));

@@ -337,9 +337,11 @@ __device__ __noinline__ Fallback closest_stackless_rec(const DevScene s, const R
     return f;
 }
 
-// The reference's stackless any-hit loop from `node` (raytracing.h:249-286).
+// The reference's stackless any-hit loop from `node` (raytracing.h:249-286),
+// inlined into the any-hit kernels (any_stackless_loop) and called out of
+// line elsewhere (any_stackless_rec).
 template <bool COUNT>
-__device__ __noinline__ Fallback any_stackless_rec(const DevScene s, const RayQ r, uint32_t node, HitRec hit)
+__device__ __forceinline__ Fallback any_stackless_loop(const DevScene& s, const RayQ& r, uint32_t node, HitRec hit)
 {
     Fallback f;
     f.nInner = 0;
@@ -386,6 +388,11 @@ __device__ __noinline__ Fallback any_stackless_rec(const DevScene s, const RayQ 
     }
     f.hit = hit;
     return f;
+}
+template <bool COUNT>
+__device__ __noinline__ Fallback any_stackless_rec(const DevScene s, const RayQ r, uint32_t node, HitRec hit)
+{
+    return any_stackless_loop<COUNT>(s, r, node, hit);
 }
 
 // Per-query traversal state for the step functions.
@@ -562,11 +569,86 @@ __device__ __forceinline__ void closest_leaf(const DevScene& s, Trav& T, uint32_
     }
 }
 
+// Traversal stacks: closest hit keeps (entry ref, entry distance) pairs,
+// any hit entry refs.  LocalStack / LocalStackN are per-thread arrays (local
+// memory).  SplitStack / SplitStackN keep the entries below depth S in shared
+// memory, entry i of a thread at sm[i * STRIDE] (consecutive threads in
+// consecutive words, so a warp's accesses are free of bank conflicts whatever
+// depths its lanes are at), and deeper ones in local memory: a pop then costs
+// a shared-memory read instead of a local load that mostly misses L1 behind
+// the node stream.
+struct LocalStack {
+    uint32_t n[SB_STACK];
+    float t[SB_STACK];
+    __device__ __forceinline__ void set(int i, uint32_t r, float d)
+    {
+        n[i] = r;
+        t[i] = d;
+    }
+    __device__ __forceinline__ uint32_t ref(int i) const { return n[i]; }
+    __device__ __forceinline__ float dist(int i) const { return t[i]; }
+};
+struct LocalStackN {
+    uint32_t n[SB_STACK];
+    __device__ __forceinline__ void set(int i, uint32_t ref) { n[i] = ref; }
+    __device__ __forceinline__ uint32_t get(int i) const { return n[i]; }
+};
+template <int STRIDE, int S>
+struct SplitStack {
+    uint2* sm;
+    uint2 deep[SB_STACK - S];
+    __device__ __forceinline__ void set(int i, uint32_t ref, float d)
+    {
+        const uint2 v = make_uint2(ref, __float_as_uint(d));
+        if (i < S) sm[i * STRIDE] = v;
+        else deep[i - S] = v;
+    }
+    __device__ __forceinline__ uint2 get(int i) const { return i < S ? sm[i * STRIDE] : deep[i - S]; }
+    __device__ __forceinline__ uint32_t ref(int i) const { return get(i).x; }
+    __device__ __forceinline__ float dist(int i) const { return __uint_as_float(get(i).y); }
+};
+template <int STRIDE, int S>
+struct SplitStackN {
+    uint32_t* sm;
+    uint32_t deep[SB_STACK - S];
+    __device__ __forceinline__ void set(int i, uint32_t ref)
+    {
+        if (i < S) sm[i * STRIDE] = ref;
+        else deep[i - S] = ref;
+    }
+    __device__ __forceinline__ uint32_t get(int i) const { return i < S ? sm[i * STRIDE] : deep[i - S]; }
+};
+
+// Pops until an entry within the best hit is found (T.cur stays SB_INVALID
+// when the stack runs out).  PAIR reads an entry's ref and distance with one
+// access (split stacks only) instead of the distance first; both forms
+// compute the same, and each kernel uses the one that compiles to fewer
+// spilled registers.
+template <bool PAIR = false, class STK>
+__device__ __forceinline__ void closest_pop(Trav& T, const STK& st)
+{
+    const float lim = T.minHit * SB_PRUNE_SCALE;
+    while (T.sp > 0) {
+        --T.sp;
+        if constexpr (PAIR) {
+            const uint2 e = st.get(T.sp);
+            if (!(__uint_as_float(e.y) > lim)) {
+                T.cur = e.x;
+                return;
+            }
+        } else {
+            if (!(st.dist(T.sp) > lim)) {
+                T.cur = st.ref(T.sp);
+                return;
+            }
+        }
+    }
+}
+
 // One closest-hit step: processes the 4-wide node T.cur (or the root leaf),
 // then pops until a node to process is found.  Returns true when finished.
-template <bool COUNT>
-__device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, uint32_t* stackN, float* stackT, uint32_t& nInner,
-                                             uint32_t& nLeaf)
+template <bool COUNT, class STK>
+__device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, STK& st, uint32_t& nInner, uint32_t& nLeaf)
 {
     const uint32_t cur = T.cur;
     if (cur != SB_INVALID) {
@@ -630,8 +712,7 @@ __device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, uint32_
             for (int k = 3; k >= 1; --k) {
                 if (cr[k] == SB_INVALID || ct[k] > lim) continue;
                 if (T.sp < SB_STACK) {
-                    stackN[T.sp] = cr[k];
-                    stackT[T.sp] = ct[k];
+                    st.set(T.sp, cr[k], ct[k]);
                     ++T.sp;
                 } else {
                     // stack full: finish with the stackless loop from the root
@@ -652,14 +733,7 @@ __device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, uint32_
         }
     }
     if (T.cur == SB_INVALID) {
-        const float lim = T.minHit * SB_PRUNE_SCALE;
-        while (T.sp > 0) {
-            --T.sp;
-            if (!(stackT[T.sp] > lim)) {
-                T.cur = stackN[T.sp];
-                break;
-            }
-        }
+        closest_pop(T, st);
         if (T.cur == SB_INVALID) return true;
     }
     return false;
@@ -689,19 +763,6 @@ __device__ __forceinline__ bool closest_step(const DevScene& s, Trav& T, uint32_
 #define SB_DEFER_LANES 16
 #endif
 
-// Pops until an entry within the best hit is found (T.cur stays SB_INVALID
-// when the stack runs out).
-__device__ __forceinline__ void closest_pop(Trav& T, const uint32_t* stackN, const float* stackT)
-{
-    const float lim = T.minHit * SB_PRUNE_SCALE;
-    while (T.sp > 0) {
-        --T.sp;
-        if (!(stackT[T.sp] > lim)) {
-            T.cur = stackN[T.sp];
-            return;
-        }
-    }
-}
 
 // One node of the deferred traversal (T.cur is a 4-wide node or the root
 // leaf; the caller guarantees room for four more pending leaves): passing
@@ -709,9 +770,9 @@ __device__ __forceinline__ void closest_pop(Trav& T, const uint32_t* stackN, con
 // the others go onto the stack, farthest first.  Returns true when the
 // traversal ended early (a fault, the step cap, or the stackless fallback,
 // which tests every leaf itself, pending ones included).
-template <bool COUNT, int STRIDE>
-__device__ __forceinline__ bool closest_defer_node(const DevScene& s, Trav& T, uint32_t* stackN, float* stackT, uint32_t* pend,
-                                                   uint32_t& np, uint32_t& nInner, uint32_t& nLeaf)
+template <bool COUNT, int STRIDE, class STK>
+__device__ __forceinline__ bool closest_defer_node(const DevScene& s, Trav& T, STK& st, uint32_t* pend, uint32_t& np,
+                                                   uint32_t& nInner, uint32_t& nLeaf)
 {
     const uint32_t cur = T.cur;
     if (++T.steps > s.numNodes + 1u) {
@@ -761,8 +822,7 @@ __device__ __forceinline__ bool closest_defer_node(const DevScene& s, Trav& T, u
     for (int k = 3; k >= 1; --k) {
         if (cr[k] == SB_INVALID) continue;
         if (T.sp < SB_STACK) {
-            stackN[T.sp] = cr[k];
-            stackT[T.sp] = ct[k];
+            st.set(T.sp, cr[k], ct[k]);
             ++T.sp;
         } else {
             // stack full: finish with the stackless loop from the root
@@ -801,27 +861,10 @@ __device__ __forceinline__ void closest_defer_leaves(const DevScene& s, Trav& T,
     }
 }
 
-// One iteration of a lane's deferred closest-hit query, after the warp's
-// closest_defer_leaves: a node step when there is room for its leaves, then
-// a pop when nothing is current.  Returns true when the query is finished.
-template <bool COUNT, int STRIDE>
-__device__ __forceinline__ bool closest_defer_step(const DevScene& s, Trav& T, uint32_t* stackN, float* stackT, uint32_t* pend,
-                                                   uint32_t& np, uint32_t& nInner, uint32_t& nLeaf)
-{
-    if (T.cur != SB_INVALID && np <= SB_DEFER_CAP - 4) {
-        if (closest_defer_node<COUNT, STRIDE>(s, T, stackN, stackT, pend, np, nInner, nLeaf)) {
-            np = 0;
-            return true;
-        }
-    }
-    if (T.cur == SB_INVALID) closest_pop(T, stackN, stackT);
-    return T.cur == SB_INVALID && np == 0;
-}
-
 // One any-hit step (the reference's depth-first order).  Returns true when
 // finished; T.found tells whether a hit with t < tmax was found.
-template <bool COUNT>
-__device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, uint32_t* stackN, uint32_t& nInner, uint32_t& nLeaf)
+template <bool COUNT, bool INLINE_FALLBACK = false, class STK>
+__device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, STK& st, uint32_t& nInner, uint32_t& nLeaf)
 {
     const uint32_t cur = T.cur;
     if (cur != SB_INVALID && !(cur & SB_LEAF_BIT)) {
@@ -853,11 +896,12 @@ __device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, uint32_t* s
             if (!pass[k]) continue;
             if (first != SB_INVALID) {
                 if (T.sp < SB_STACK) {
-                    stackN[T.sp++] = first;
+                    st.set(T.sp++, first);
                 } else {
                     // stack full: the reference's stackless loop from the root
                     // gives the same first hit
-                    const Fallback f = any_stackless_rec<COUNT>(s, T.r, 0u, T.hit);
+                    const Fallback f = INLINE_FALLBACK ? any_stackless_loop<COUNT>(s, T.r, 0u, T.hit)
+                                                       : any_stackless_rec<COUNT>(s, T.r, 0u, T.hit);
                     T.hit = f.hit;
                     T.found = f.found;
                     if (COUNT) {
@@ -877,7 +921,7 @@ __device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, uint32_t* s
     for (;;) {
         if (T.cur == SB_INVALID) {
             if (T.sp == 0) return true;
-            T.cur = stackN[--T.sp];
+            T.cur = st.get(--T.sp);
         }
         if (!(T.cur & SB_LEAF_BIT)) return false;
         if (COUNT) ++nLeaf;
@@ -899,12 +943,11 @@ template <bool COUNT>
 __device__ __forceinline__ bool trace_closest_rec(const DevScene& s, v3 o, float tmax, v3 d, HitRec& hit, uint32_t& nInner,
                                                   uint32_t& nLeaf)
 {
-    uint32_t stackN[SB_STACK];
-    float stackT[SB_STACK];
+    LocalStack st;
     Trav T;
     trav_init(s, T, o, tmax, d, false);
     if (T.cur != SB_INVALID)
-        while (!closest_step<COUNT>(s, T, stackN, stackT, nInner, nLeaf)) {
+        while (!closest_step<COUNT>(s, T, st, nInner, nLeaf)) {
         }
     hit = T.hit;
     return T.found;
@@ -914,11 +957,11 @@ template <bool COUNT>
 __device__ __forceinline__ bool trace_any_rec(const DevScene& s, v3 o, float tmax, v3 d, HitRec& hit, uint32_t& nInner,
                                               uint32_t& nLeaf)
 {
-    uint32_t stackN[SB_STACK];
+    LocalStackN st;
     Trav T;
     trav_init(s, T, o, tmax, d, true);
     if (T.cur != SB_INVALID)
-        while (!any_step<COUNT>(s, T, stackN, nInner, nLeaf)) {
+        while (!any_step<COUNT>(s, T, st, nInner, nLeaf)) {
         }
     hit = T.hit;
     return T.found;

@@ -4,6 +4,8 @@ arguments end in error statuses, never in a hang or a device fault.
 The reference's traversal loops have no bound (a cycle in nodeOffset spins
 forever); here every traversal stops after 2*numNodes+2 visits and raises
 STRELKA_DEV_TRAVERSAL_CAP, and every fetch is range-checked first."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -109,6 +111,10 @@ def test_bad_execute_arguments(cuda, base):
     d = ds.desc(p, None)
     with pytest.raises(abi.StrelkaError):
         pt.execute(d, 16 * 16 * 2, 1, 0)
+    # the two scene-kernel overrides exclude each other
+    cfg = abi.StrelkaPathTracerConfig(abi.MODE_WAVEFRONT, 0, 0, abi.PT_LARGE_SCENE_KERNELS | abi.PT_SMALL_SCENE_KERNELS, 0, 0)
+    h = C.c_void_p()
+    assert pt.lib.strelka_pathtracer_create(C.byref(cfg), C.byref(h)) == abi.ERR_INVALID_ARGUMENT
 
 
 @pytest.mark.parametrize("arrive", [0, 1])

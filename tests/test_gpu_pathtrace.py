@@ -122,6 +122,27 @@ def test_large_scene_small(cuda):
         assert bits_equal_fraction(g, r) >= EXACT_BAR
 
 
+@pytest.mark.parametrize("variant", ["large", "small"])
+def test_scene_kernel_variants(cuda, cornell, variant):
+    # the wavefront's large-scene traversal variants (shared-memory stacks,
+    # leaf tests deferred across the warp from bounce 1 on) and its
+    # small-scene ones give the oracle's samples bit for bit; the tail kernel
+    # is off so that every bounce runs the wavefront passes
+    s, view, ds = cornell
+    big = scenes.large(width=48, height=32, instances=6, frequency=6, num_textures=2, tex_size=64, env_width=64,
+                       env_height=32, max_depth=8, spp=2, seed=5)
+    for sc, v, d, p in ((s, view, ds, s.param(spp=2, maxDepth=8, frameNumber=9, stratifiedSamplingType=1)),
+                        (big, oracle.SceneView(big), DeviceScene(big), big.param(frameNumber=2))):
+        total = p.dimension[0] * p.dimension[1] * p.spp
+        sb = cuda.full((total * 3,), -7.0, dtype=cuda.float32, device="cuda")
+        pt = PathTracer(mode=abi.MODE_WAVEFRONT, chunk_paths=1111, tail_depth=100, scene_kernels=variant)
+        pt.execute(d.desc(p, sb), total, 1, 0)
+        assert pt.device_status() == 0
+        g = sb.cpu().numpy()
+        r = oracle.pathtrace(v, p)
+        assert bits_equal_fraction(g, r) >= EXACT_BAR
+
+
 def test_golden_fixture(cuda):
     # the fixture is the reference's own shader code compiled on the host
     # (tests/golden/make_golden.py); samples it leaves undefined are skipped
