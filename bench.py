@@ -44,17 +44,17 @@ UNIT = "Mpaths/s"
 # DRAM bytes (read + write) per closest-hit query of the extend kernel on the
 # large scene, from one ncu capture of the five extend launches of a
 # 960x540 x 4 spp frame (dram__bytes_read.sum + dram__bytes_write.sum =
-# 1693.1 MB for 4,300,568 queries).  The per-query figure falls as the frame
-# grows (481 B per query at 480x270 x 4 spp): more queries share the cached
+# 1717.5 MB for 4,300,568 queries).  The per-query figure falls as the frame
+# grows (496 B per query at 480x270 x 4 spp): more queries share the cached
 # nodes.  bench.py cannot run ncu itself, so roofline.traffic is this figure
 # times the queries of an average launch, an upper bound for the full frame.
-EXTEND_DRAM_BYTES_PER_RAY = 393.7
+EXTEND_DRAM_BYTES_PER_RAY = 399.4
 
 # DRAM bytes (read + write) per closest-hit query of the ray-query kernel on
 # the 1M-triangle soup, from one ncu capture of a timed launch with 4M rays
-# (1693.7 + 157.9 MB); 458.6 B per query with 1M rays, so the figure scales
+# (1404.8 + 122.1 MB); 380.0 B per query with 1M rays, so the figure scales
 # with the number of rays.
-TRACE_SOUP_DRAM_BYTES_PER_RAY = 462.9
+TRACE_SOUP_DRAM_BYTES_PER_RAY = 381.7
 
 # Bytes a traversal reads per 4-wide node it processes: the bounds of its four
 # entries (6 float4) and their refs (1 float4).
