@@ -61,3 +61,25 @@ def test_error_reporting_without_gpu(lib):
     cnt = C.c_uint32(7)
     assert lib.strelka_bvh_build(None, 4, C.byref(out), C.byref(cnt)) == abi.ERR_INVALID_ARGUMENT
     assert lib.strelka_bvh_build(None, 0, C.byref(out), C.byref(cnt)) == abi.OK and cnt.value == 0
+
+
+def header_constants():
+    """Enumerators and #define constants of the public header, by name."""
+    text = open(os.path.join(ROOT, "include", "strelka_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(STRELKA_\w+)\s*=\s*1u\s*<<\s*(\d+)", text):
+        out[m.group(1)] = 1 << int(m.group(2))
+    for m in re.finditer(r"#define\s+(STRELKA_\w+)\s+\(1u\s*<<\s*(\d+)\)", text):
+        out[m.group(1)] = 1 << int(m.group(2))
+    return out
+
+
+def test_pass_flags_match_header():
+    c = header_constants()
+    assert c["STRELKA_PT_PROFILE"] == abi.PT_PROFILE
+    assert c["STRELKA_PT_COUNT"] == abi.PT_COUNT
+    assert c["STRELKA_PT_NO_SHADE_SORT"] == abi.PT_NO_SHADE_SORT
+    assert c["STRELKA_PT_LARGE_SCENE_KERNELS"] == abi.PT_LARGE_SCENE_KERNELS
+    assert c["STRELKA_PT_SMALL_SCENE_KERNELS"] == abi.PT_SMALL_SCENE_KERNELS
+    assert c["STRELKA_LARGE_SCENE_NODES"] == abi.LARGE_SCENE_NODES

@@ -116,3 +116,20 @@ def test_instanced_scene():
         assert np.array_equal(wide, ref)
         if not any_hit:
             assert warp_matches(v, rays, ref)
+
+
+def test_warp_replay_constants_match_the_kernels():
+    # the oracle's replay of a deferring warp uses the kernels' pending-list
+    # size and lane threshold
+    import os
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cuh = open(os.path.join(root, "strelka_b200", "csrc", "traverse.cuh")).read()
+    orc = open(os.path.join(root, "oracle", "oracle.c")).read()
+
+    def define(text, name):
+        return int(re.search(r"#define\s+" + name + r"\s+(\d+)", text).group(1))
+
+    assert define(cuh, "SB_DEFER_CAP") == define(orc, "DEFER_CAP")
+    assert define(cuh, "SB_DEFER_LANES") == define(orc, "DEFER_LANES")
+    assert define(cuh, "SB_STACK") == define(orc, "WIDE_STACK")
