@@ -302,8 +302,9 @@ typedef struct UpscaleDesc {
 /* Path tracer pass object (replaces PathTracer : ComputePass<PathTracerParam>,
  * include/render/pathtracer.h:33-50, src/render/pathtracer.cpp:1-94).  The
  * object caches scene-derived device data (a leaf triangle table of 48
- * bytes per leaf, each node's leaf index, a 4-wide BVH derived from bvhNodes
- * and its build scratch: about 108 bytes per BVH node allocated) keyed by
+ * bytes per leaf, a leaf shading table of 96 bytes per leaf, each node's
+ * leaf index, a 4-wide BVH derived from bvhNodes and its build scratch:
+ * about 156 bytes per BVH node allocated) keyed by
  * PathTracerDesc.sceneVersion and the buffer pointers, and owns the
  * wavefront path queues. */
 

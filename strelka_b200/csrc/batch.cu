@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(BLOCK, kExtendThreadsPerSM / BLOCK) k_batch_ex
         if (!done) continue;
         w.hit[slot] = T.found ? make_float4(T.hit.u, T.hit.v, T.hit.t, __uint_as_float(T.hit.instId))
                               : make_float4(0.0f, 0.0f, 1e9f, __uint_as_float(SB_INVALID));
-        w.hitPrim[slot] = T.found ? T.hit.primId : SB_INVALID;
+        w.hitRef[slot] = T.found ? T.hit.primId : SB_INVALID;
         have = false;
     }
 }
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(BLOCK) k_batch_shade(JobTable jt, Wave w, int 
             h.v = h4.y;
             h.t = h4.z;
             h.instId = __float_as_uint(h4.w);
-            h.primId = w.hitPrim[slot];
+            h.primId = w.hitRef[slot];
             cont = shade(J.s, J.ubo, ps, h.instId != SB_INVALID, h, sr);
             if (cont) {
                 ++ps.depth;
@@ -642,7 +642,7 @@ int ensure_wave(StrelkaBatch* b, size_t cap)
     int rc;
     if ((rc = balloc(b, &w.ray_o, cap)) || (rc = balloc(b, &w.ray_d, cap)) || (rc = balloc(b, &w.thr, cap)) ||
         (rc = balloc(b, &w.col, cap)) || (rc = balloc(b, &w.rng, cap)) || (rc = balloc(b, &w.hit, cap)) ||
-        (rc = balloc(b, &w.hitPrim, cap)) || (rc = balloc(b, &w.queue[0], cap)) || (rc = balloc(b, &w.queue[1], cap)) ||
+        (rc = balloc(b, &w.hitRef, cap)) || (rc = balloc(b, &w.queue[0], cap)) || (rc = balloc(b, &w.queue[1], cap)) ||
         (rc = balloc(b, &w.sh_o, cap)) || (rc = balloc(b, &w.sh_d, cap)) || (rc = balloc(b, &w.sh_cd, cap)) ||
         (rc = balloc(b, &w.sh_cg, cap)) || (rc = balloc(b, &w.counters, kWaveCounters)) || (rc = balloc(b, &b->sorted, cap)) ||
         (rc = balloc(b, &b->keys, cap))) {

@@ -87,6 +87,55 @@ __global__ void k_leaf_flag(const float4* __restrict__ nodes, uint32_t numNodes,
         flag[i] = __float_as_uint(nodes[2 * (size_t)i].w) != SB_INVALID ? 1u : 0u;
 }
 
+// Per-leaf shading record, 6 float4 at the leaf's compact index: the
+// world-space positions and normals of its triangle's vertices and their
+// UVs, with exactly the arithmetic the shade kernel applies at a hit
+// (pathtracerMdl.hlsl:237-267), so reading them gives the same bits while a
+// shaded hit reads 96 contiguous bytes instead of three indices and three
+// vertices behind its instance record:
+// [0] p0|u0  [1] p1|v0  [2] p2|u1  [3] n0|v1  [4] n1|u2  [5] n2|v2.
+// Leaves that k_prep_rec rejects are never hit and are skipped here.
+__global__ void k_prep_shade(const float4* __restrict__ nodes, uint32_t numNodes, const InstanceConstants* __restrict__ inst,
+                             uint32_t numInstances, const uint32_t* __restrict__ ib, uint32_t numIndices,
+                             const Vertex* __restrict__ vb, uint32_t numVertices, const uint32_t* __restrict__ leafOf,
+                             uint32_t recCap, float4* __restrict__ out)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < numNodes; i += gridDim.x * blockDim.x) {
+        const float4 lo = nodes[2 * (size_t)i];
+        const uint32_t instId = __float_as_uint(lo.w);
+        if (instId == SB_INVALID || instId >= numInstances) continue;
+        const uint32_t li = leafOf[i];
+        if (li >= recCap) continue;
+        const InstanceConstants* ic = &inst[instId];
+        const uint32_t base = (uint32_t)ic->indexOffset + __float_as_uint(lo.x) * 3u;
+        if ((uint64_t)base + 2 >= numIndices) continue;
+        const uint32_t i0 = ib[base], i1 = ib[base + 1], i2 = ib[base + 2];
+        if (i0 >= numVertices || i1 >= numVertices || i2 >= numVertices) continue;
+        const float* o2w = ic->objectToWorld.m;
+        const float* nrm = ic->normalMatrix.m;
+        const Vertex& V0 = vb[i0];
+        const Vertex& V1 = vb[i1];
+        const Vertex& V2 = vb[i2];
+        const v3 p0 = mat_mul_point(o2w, V(V0.position[0], V0.position[1], V0.position[2]), 1.0f);
+        const v3 p1 = mat_mul_point(o2w, V(V1.position[0], V1.position[1], V1.position[2]), 1.0f);
+        const v3 p2 = mat_mul_point(o2w, V(V2.position[0], V2.position[1], V2.position[2]), 1.0f);
+        const v3 n0 = mat_mul_dir3(nrm, unpack_normal(V0.normal));
+        const v3 n1 = mat_mul_dir3(nrm, unpack_normal(V1.normal));
+        const v3 n2 = mat_mul_dir3(nrm, unpack_normal(V2.normal));
+        float uv0[2], uv1[2], uv2[2];
+        unpack_uv(V0.uv, uv0[0], uv0[1]);
+        unpack_uv(V1.uv, uv1[0], uv1[1]);
+        unpack_uv(V2.uv, uv2[0], uv2[1]);
+        float4* r = &out[6 * (size_t)li];
+        r[0] = f4(p0, uv0[0]);
+        r[1] = f4(p1, uv0[1]);
+        r[2] = f4(p2, uv1[0]);
+        r[3] = f4(n0, uv1[1]);
+        r[4] = f4(n1, uv2[0]);
+        r[5] = f4(n2, uv2[1]);
+    }
+}
+
 __global__ void k_prep_rec(const float4* __restrict__ nodes, uint32_t numNodes, const InstanceConstants* __restrict__ inst,
                            uint32_t numInstances, const uint32_t* __restrict__ ib, uint32_t numIndices,
                            const Vertex* __restrict__ vb, uint32_t numVertices, const uint32_t* __restrict__ leafOf,
@@ -447,7 +496,7 @@ __global__ void __launch_bounds__(kExtendBlock, SB_EXTEND_MINBLOCKS) k_extend(De
         }
         w.hit[slot] = T.found ? make_float4(T.hit.u, T.hit.v, T.hit.t, __uint_as_float(T.hit.instId))
                               : make_float4(0.0f, 0.0f, 1e9f, __uint_as_float(SB_INVALID));
-        w.hitPrim[slot] = T.found ? T.hit.primId : SB_INVALID;
+        w.hitRef[slot] = T.found ? T.leaf : SB_INVALID;  // k_shade reads the leaf's shading record
         if (COUNT) ++nR;
         have = false;
     }
@@ -632,21 +681,21 @@ __global__ void __launch_bounds__(kShadeBlock, SB_SHADE_MINBLOCKS) k_shade(DevSc
             h.v = h4.y;
             h.t = h4.z;
             h.instId = __float_as_uint(h4.w);
-            h.primId = w.hitPrim[slot];
+            h.primId = w.hitRef[slot];  // the compact leaf index (shade<true>)
             const bool found = h.instId != SB_INVALID;
             if (NRC) {
                 nq.mode = 2;
                 nq.diffuseRoughness = nw.diffuseRoughness;
                 nq.has = false;
                 nq.terminate = false;
-                cont = shade(s, ubo, ps, found, h, sr, &nq);
+                cont = shade<true>(s, ubo, ps, found, h, sr, &nq);
                 if (nq.terminate) {
                     query = true;
                     qdir = vneg(ps.rd);
                     qthr = ps.throughput;
                 }
             } else {
-                cont = shade(s, ubo, ps, found, h, sr);
+                cont = shade<true>(s, ubo, ps, found, h, sr);
             }
             if (cont) {
                 ++ps.depth;
@@ -992,6 +1041,8 @@ struct StrelkaPathTracer {
     uint32_t keyNumNodes = 0;
     void* tablesMem = nullptr;  // derived scene tables (internal.h SceneTables)
     size_t tablesCap = 0;       // nodes they were sized for
+    float4* shadeRec = nullptr; // per-leaf shading records (k_prep_shade)
+    size_t shadeCap = 0;        // leaves they were sized for
     SceneTables tables;
     float* srgbLut = nullptr;
     uint32_t* status = nullptr;
@@ -1058,7 +1109,7 @@ int ensure_wave(WaveBuf& b, size_t cap)
     int rc;
     if ((rc = walloc(b, &w.ray_o, cap)) || (rc = walloc(b, &w.ray_d, cap)) || (rc = walloc(b, &w.thr, cap)) ||
         (rc = walloc(b, &w.col, cap)) || (rc = walloc(b, &w.rng, cap)) || (rc = walloc(b, &w.hit, cap)) ||
-        (rc = walloc(b, &w.hitPrim, cap)) || (rc = walloc(b, &w.queue[0], cap)) || (rc = walloc(b, &w.queue[1], cap)) ||
+        (rc = walloc(b, &w.hitRef, cap)) || (rc = walloc(b, &w.queue[0], cap)) || (rc = walloc(b, &w.queue[1], cap)) ||
         (rc = walloc(b, &w.sh_o, cap)) || (rc = walloc(b, &w.sh_d, cap)) || (rc = walloc(b, &w.sh_cd, cap)) ||
         (rc = walloc(b, &w.sh_cg, cap)) || (rc = walloc(b, &w.counters, kWaveCounters)) ||
         (rc = walloc(b, &b.sorted, cap)) || (rc = walloc(b, &b.keys, cap))) {
@@ -1131,11 +1182,22 @@ int ensure_scene(StrelkaPathTracer* pt, const BVHNode* nodes, uint32_t numNodes,
         pt->tablesCap = cap;
     }
     pt->tables = scene_tables(pt->tablesMem, numNodes);
+    if (pt->tables.recCap > pt->shadeCap || !pt->shadeRec) {
+        if (pt->shadeRec) cudaFree(pt->shadeRec);
+        pt->shadeRec = nullptr;
+        pt->shadeCap = 0;
+        SB_CUDA_TRY(cudaMalloc(&pt->shadeRec, (size_t)pt->tables.recCap * 6 * sizeof(float4)));
+        pt->shadeCap = pt->tables.recCap;
+    }
     if (numNodes) {
-        Timer t(pt, KC_PREP, st, 6);
+        Timer t(pt, KC_PREP, st, 7);
         int rc = launch_prep_tables(nodes, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, pt->tables,
                                     pt->status, pt->numSMs, st);
         if (rc) return rc;
+        const int grid = std::min<int>((numNodes + 255) / 256, pt->numSMs * 16);
+        k_prep_shade<<<grid, 256, 0, st>>>(reinterpret_cast<const float4*>(nodes), numNodes, inst, numInstances, ib,
+                                            numIndices, vb, numVertices, pt->tables.leafOf, pt->tables.recCap, pt->shadeRec);
+        SB_CUDA_TRY(cudaGetLastError());
     }
     pt->sceneVersion = version;
     pt->keyNodes = nodes;
@@ -1148,7 +1210,9 @@ int ensure_scene(StrelkaPathTracer* pt, const BVHNode* nodes, uint32_t numNodes,
 
 DevScene make_scene(StrelkaPathTracer* pt, const PathTracerDesc* d)
 {
-    return scene_from_desc(d, pt->tables, pt->srgbLut, pt->status);
+    DevScene s = scene_from_desc(d, pt->tables, pt->srgbLut, pt->status);
+    s.shadeRec = pt->shadeRec;
+    return s;
 }
 
 int occupancy_grid(const void* fn, int block, int numSMs)
@@ -1262,6 +1326,7 @@ DevScene scene_from_desc(const PathTracerDesc* d, const SceneTables& t, const fl
     s.nodes = reinterpret_cast<const float4*>(d->bvhNodes);
     s.tris = nullptr;
     s.rec = t.rec;
+    s.shadeRec = nullptr;  // the single-job passes attach their shading records
     s.leafOf = t.leafOf;
     s.numRec = t.recCap;
     s.wide = t.wide;
@@ -1353,6 +1418,7 @@ extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
     if (!pt) return STRELKA_OK;
     free_wave(pt->main);
     if (pt->tablesMem) cudaFree(pt->tablesMem);
+    if (pt->shadeRec) cudaFree(pt->shadeRec);
     if (pt->srgbLut) cudaFree(pt->srgbLut);
     if (pt->status) cudaFree(pt->status);
     if (pt->visitCounters) cudaFree(pt->visitCounters);

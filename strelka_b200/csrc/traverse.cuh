@@ -25,6 +25,7 @@ struct DevScene {
     const float4* rec;    // 3 float4 per leaf, at the leaf's compact index
     const uint32_t* leafOf;  // per node: its compact leaf index (leaves only)
     uint32_t numRec;      // capacity of `rec` in leaves
+    const float4* shadeRec;  // 6 float4 per leaf at its compact index (shading vertex data), or null
     const float4* wide;   // 8 float4 per 4-wide node (see below)
     uint32_t numWide;     // capacity of `wide` in nodes
     uint32_t numNodes;

@@ -14,7 +14,7 @@ struct Wave {
     float4* col;     // color
     uint32_t* rng;
     float4* hit;     // u, v, t, instId (SB_INVALID = miss)
-    uint32_t* hitPrim;
+    uint32_t* hitRef;  // the hit primitive id (batch) or its compact leaf index (single-job passes)
     uint32_t* queue[2];
     float4* sh_o;    // origin, tmax
     float4* sh_d;    // direction, slot
