@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(BLOCK, kExtendThreadsPerSM / BLOCK) k_batch_ex
         if (!done) continue;
         w.hit[slot] = T.found ? make_float4(T.hit.u, T.hit.v, T.hit.t, __uint_as_float(T.hit.instId))
                               : make_float4(0.0f, 0.0f, 1e9f, __uint_as_float(SB_INVALID));
-        w.hitRef[slot] = T.found ? T.hit.primId : SB_INVALID;
+        w.hitRef[slot] = T.found ? T.leaf : SB_INVALID;  // k_batch_shade reads the leaf's shading record
         have = false;
     }
 }
@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(BLOCK) k_batch_shade(JobTable jt, Wave w, int 
             h.t = h4.z;
             h.instId = __float_as_uint(h4.w);
             h.primId = w.hitRef[slot];
-            cont = shade(J.s, J.ubo, ps, h.instId != SB_INVALID, h, sr);
+            cont = shade<true>(J.s, J.ubo, ps, h.instId != SB_INVALID, h, sr);
             if (cont) {
                 ++ps.depth;
                 cont = ps.depth < (int)J.ubo.maxDepth;

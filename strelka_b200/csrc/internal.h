@@ -21,6 +21,7 @@ int validate_scene_desc(const PathTracerDesc* d);
 struct SceneTables {
     float4* rec = nullptr;
     uint32_t recCap = 0;
+    float4* shade = nullptr;  // 6 float4 per leaf: its triangle's shading vertex data (k_prep_shade)
     uint32_t* leafOf = nullptr;
     float4* wide = nullptr;
     uint32_t wideCap = 0;

@@ -1041,8 +1041,6 @@ struct StrelkaPathTracer {
     uint32_t keyNumNodes = 0;
     void* tablesMem = nullptr;  // derived scene tables (internal.h SceneTables)
     size_t tablesCap = 0;       // nodes they were sized for
-    float4* shadeRec = nullptr; // per-leaf shading records (k_prep_shade)
-    size_t shadeCap = 0;        // leaves they were sized for
     SceneTables tables;
     float* srgbLut = nullptr;
     uint32_t* status = nullptr;
@@ -1182,22 +1180,11 @@ int ensure_scene(StrelkaPathTracer* pt, const BVHNode* nodes, uint32_t numNodes,
         pt->tablesCap = cap;
     }
     pt->tables = scene_tables(pt->tablesMem, numNodes);
-    if (pt->tables.recCap > pt->shadeCap || !pt->shadeRec) {
-        if (pt->shadeRec) cudaFree(pt->shadeRec);
-        pt->shadeRec = nullptr;
-        pt->shadeCap = 0;
-        SB_CUDA_TRY(cudaMalloc(&pt->shadeRec, (size_t)pt->tables.recCap * 6 * sizeof(float4)));
-        pt->shadeCap = pt->tables.recCap;
-    }
     if (numNodes) {
         Timer t(pt, KC_PREP, st, 7);
         int rc = launch_prep_tables(nodes, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, pt->tables,
                                     pt->status, pt->numSMs, st);
         if (rc) return rc;
-        const int grid = std::min<int>((numNodes + 255) / 256, pt->numSMs * 16);
-        k_prep_shade<<<grid, 256, 0, st>>>(reinterpret_cast<const float4*>(nodes), numNodes, inst, numInstances, ib,
-                                            numIndices, vb, numVertices, pt->tables.leafOf, pt->tables.recCap, pt->shadeRec);
-        SB_CUDA_TRY(cudaGetLastError());
     }
     pt->sceneVersion = version;
     pt->keyNodes = nodes;
@@ -1210,9 +1197,7 @@ int ensure_scene(StrelkaPathTracer* pt, const BVHNode* nodes, uint32_t numNodes,
 
 DevScene make_scene(StrelkaPathTracer* pt, const PathTracerDesc* d)
 {
-    DevScene s = scene_from_desc(d, pt->tables, pt->srgbLut, pt->status);
-    s.shadeRec = pt->shadeRec;
-    return s;
+    return scene_from_desc(d, pt->tables, pt->srgbLut, pt->status);
 }
 
 int occupancy_grid(const void* fn, int block, int numSMs)
@@ -1248,8 +1233,8 @@ size_t scene_tables_bytes(uint32_t numNodes)
 {
     const size_t n = std::max<uint32_t>(numNodes, 1);
     const size_t wideCap = n / 2 + 1, recCap = n / 2 + 1;
-    return align256(recCap * 3 * sizeof(float4)) + align256(wideCap * 8 * sizeof(float4)) + 5 * align256(n * 4) + 256 +
-           align256(scan_bytes(numNodes));
+    return align256(recCap * 3 * sizeof(float4)) + align256(recCap * 6 * sizeof(float4)) +
+           align256(wideCap * 8 * sizeof(float4)) + 5 * align256(n * 4) + 256 + align256(scan_bytes(numNodes));
 }
 
 SceneTables scene_tables(void* base, uint32_t numNodes)
@@ -1261,6 +1246,8 @@ SceneTables scene_tables(void* base, uint32_t numNodes)
     char* p = static_cast<char*>(base);
     t.rec = reinterpret_cast<float4*>(p);
     p += align256((size_t)t.recCap * 3 * sizeof(float4));
+    t.shade = reinterpret_cast<float4*>(p);
+    p += align256((size_t)t.recCap * 6 * sizeof(float4));
     t.leafOf = reinterpret_cast<uint32_t*>(p);
     p += align256(n * 4);
     t.wide = reinterpret_cast<float4*>(p);
@@ -1294,6 +1281,8 @@ int launch_prep_tables(const BVHNode* nodes, uint32_t numNodes, const InstanceCo
     SB_CUDA_TRY(cub::DeviceScan::ExclusiveSum(t.scan, bytes, t.parent, t.leafOf, (int)numNodes, st));
     k_prep_rec<<<grid, 256, 0, st>>>(nd, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, t.leafOf,
                                      t.recCap, t.rec, status);
+    k_prep_shade<<<grid, 256, 0, st>>>(nd, numNodes, inst, numInstances, ib, numIndices, vb, numVertices, t.leafOf,
+                                       t.recCap, t.shade);
     SB_CUDA_TRY(cudaMemsetAsync(t.parent, 0xFF, (size_t)numNodes * 4, st));
     k_wide_parent<<<grid, 256, 0, st>>>(nd, numNodes, t.parent);
     SB_CUDA_TRY(cudaMemsetAsync(t.deep, 0, sizeof(uint32_t), st));
@@ -1326,7 +1315,7 @@ DevScene scene_from_desc(const PathTracerDesc* d, const SceneTables& t, const fl
     s.nodes = reinterpret_cast<const float4*>(d->bvhNodes);
     s.tris = nullptr;
     s.rec = t.rec;
-    s.shadeRec = nullptr;  // the single-job passes attach their shading records
+    s.shadeRec = t.shade;
     s.leafOf = t.leafOf;
     s.numRec = t.recCap;
     s.wide = t.wide;
@@ -1418,7 +1407,6 @@ extern "C" int strelka_pathtracer_destroy(StrelkaPathTracer* pt)
     if (!pt) return STRELKA_OK;
     free_wave(pt->main);
     if (pt->tablesMem) cudaFree(pt->tablesMem);
-    if (pt->shadeRec) cudaFree(pt->shadeRec);
     if (pt->srgbLut) cudaFree(pt->srgbLut);
     if (pt->status) cudaFree(pt->status);
     if (pt->visitCounters) cudaFree(pt->visitCounters);
