@@ -44,11 +44,11 @@ UNIT = "Mpaths/s"
 # DRAM bytes (read + write) per closest-hit query of the extend kernel on the
 # large scene, from one ncu capture of the five extend launches of a
 # 960x540 x 4 spp frame (dram__bytes_read.sum + dram__bytes_write.sum =
-# 1717.5 MB for 4,300,568 queries).  The per-query figure falls as the frame
+# 1714.7 MB for 4,300,568 queries).  The per-query figure falls as the frame
 # grows (496 B per query at 480x270 x 4 spp): more queries share the cached
 # nodes.  bench.py cannot run ncu itself, so roofline.traffic is this figure
 # times the queries of an average launch, an upper bound for the full frame.
-EXTEND_DRAM_BYTES_PER_RAY = 399.4
+EXTEND_DRAM_BYTES_PER_RAY = 398.7
 
 # DRAM bytes (read + write) per closest-hit query of the ray-query kernel on
 # the 1M-triangle soup, from one ncu capture of a timed launch with 4M rays
