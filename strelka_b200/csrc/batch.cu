@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(BLOCK) k_batch_persistent(JobTable jt, uint32_
             const BatchJobDev& J = jt.jobs[job];
             HitRec h;
             uint32_t a = 0, b = 0;
-            const bool found = J.s.numNodes != 0 && trace_closest_rec<false>(J.s, ps.ro, ps.tmax, ps.rd, h, a, b);
+            const bool found = J.s.numNodes != 0 && trace_closest_rec<false, true>(J.s, ps.ro, ps.tmax, ps.rd, h, a, b);
             ShadowReq sr;
             bool cont = shade(J.s, J.ubo, ps, found, h, sr);
             if (sr.kind != 0 && shadow_visible(J.s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(BLOCK) k_batch_shade(JobTable jt, Wave w, int 
             h.t = h4.z;
             h.instId = __float_as_uint(h4.w);
             h.primId = w.hitRef[slot];
-            cont = shade<true>(J.s, J.ubo, ps, h.instId != SB_INVALID, h, sr);
+            cont = shade(J.s, J.ubo, ps, h.instId != SB_INVALID, h, sr);
             if (cont) {
                 ++ps.depth;
                 cont = ps.depth < (int)J.ubo.maxDepth;
@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(BLOCK) k_batch_tail(JobTable jt, Wave w, int q
         const BatchJobDev& J = jt.jobs[job];
         HitRec h;
         uint32_t a = 0, b = 0;
-        const bool found = J.s.numNodes != 0 && trace_closest_rec<false>(J.s, ps.ro, ps.tmax, ps.rd, h, a, b);
+        const bool found = J.s.numNodes != 0 && trace_closest_rec<false, true>(J.s, ps.ro, ps.tmax, ps.rd, h, a, b);
         ShadowReq sr;
         const bool cont = shade(J.s, J.ubo, ps, found, h, sr);
         if (sr.kind != 0 && shadow_visible(J.s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);

@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(kExtendBlock) k_megakernel(DevScene s, PathTra
     while (ps.depth < maxDepth) {
         HitRec h;
         uint32_t a = 0, b = 0;
-        bool found = s.numNodes != 0 && trace_closest_rec<false>(s, ps.ro, ps.tmax, ps.rd, h, a, b);
+        bool found = s.numNodes != 0 && trace_closest_rec<false, true>(s, ps.ro, ps.tmax, ps.rd, h, a, b);
         ShadowReq sr;
         bool cont = shade(s, ubo, ps, found, h, sr);
         if (sr.kind != 0 && shadow_visible(s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
@@ -681,21 +681,21 @@ __global__ void __launch_bounds__(kShadeBlock, SB_SHADE_MINBLOCKS) k_shade(DevSc
             h.v = h4.y;
             h.t = h4.z;
             h.instId = __float_as_uint(h4.w);
-            h.primId = w.hitRef[slot];  // the compact leaf index (shade<true>)
+            h.primId = w.hitRef[slot];  // the compact leaf index (shade reads its shading record)
             const bool found = h.instId != SB_INVALID;
             if (NRC) {
                 nq.mode = 2;
                 nq.diffuseRoughness = nw.diffuseRoughness;
                 nq.has = false;
                 nq.terminate = false;
-                cont = shade<true>(s, ubo, ps, found, h, sr, &nq);
+                cont = shade(s, ubo, ps, found, h, sr, &nq);
                 if (nq.terminate) {
                     query = true;
                     qdir = vneg(ps.rd);
                     qthr = ps.throughput;
                 }
             } else {
-                cont = shade<true>(s, ubo, ps, found, h, sr);
+                cont = shade(s, ubo, ps, found, h, sr);
             }
             if (cont) {
                 ++ps.depth;
@@ -827,7 +827,7 @@ __global__ void __launch_bounds__(kExtendBlock) k_tail(DevScene s, PathTracerPar
         if (!have) continue;
         HitRec h;
         uint32_t a = 0, b = 0;
-        const bool found = s.numNodes != 0 && trace_closest_rec<false>(s, ps.ro, ps.tmax, ps.rd, h, a, b);
+        const bool found = s.numNodes != 0 && trace_closest_rec<false, true>(s, ps.ro, ps.tmax, ps.rd, h, a, b);
         ShadowReq sr;
         const bool cont = shade(s, ubo, ps, found, h, sr);
         if (sr.kind != 0 && shadow_visible(s, sr.kind, sr.o, sr.tmax, sr.d)) apply_shadow(ps.color, sr.cd, sr.cg);
@@ -924,7 +924,7 @@ __global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, P
         if (!have) continue;
         HitRec hit;
         uint32_t a = 0, b = 0;
-        const bool found = s.numNodes != 0 && trace_closest_rec<false>(s, ps.ro, ps.tmax, ps.rd, hit, a, b);
+        const bool found = s.numNodes != 0 && trace_closest_rec<false, true>(s, ps.ro, ps.tmax, ps.rd, hit, a, b);
         const v3 c0 = ps.color, t0 = ps.throughput, dOut = vneg(ps.rd);
         NrcShade nq;
         nq.mode = 1;

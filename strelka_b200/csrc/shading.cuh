@@ -681,11 +681,11 @@ __device__ __forceinline__ void apply_shadow(v3& color, v3 cd, v3 cg)
 
 // One iteration of the loop body of pathTraceCameraRays after closestHit
 // (pathtracerMdl.hlsl:225-401).  Returns true when the path continues (the
-// caller then increments depth and tests depth < maxDepth).  LEAF: hit.primId
-// holds the hit's compact leaf index, and the triangle's world-space vertex
-// data comes from the scene's shading records (s.shadeRec, the same values
-// as computing them here from the instance, index and vertex buffers).
-template <bool LEAF = false>
+// caller then increments depth and tests depth < maxDepth).  hit.primId holds
+// the hit's compact leaf index: the triangle's world-space vertex data comes
+// from the leaf's shading record (s.shadeRec, built by k_prep_shade with the
+// arithmetic of pathtracerMdl.hlsl:237-267 applied to the instance, index
+// and vertex buffers, so the values are the same bits).
 __device__ __forceinline__ bool shade(const DevScene& s, const PathTracerParam& ubo, PathState& ps, bool found,
                                       const HitRec& hit, ShadowReq& sr, NrcShade* nq = nullptr)
 {
@@ -717,47 +717,16 @@ __device__ __forceinline__ bool shade(const DevScene& s, const PathTracerParam& 
     }
     if (lightId != -1) return false;  // diffuse bounce reached an emitter (reference reads mdlMaterials[-1])
 
-    v3 p0, p1, p2, n0, n1, n2;
-    float uv0[2], uv1[2], uv2[2];
-    if constexpr (LEAF) {
-        const uint32_t leaf = hit.primId;
-        if (leaf >= s.numRec) {
-            raise_status(s, STRELKA_DEV_NODE_OOB);
-            return false;
-        }
-        const float4* r = &s.shadeRec[6 * (size_t)leaf];
-        const float4 a0 = __ldg(r), a1 = __ldg(r + 1), a2 = __ldg(r + 2), a3 = __ldg(r + 3), a4 = __ldg(r + 4),
-                     a5 = __ldg(r + 5);
-        p0 = xyz(a0);
-        p1 = xyz(a1);
-        p2 = xyz(a2);
-        n0 = xyz(a3);
-        n1 = xyz(a4);
-        n2 = xyz(a5);
-        uv0[0] = a0.w;
-        uv0[1] = a1.w;
-        uv1[0] = a2.w;
-        uv1[1] = a3.w;
-        uv2[0] = a4.w;
-        uv2[1] = a5.w;
-    } else {
-        const float* o2w = ic->objectToWorld.m;
-        const float* nrm = ic->normalMatrix.m;
-        const uint32_t base = (uint32_t)__ldg(&ic->indexOffset) + hit.primId * 3u;
-        const uint32_t i0 = __ldg(&s.ib[base + 0]), i1 = __ldg(&s.ib[base + 1]), i2 = __ldg(&s.ib[base + 2]);
-        const Vertex* V0 = &s.vb[i0];
-        const Vertex* V1 = &s.vb[i1];
-        const Vertex* V2 = &s.vb[i2];
-        p0 = mat_mul_point(o2w, V(V0->position[0], V0->position[1], V0->position[2]), 1.0f);
-        p1 = mat_mul_point(o2w, V(V1->position[0], V1->position[1], V1->position[2]), 1.0f);
-        p2 = mat_mul_point(o2w, V(V2->position[0], V2->position[1], V2->position[2]), 1.0f);
-        n0 = mat_mul_dir3(nrm, unpack_normal(V0->normal));
-        n1 = mat_mul_dir3(nrm, unpack_normal(V1->normal));
-        n2 = mat_mul_dir3(nrm, unpack_normal(V2->normal));
-        unpack_uv(V0->uv, uv0[0], uv0[1]);
-        unpack_uv(V1->uv, uv1[0], uv1[1]);
-        unpack_uv(V2->uv, uv2[0], uv2[1]);
+    const uint32_t leaf = hit.primId;
+    if (leaf >= s.numRec) {
+        raise_status(s, STRELKA_DEV_NODE_OOB);
+        return false;
     }
+    const float4* r = &s.shadeRec[6 * (size_t)leaf];
+    const float4 a0 = __ldg(r), a1 = __ldg(r + 1), a2 = __ldg(r + 2), a3 = __ldg(r + 3), a4 = __ldg(r + 4), a5 = __ldg(r + 5);
+    const v3 p0 = xyz(a0), p1 = xyz(a1), p2 = xyz(a2);
+    const v3 n0 = xyz(a3), n1 = xyz(a4), n2 = xyz(a5);
+    const float uv0[2] = {a0.w, a1.w}, uv1[2] = {a2.w, a3.w}, uv2[2] = {a4.w, a5.w};
     v3 geomNormal = vnormalize(vcross(vsub(p1, p0), vsub(p2, p0)));
     const float bx = hit.u, by = hit.v;
     v3 worldPosition = interp3(p0, p1, p2, bx, by);

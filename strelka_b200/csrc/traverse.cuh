@@ -25,7 +25,7 @@ struct DevScene {
     const float4* rec;    // 3 float4 per leaf, at the leaf's compact index
     const uint32_t* leafOf;  // per node: its compact leaf index (leaves only)
     uint32_t numRec;      // capacity of `rec` in leaves
-    const float4* shadeRec;  // 6 float4 per leaf at its compact index (shading vertex data), or null
+    const float4* shadeRec;  // 6 float4 per leaf at its compact index: shading vertex data (k_prep_shade)
     const float4* wide;   // 8 float4 per 4-wide node (see below)
     uint32_t numWide;     // capacity of `wide` in nodes
     uint32_t numNodes;
@@ -940,7 +940,9 @@ __device__ __forceinline__ bool any_step(const DevScene& s, Trav& T, STK& st, ui
     }
 }
 
-template <bool COUNT>
+// LEAF_REF: the record's primId holds the hit's compact leaf index instead
+// (for shade(), which reads the leaf's shading record).
+template <bool COUNT, bool LEAF_REF = false>
 __device__ __forceinline__ bool trace_closest_rec(const DevScene& s, v3 o, float tmax, v3 d, HitRec& hit, uint32_t& nInner,
                                                   uint32_t& nLeaf)
 {
@@ -951,6 +953,7 @@ __device__ __forceinline__ bool trace_closest_rec(const DevScene& s, v3 o, float
         while (!closest_step<COUNT>(s, T, st, nInner, nLeaf)) {
         }
     hit = T.hit;
+    if (LEAF_REF) hit.primId = T.leaf;
     return T.found;
 }
 
