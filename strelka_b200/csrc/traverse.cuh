@@ -200,6 +200,9 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, v3 o, float tmax, v
 //     depth-first node order (leafOf, an exclusive scan of the leaf flags);
 //   record table, 3 float4 per leaf at its compact index: the triangle
 //     [0] = v0 | instId  [1] = e0 | primId  [2] = e1 | 0;
+//   shading table, 6 float4 per leaf at its compact index: the triangle's
+//     world-space vertex positions and normals and its UVs (k_prep_shade;
+//     read by shade(), which receives the hit's compact leaf index);
 //   4-wide BVH, 8 float4 per node: the binary inner nodes at even depth of
 //     the reference's tree (children L = n+1 and R = escape(n+1), the
 //     implicit tree of the depth-first layout, bvh.cpp:182-220).  Node w:
@@ -232,7 +235,11 @@ __device__ __forceinline__ bool trace_any(const DevScene& s, v3 o, float tmax, v
 // reached.  A full stack falls back to the reference's stackless loop from
 // the root (closest: with the best hit so far).  tests/test_traversal_rule.py
 // checks the rule, replayed by the oracle, against the reference loop bit for
-// bit; tests/test_gpu_trace.py checks the kernels against both.
+// bit; tests/test_gpu_trace.py checks the kernels against both.  The
+// ray-query kernels and the large-scene wavefront passes run closest hit with
+// its leaf tests deferred across the warp (closest_defer_*, below) and keep
+// the top of each stack in shared memory (SplitStack); the results are the
+// same.
 // ===========================================================================
 
 namespace sb {
