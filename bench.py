@@ -522,12 +522,12 @@ def nrc_study(args, hs, ds) -> dict:
 
     lo, hi = hs.bounds()
     trials = []
-    kernel_ms = None
     clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
     # one renderer for every trial, its buffers allocated by an untimed frame
-    # with a throwaway cache (as the plain renderer had warm-up frames)
-    pt = PathTracer(mode=abi.MODE_WAVEFRONT, profile=True)
+    # with a throwaway cache (as the plain renderer had warm-up frames); it
+    # records no per-kernel events, like the plain renderer
+    pt = PathTracer(mode=abi.MODE_WAVEFRONT)
     scratch_cache = RadianceCache(lo, hi, learning_rate=args.nrc_lr, seed=99, log2_table_size=args.nrc_log2t)
     pt.set_nrc(scratch_cache, train_paths=args.nrc_train_paths, train_steps=args.nrc_train_steps,
                diffuse_roughness=args.nrc_diffuse_roughness)
@@ -540,7 +540,6 @@ def nrc_study(args, hs, ds) -> dict:
         pt.set_nrc(cache, train_paths=args.nrc_train_paths, train_steps=args.nrc_train_steps,
                    diffuse_roughness=args.nrc_diffuse_roughness)
         torch.cuda.synchronize()
-        pt.kernel_times(stream)
         base = 100_000 * (trial + 1)
         t_nrc = 0.0
         # warm-up: training only (training paths + Adam steps), no image;
@@ -573,9 +572,6 @@ def nrc_study(args, hs, ds) -> dict:
             if below >= 2:
                 reached = (k + 1) * args.nrc_spp
                 break
-        times = pt.kernel_times(stream)
-        if kernel_ms is None:
-            kernel_ms = {k: v[0] / max(len(frames_ms), 1) for k, v in times.items() if v[1]}
         st |= pt.device_status()
         pt.set_nrc(None)
         cache.close()
@@ -586,6 +582,26 @@ def nrc_study(args, hs, ds) -> dict:
                        "curve_spp_relmse_ms": curve})
     clk = clocks.stop()
     pt.close()
+    # per-kernel times of cached frames, from a separate profiling renderer
+    # (untimed): the first trial's warm-up and four frames with a fresh cache
+    ptp = PathTracer(mode=abi.MODE_WAVEFRONT, profile=True)
+    cache = RadianceCache(lo, hi, learning_rate=args.nrc_lr, seed=1, log2_table_size=args.nrc_log2t)
+    ptp.set_nrc(cache, train_paths=args.nrc_train_paths, train_steps=args.nrc_train_steps,
+                diffuse_roughness=args.nrc_diffuse_roughness)
+    for k in range(0, args.nrc_warmup, args.nrc_warmup_group):
+        nb = min(args.nrc_warmup_group, args.nrc_warmup - k)
+        ptp.train_nrc(ds.desc(hs.param(spp=args.nrc_spp, frameNumber=100_000 + k), sb), 100_000 + k, nb, stream)
+    render(ptp, 99, args.nrc_spp)
+    torch.cuda.synchronize()
+    ptp.kernel_times(stream)
+    for k in range(4):
+        render(ptp, 150_000 + k, args.nrc_spp)
+    times = ptp.kernel_times(stream)
+    kernel_ms = {k: v[0] / 4 for k, v in times.items() if v[1]}
+    st |= ptp.device_status()
+    ptp.set_nrc(None)
+    cache.close()
+    ptp.close()
     scratch_cache.close()
     if st != 0:
         raise RuntimeError(f"device status {st:#x}")
@@ -610,7 +626,7 @@ def nrc_study(args, hs, ds) -> dict:
                    "diffuse_roughness": args.nrc_diffuse_roughness, "learning_rate": args.nrc_lr,
                    "relmse": "mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)"},
         "plain": {"relmse": target, "relmse_frames": plain_err, "ms": t_plain},
-        "trials": trials, "kernel_ms_per_frame_first_trial": kernel_ms,
+        "trials": trials, "kernel_ms_per_frame_profiled": kernel_ms,
         "reference_seconds": ref_s, "clocks": clk,
     }
 

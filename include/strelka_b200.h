@@ -327,7 +327,8 @@ typedef struct StrelkaPathTracerConfig {
 enum {
     STRELKA_PT_PROFILE = 1u << 0,       /* record per-kernel CUDA events (strelka_pathtracer_get_kernel_times) */
     STRELKA_PT_COUNT = 1u << 1,         /* count traversal visits (strelka_pathtracer_get_counters) */
-    STRELKA_PT_NO_SHADE_SORT = 1u << 2, /* wavefront: shade paths in queue order, not sorted by material */
+    STRELKA_PT_NO_SHADE_SORT = 1u << 2, /* wavefront: shade paths in queue order, not sorted by material
+                                           (frames with the radiance cache are never sorted) */
     /* wavefront traversal variants (default: by tree size, STRELKA_LARGE_SCENE_NODES): the large-scene
        variants keep the top of each traversal stack in shared memory and defer the leaf tests of
        bounces >= 1 across the warp; the small-scene ones leave L1 to the scene.  Same results. */

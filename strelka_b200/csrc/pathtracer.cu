@@ -1549,9 +1549,12 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
         SB_CUDA_TRY(cudaEventCreateWithFlags(&pt->shadowDone, cudaEventDisableTiming));
     }
 #endif
-    // shade-queue sort by material: one key per material + miss + light/invalid
+    // shade-queue sort by material: one key per material + miss + light/invalid.
+    // Not with the radiance cache: its paths end at the first diffuse-ish
+    // vertex, so the queues of bounces >= 1 are short and sorting them costs
+    // more than it saves (time to the plain relMSE 0.411 -> 0.407 x plain).
     uint32_t sortKeys = 0;
-    if (!(pt->cfg.flags & STRELKA_PT_NO_SHADE_SORT) && s.numMaterials + 2 <= kMaxSortKeys) {
+    if (!(pt->cfg.flags & STRELKA_PT_NO_SHADE_SORT) && !useNrc && s.numMaterials + 2 <= kMaxSortKeys) {
         sortKeys = s.numMaterials + 2;
         if (!pt->sortHist) {
             SB_CUDA_TRY(cudaMalloc(&pt->sortHist, kMaxSortKeys * sizeof(uint32_t)));
