@@ -978,7 +978,28 @@ def main():
     achieved = bytes_alg / (ext_ms * 1e-3) / 1e9 if ext_ms > 0 else None
     sh_ms, sh_launches = times["shadow"]
     sh_bytes = WIDE_NODE_BYTES * cnt["shadow_inner"] + 48 * cnt["shadow_leaf"] + 64 * cnt["shadow_rays"]
-    sh_achieved = sh_bytes / (sh_ms * 1e-3) / 1e9 if sh_ms > 0 else None
+    sh_overlapped = sh_bytes / (sh_ms * 1e-3) / 1e9 if sh_ms > 0 else None
+    # the shadow kernel alone: the timed frames again (same samples, so the
+    # same visit counts) with each bounce's shadow queries on the frame's
+    # stream after its shading, every launch timed by CUDA events
+    pt_serial = PathTracer(mode=mode, chunk_paths=args.chunk, profile=True, serial_shadow=True)
+    pt_serial.execute(ds.desc(frame_param(args.warmup), sb), local_total, 1, 0, stream)  # scene tables, warm-up
+    torch.cuda.synchronize()
+    pt_serial.kernel_times(stream)
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for k in range(args.steps):
+        pt_serial.execute(ds.desc(frame_param(args.warmup + k), sb), local_total, 1, 0, stream)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    serial_frame_ms = s0.elapsed_time(s1) / args.steps
+    sh_alone_ms, sh_alone_launches = pt_serial.kernel_times(stream)["shadow"]
+    st = pt_serial.device_status()
+    pt_serial.close()
+    if st != 0:
+        raise RuntimeError(f"device status {st:#x}")
+    sh_achieved = sh_bytes / (sh_alone_ms * 1e-3) / 1e9 if sh_alone_ms > 0 else None
 
     # ---- end to end through the C ABI: host param in, tonemapped RGBA8 out ---
     out_img = tmimg if split else rgba8
@@ -1059,10 +1080,15 @@ def main():
                             "achieved": sh_achieved, "peak": peak, "unit": "GB/s",
                             "frac": (sh_achieved / peak) if sh_achieved else None,
                             "bytes_alg_per_launch": sh_bytes / max(sh_launches, 1),
+                            "kernel_ms_alone": sh_alone_ms, "kernel_launches_alone": sh_alone_launches,
+                            "frame_ms_serial": serial_frame_ms,
+                            "frac_overlapped": (sh_overlapped / peak) if sh_overlapped else None,
                             "kernel_ms_timed_region": sh_ms, "kernel_launches_timed_region": sh_launches,
-                            "note": "112 B per 4-wide node + 48 B per triangle test + 64 B request per query; "
-                                    "the kernel runs on the second stream beside the next bounce's extend, so its "
-                                    "duration includes SM time shared with that kernel"},
+                            "note": "112 B per 4-wide node + 48 B per triangle test + 64 B request per query. frac: "
+                                    "the timed frames replayed with each bounce's shadow launch alone on the "
+                                    "frame's stream (frame_ms_serial per frame), CUDA events per launch; "
+                                    "frac_overlapped: the timed region's event intervals, where the kernel runs on "
+                                    "a second stream beside the next bounce's extend and shares its SMs"},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": param_bytes,
                 "d2h_bytes_per_step": out_img.numel() * out_img.element_size()},

@@ -333,7 +333,11 @@ enum {
        variants keep the top of each traversal stack in shared memory and defer the leaf tests of
        bounces >= 1 across the warp; the small-scene ones leave L1 to the scene.  Same results. */
     STRELKA_PT_LARGE_SCENE_KERNELS = 1u << 3, /* always the large-scene variants */
-    STRELKA_PT_SMALL_SCENE_KERNELS = 1u << 4  /* always the small-scene variants */
+    STRELKA_PT_SMALL_SCENE_KERNELS = 1u << 4, /* always the small-scene variants */
+    STRELKA_PT_SERIAL_SHADOW = 1u << 5        /* wavefront: each bounce's shadow queries run on the caller's
+                                                 stream after its shading, not on a second stream beside the
+                                                 next bounce's closest-hit queries (same results; lets the
+                                                 shadow kernel be timed alone) */
 };
 
 /* BVH nodes from which the wavefront passes use their large-scene variants. */

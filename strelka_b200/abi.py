@@ -51,6 +51,7 @@ PT_COUNT = 2
 PT_NO_SHADE_SORT = 4
 PT_LARGE_SCENE_KERNELS = 8
 PT_SMALL_SCENE_KERNELS = 16
+PT_SERIAL_SHADOW = 32
 LARGE_SCENE_NODES = 1 << 21
 
 TRACE_CLOSEST = 0

@@ -1542,13 +1542,14 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
     if (rc) return rc;
     const int maxDepth = (int)ubo.maxDepth;
     const uint32_t qchunk = pt->cfg.queueChunk ? pt->cfg.queueChunk : kDefaultQueueChunk;
-#if SB_OVERLAP_SHADOW
-    if (!pt->aux) {
+    // shadow(k) beside extend(k+1) on the auxiliary stream, unless the
+    // caller asked for the serial order
+    const bool overlap = SB_OVERLAP_SHADOW && !(pt->cfg.flags & STRELKA_PT_SERIAL_SHADOW);
+    if (overlap && !pt->aux) {
         SB_CUDA_TRY(cudaStreamCreateWithFlags(&pt->aux, cudaStreamNonBlocking));
         SB_CUDA_TRY(cudaEventCreateWithFlags(&pt->shadeDone, cudaEventDisableTiming));
         SB_CUDA_TRY(cudaEventCreateWithFlags(&pt->shadowDone, cudaEventDisableTiming));
     }
-#endif
     // shade-queue sort by material: one key per material + miss + light/invalid.
     // Not with the radiance cache: its paths end at the first diffuse-ish
     // vertex, so the queues of bounces >= 1 are short and sorting them costs
@@ -1632,9 +1633,7 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
                                                              pt->main.sorted);
                 order = pt->main.sorted;
             }
-#if SB_OVERLAP_SHADOW
             if (pendingShadow) SB_CUDA_TRY(cudaStreamWaitEvent(st, pt->shadowDone, 0));
-#endif
             {
                 Timer t(pt, KC_SHADE, st);
                 if (useNrc)
@@ -1645,11 +1644,11 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
             // shadow(k) runs on the auxiliary stream beside extend(k+1): both
             // read only shade(k)'s outputs; shade(k+1) waits for both
             cudaStream_t sst = st;
-#if SB_OVERLAP_SHADOW
-            SB_CUDA_TRY(cudaEventRecord(pt->shadeDone, st));
-            SB_CUDA_TRY(cudaStreamWaitEvent(pt->aux, pt->shadeDone, 0));
-            sst = pt->aux;
-#endif
+            if (overlap) {
+                SB_CUDA_TRY(cudaEventRecord(pt->shadeDone, st));
+                SB_CUDA_TRY(cudaStreamWaitEvent(pt->aux, pt->shadeDone, 0));
+                sst = pt->aux;
+            }
             {
                 Timer t(pt, KC_SHADOW, sst);
                 if (large_scene(pt, s)) {
@@ -1660,14 +1659,12 @@ extern "C" int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTrace
                     else k_shadow<false, false><<<gridW, kExtendBlock, 0, sst>>>(s, pt->main.w, qin, qchunk, nullptr);
                 }
             }
-#if SB_OVERLAP_SHADOW
-            SB_CUDA_TRY(cudaEventRecord(pt->shadowDone, pt->aux));
-            pendingShadow = true;
-#endif
+            if (overlap) {
+                SB_CUDA_TRY(cudaEventRecord(pt->shadowDone, pt->aux));
+                pendingShadow = true;
+            }
         }
-#if SB_OVERLAP_SHADOW
         if (pendingShadow) SB_CUDA_TRY(cudaStreamWaitEvent(st, pt->shadowDone, 0));
-#endif
         if (tailDepth < maxDepth) {
             Timer t(pt, KC_TAIL, st);
             const int gridE = std::min<int>((n + kExtendBlock - 1) / kExtendBlock, pt->tailGrid);

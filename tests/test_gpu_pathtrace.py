@@ -143,6 +143,30 @@ def test_scene_kernel_variants(cuda, cornell, variant):
         assert bits_equal_fraction(g, r) >= EXACT_BAR
 
 
+def test_serial_shadow_equals_overlapped(cuda):
+    # STRELKA_PT_SERIAL_SHADOW runs each bounce's shadow queries on the
+    # frame's stream instead of beside the next bounce's closest-hit queries:
+    # the same samples bit for bit, and the shadow launches are timed
+    s = scenes.large(width=48, height=32, instances=6, frequency=6, num_textures=2, tex_size=64, env_width=64,
+                     env_height=32, max_depth=8, spp=2, seed=6)
+    ds = DeviceScene(s)
+    p = s.param(frameNumber=5)
+    total = p.dimension[0] * p.dimension[1] * p.spp
+    out = []
+    for serial in (False, True):
+        sb = cuda.full((total * 3,), -7.0, dtype=cuda.float32, device="cuda")
+        pt = PathTracer(mode=abi.MODE_WAVEFRONT, chunk_paths=1111, profile=True, serial_shadow=serial)
+        pt.execute(ds.desc(p, sb), total, 1, 0)
+        cuda.cuda.synchronize()
+        times = pt.kernel_times()
+        assert pt.device_status() == 0
+        assert times["shadow"][1] > 0
+        pt.close()
+        out.append(sb.cpu().numpy())
+    assert np.array_equal(out[0].view(np.uint32), out[1].view(np.uint32))
+    assert bits_equal_fraction(out[1], oracle.pathtrace(oracle.SceneView(s), p)) >= EXACT_BAR
+
+
 def test_golden_fixture(cuda):
     # the fixture is the reference's own shader code compiled on the host
     # (tests/golden/make_golden.py); samples it leaves undefined are skipped
