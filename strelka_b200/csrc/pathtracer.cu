@@ -35,7 +35,12 @@ constexpr int kExtendBlock = 128;
 // 8, its any-hit pass and the ray-query kernels 16.
 constexpr int kExtendStackShared = 8;
 constexpr int kShadowStackShared = 16;
-constexpr int kTraceStackShared = 16;
+#ifndef SB_TRACE_STACK_SHARED_CLOSEST
+#define SB_TRACE_STACK_SHARED_CLOSEST 16
+#endif
+#ifndef SB_TRACE_STACK_SHARED_ANY
+#define SB_TRACE_STACK_SHARED_ANY 16
+#endif
 constexpr int kShadeBlock = 128;
 constexpr int kSmallBlock = 256;
 constexpr uint32_t kMaxSortKeys = 4096;
@@ -952,11 +957,19 @@ __global__ void __launch_bounds__(kNrcPathBlock) k_nrc_train_paths(DevScene s, P
 // Ray-query microbenchmark kernels.
 // Resident blocks asked of the ray-query kernel: 8 for closest hit and 9 for
 // any hit measured fastest on the 1M-triangle soup (few spills either way).
+#ifndef SB_TRACE_MINBLOCKS_CLOSEST
+#define SB_TRACE_MINBLOCKS_CLOSEST 8
+#endif
+#ifndef SB_TRACE_MINBLOCKS_ANY
+#define SB_TRACE_MINBLOCKS_ANY 9
+#endif
 template <bool ANY, bool COUNT, bool REFINE>
-__global__ void __launch_bounds__(kExtendBlock, ANY ? 9 : 8) k_trace(DevScene s, const float4* __restrict__ rays, Hit* __restrict__ hits,
-                                                        uint32_t n, uint32_t* head, uint32_t chunk,
-                                                        unsigned long long* counters)
+__global__ void __launch_bounds__(kExtendBlock, ANY ? SB_TRACE_MINBLOCKS_ANY : SB_TRACE_MINBLOCKS_CLOSEST)
+    k_trace(DevScene s, const float4* __restrict__ rays, Hit* __restrict__ hits, uint32_t n, uint32_t* head,
+            uint32_t chunk, unsigned long long* counters)
 {
+    // traversal stack entries kept in shared memory per thread
+    constexpr int kTraceStackShared = ANY ? SB_TRACE_STACK_SHARED_ANY : SB_TRACE_STACK_SHARED_CLOSEST;
     using Stack = std::conditional_t<ANY, SplitStackN<kExtendBlock, kTraceStackShared>,
                                      SplitStack<kExtendBlock, kTraceStackShared>>;
     __shared__ std::conditional_t<ANY, uint32_t, uint2> sStack[kTraceStackShared * kExtendBlock];
