@@ -301,9 +301,10 @@ def cornell_study(args, steps: int = 3, warmup: int = 1) -> dict:
     4, frameNumber = iteration, accumulated and tonemapped (ACESFitted) every
     iteration: PathTracer::execute then the fused reduce + accumulate +
     tonemap, as PtRender::drawFrame records them (ptrender.cpp:735-862).
-    One step is the whole 64-iteration sequence, timed with CUDA events.
-    The last step's accumulated and tonemapped images are compared with the
-    oracle's same chain."""
+    One step is the whole 64-iteration sequence, timed with CUDA events,
+    issued call by call (mpaths_s_stream) and replayed from a CUDA graph of
+    the same calls (mpaths_s).  The last step's accumulated and tonemapped
+    images are compared with the oracle's same chain."""
     import torch
 
     import oracle
@@ -324,27 +325,45 @@ def cornell_study(args, steps: int = 3, warmup: int = 1) -> dict:
     params = [s.param(spp=1, maxDepth=4, frameNumber=it, iteration=it, stratifiedSamplingType=0) for it in range(iters)]
     aps = [accumulation_param(W, H, it) for it in range(iters)]
 
-    def sequence():
+    def sequence(st):
         for it in range(iters):
-            pt.execute(ds.desc(params[it], sb), npx, 1, it, stream)
-            resolve(params[it], sb, tp, aps[it], acc[it % 2], acc[(it + 1) % 2], tm, None, stream)
+            pt.execute(ds.desc(params[it], sb), npx, 1, it, st)
+            resolve(params[it], sb, tp, aps[it], acc[it % 2], acc[(it + 1) % 2], tm, None, st)
+
+    def timed(run):
+        times = []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        return statistics.median(times)
 
     for _ in range(warmup):
-        sequence()
+        sequence(stream)
     torch.cuda.synchronize()
-    times = []
-    for _ in range(steps):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        sequence()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
+    ms_stream = timed(lambda: sequence(stream))
+    stream_acc = acc[iters % 2].clone()
+    # the same 64 iterations captured once into a CUDA graph (after the
+    # frames above, the calls allocate nothing and never synchronise) and
+    # replayed: the same kernels with the launch gaps between them removed
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    with torch.cuda.graph(graph, stream=side):
+        sequence(side)
+    for _ in range(warmup):
+        graph.replay()
+    torch.cuda.synchronize()
+    ms = timed(graph.replay)
     st = pt.device_status()
+    del graph
     pt.close()
     if st != 0:
         raise RuntimeError(f"device status {st:#x}")
-    ms = statistics.median(times)
+    if not torch.equal(acc[iters % 2].view(torch.int32), stream_acc.view(torch.int32)):
+        raise RuntimeError("the graph's accumulated image differs from the stream-ordered one")
     # the oracle's chain (pathtracerMdl.hlsl, reduction, accumulation, tonemap)
     t0 = time.perf_counter()
     view = oracle.SceneView(s)
@@ -360,7 +379,10 @@ def cornell_study(args, steps: int = 3, warmup: int = 1) -> dict:
     rel = float(np.mean((g_acc.astype(np.float64) - hist) ** 2 / (hist.astype(np.float64) ** 2 + 1e-2)))
     return {"workload": "Cornell box 512x512 (10,252 triangles), 1 spp x 64 iterations, depth 4, frameNumber = "
                         "iteration, accumulation + ACESFitted every iteration", "mode": args.mode,
-            "mpaths_s": npx * iters / (ms * 1e-3) / 1e6, "ms_per_64_iterations": ms, "steps": steps, "warmup": warmup,
+            "launch": "the 64 iterations captured once into a CUDA graph and replayed",
+            "mpaths_s": npx * iters / (ms * 1e-3) / 1e6, "ms_per_64_iterations": ms,
+            "mpaths_s_stream": npx * iters / (ms_stream * 1e-3) / 1e6, "ms_per_64_iterations_stream": ms_stream,
+            "steps": steps, "warmup": warmup,
             "parity": {"relmse_accumulated": rel,
                        "bit_exact_accumulated": float(np.mean(g_acc.view(np.uint32) == hist.view(np.uint32))),
                        "bit_exact_tonemapped": float(np.mean(g_tm.view(np.uint32) == o_tm.view(np.uint32))),

@@ -351,7 +351,10 @@ int strelka_pathtracer_create(const StrelkaPathTracerConfig* config, StrelkaPath
 int strelka_pathtracer_destroy(StrelkaPathTracer* pt);
 
 /* PathTracer::execute (src/render/pathtracer.cpp:50-59).  As in the reference,
- * w = W*H*spp threads of work and h = 1; writes desc->sampleBuffer. */
+ * w = W*H*spp threads of work and h = 1; writes desc->sampleBuffer.  The first
+ * call for a scene version and frame size allocates the pass's tables and
+ * path state; later calls allocate nothing and do not synchronise, so they
+ * can be captured into a CUDA graph (the descriptor is read at capture). */
 int strelka_pathtracer_execute(StrelkaPathTracer* pt, const PathTracerDesc* desc,
                                uint32_t w, uint32_t h, uint64_t frameIndex, void* stream);
 

@@ -167,6 +167,53 @@ def test_serial_shadow_equals_overlapped(cuda):
     assert bits_equal_fraction(out[1], oracle.pathtrace(oracle.SceneView(s), p)) >= EXACT_BAR
 
 
+def test_frames_captured_in_a_cuda_graph(cuda):
+    # once a frame of the scene and size has run, execute and resolve allocate
+    # nothing and never synchronise: a sequence of progressive frames
+    # (PtRender::drawFrame's path trace, reduce, accumulate, tonemap)
+    # captured into a CUDA graph and replayed gives the stream-ordered images
+    # bit for bit, the shadow pass's second stream included
+    from strelka_b200.render import accumulation_param, resolve, tonemap_param
+
+    W = H = 64
+    npx, iters = W * H, 4
+    s = scenes.cornell(W, H, sphere_levels=3)
+    ds = DeviceScene(s)
+    params = [s.param(spp=1, maxDepth=4, frameNumber=it, iteration=it) for it in range(iters)]
+    aps = [accumulation_param(W, H, it) for it in range(iters)]
+    tp = tonemap_param(W, H, 1)
+    pt = PathTracer(mode=abi.MODE_WAVEFRONT)
+    sb = cuda.zeros(npx * 3, dtype=cuda.float32, device="cuda")
+    acc = [cuda.zeros(npx * 4, dtype=cuda.float32, device="cuda") for _ in range(2)]
+    tm = cuda.zeros(npx * 4, dtype=cuda.float32, device="cuda")
+
+    def sequence(stream):
+        for it in range(iters):
+            pt.execute(ds.desc(params[it], sb), npx, 1, it, stream)
+            resolve(params[it], sb, tp, aps[it], acc[it % 2], acc[(it + 1) % 2], tm, None, stream)
+
+    main = cuda.cuda.current_stream()
+    sequence(main)
+    cuda.cuda.synchronize()
+    assert pt.device_status() == 0
+    ref_acc, ref_tm = acc[iters % 2].clone(), tm.clone()
+    g = cuda.cuda.CUDAGraph()
+    side = cuda.cuda.Stream()
+    with cuda.cuda.graph(g, stream=side):
+        sequence(side)
+    for a in acc:
+        a.zero_()
+    tm.fill_(-1.0)
+    g.replay()
+    g.replay()
+    cuda.cuda.synchronize()
+    assert pt.device_status() == 0
+    assert cuda.equal(acc[iters % 2].view(cuda.int32), ref_acc.view(cuda.int32))
+    assert cuda.equal(tm.view(cuda.int32), ref_tm.view(cuda.int32))
+    del g
+    pt.close()
+
+
 def test_golden_fixture(cuda):
     # the fixture is the reference's own shader code compiled on the host
     # (tests/golden/make_golden.py); samples it leaves undefined are skipped
