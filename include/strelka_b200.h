@@ -328,17 +328,25 @@ enum {
     STRELKA_PT_PROFILE = 1u << 0,       /* record per-kernel CUDA events (strelka_pathtracer_get_kernel_times) */
     STRELKA_PT_COUNT = 1u << 1,         /* count traversal visits (strelka_pathtracer_get_counters) */
     STRELKA_PT_NO_SHADE_SORT = 1u << 2, /* wavefront: shade paths in queue order, not sorted by material
-                                           (frames with the radiance cache are never sorted) */
+                                           (frames with the radiance cache are never sorted, nor, unless
+                                           STRELKA_PT_FORCE_SHADE_SORT is set, chunks of fewer than
+                                           STRELKA_SHADE_SORT_MIN_PATHS paths) */
     /* wavefront traversal variants (default: by tree size, STRELKA_LARGE_SCENE_NODES): the large-scene
        variants keep the top of each traversal stack in shared memory and defer the leaf tests of
        bounces >= 1 across the warp; the small-scene ones leave L1 to the scene.  Same results. */
     STRELKA_PT_LARGE_SCENE_KERNELS = 1u << 3, /* always the large-scene variants */
     STRELKA_PT_SMALL_SCENE_KERNELS = 1u << 4, /* always the small-scene variants */
-    STRELKA_PT_SERIAL_SHADOW = 1u << 5        /* wavefront: each bounce's shadow queries run on the caller's
+    STRELKA_PT_SERIAL_SHADOW = 1u << 5,       /* wavefront: each bounce's shadow queries run on the caller's
                                                  stream after its shading, not on a second stream beside the
                                                  next bounce's closest-hit queries (same results; lets the
                                                  shadow kernel be timed alone) */
+    STRELKA_PT_FORCE_SHADE_SORT = 1u << 6     /* wavefront: sort by material whatever the chunk's size */
 };
+
+/* Paths in flight from which the wavefront sorts each bounce's shade queue
+ * by material (below it the sort's three short launches per bounce cost more
+ * than the coherence they buy).  The samples are the same either way. */
+#define STRELKA_SHADE_SORT_MIN_PATHS (1u << 21)
 
 /* BVH nodes from which the wavefront passes use their large-scene variants. */
 #define STRELKA_LARGE_SCENE_NODES (1u << 21)

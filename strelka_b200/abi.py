@@ -52,6 +52,8 @@ PT_NO_SHADE_SORT = 4
 PT_LARGE_SCENE_KERNELS = 8
 PT_SMALL_SCENE_KERNELS = 16
 PT_SERIAL_SHADOW = 32
+PT_FORCE_SHADE_SORT = 64
+SHADE_SORT_MIN_PATHS = 1 << 21
 LARGE_SCENE_NODES = 1 << 21
 
 TRACE_CLOSEST = 0

@@ -185,13 +185,15 @@ class PathTracer:
     """PathTracer pass (include/render/pathtracer.h:33-50)."""
 
     def __init__(self, mode: int = abi.MODE_WAVEFRONT, chunk_paths: int = 0, profile: bool = False,
-                 count: bool = False, queue_chunk: int = 0, shade_sort: bool = True, tail_depth: int = 0,
+                 count: bool = False, queue_chunk: int = 0, shade_sort="auto", tail_depth: int = 0,
                  scene_kernels: str = "auto", serial_shadow: bool = False):
-        """scene_kernels: "auto" (by tree size), "large" or "small" (STRELKA_PT_*_SCENE_KERNELS).
+        """shade_sort: "auto" (by paths in flight, STRELKA_SHADE_SORT_MIN_PATHS), True (always,
+        STRELKA_PT_FORCE_SHADE_SORT) or False (never, STRELKA_PT_NO_SHADE_SORT).
+        scene_kernels: "auto" (by tree size), "large" or "small" (STRELKA_PT_*_SCENE_KERNELS).
         serial_shadow: shadow queries on the caller's stream after shading (STRELKA_PT_SERIAL_SHADOW)."""
         self.lib = abi.load()
         flags = ((abi.PT_PROFILE if profile else 0) | (abi.PT_COUNT if count else 0) |
-                 (0 if shade_sort else abi.PT_NO_SHADE_SORT) | (abi.PT_SERIAL_SHADOW if serial_shadow else 0) |
+                 {"auto": 0, True: abi.PT_FORCE_SHADE_SORT, False: abi.PT_NO_SHADE_SORT}[shade_sort] | (abi.PT_SERIAL_SHADOW if serial_shadow else 0) |
                  {"auto": 0, "large": abi.PT_LARGE_SCENE_KERNELS, "small": abi.PT_SMALL_SCENE_KERNELS}[scene_kernels])
         cfg = abi.StrelkaPathTracerConfig(mode, chunk_paths, 0, flags, queue_chunk, tail_depth)
         h = C.c_void_p()

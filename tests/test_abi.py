@@ -83,4 +83,6 @@ def test_pass_flags_match_header():
     assert c["STRELKA_PT_LARGE_SCENE_KERNELS"] == abi.PT_LARGE_SCENE_KERNELS
     assert c["STRELKA_PT_SMALL_SCENE_KERNELS"] == abi.PT_SMALL_SCENE_KERNELS
     assert c["STRELKA_PT_SERIAL_SHADOW"] == abi.PT_SERIAL_SHADOW
+    assert c["STRELKA_PT_FORCE_SHADE_SORT"] == abi.PT_FORCE_SHADE_SORT
+    assert c["STRELKA_SHADE_SORT_MIN_PATHS"] == abi.SHADE_SORT_MIN_PATHS
     assert c["STRELKA_LARGE_SCENE_NODES"] == abi.LARGE_SCENE_NODES

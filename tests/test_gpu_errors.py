@@ -115,6 +115,9 @@ def test_bad_execute_arguments(cuda, base):
     cfg = abi.StrelkaPathTracerConfig(abi.MODE_WAVEFRONT, 0, 0, abi.PT_LARGE_SCENE_KERNELS | abi.PT_SMALL_SCENE_KERNELS, 0, 0)
     h = C.c_void_p()
     assert pt.lib.strelka_pathtracer_create(C.byref(cfg), C.byref(h)) == abi.ERR_INVALID_ARGUMENT
+    # so do the two shade-sort overrides
+    cfg = abi.StrelkaPathTracerConfig(abi.MODE_WAVEFRONT, 0, 0, abi.PT_NO_SHADE_SORT | abi.PT_FORCE_SHADE_SORT, 0, 0)
+    assert pt.lib.strelka_pathtracer_create(C.byref(cfg), C.byref(h)) == abi.ERR_INVALID_ARGUMENT
 
 
 @pytest.mark.parametrize("arrive", [0, 1])

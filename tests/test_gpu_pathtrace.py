@@ -143,6 +143,28 @@ def test_scene_kernel_variants(cuda, cornell, variant):
         assert bits_equal_fraction(g, r) >= EXACT_BAR
 
 
+@pytest.mark.parametrize("sort", ["auto", True, False])
+def test_shade_sort_modes(cuda, sort):
+    # the material sort of the shade queue (by default only for chunks of
+    # STRELKA_SHADE_SORT_MIN_PATHS paths or more; forced here on a small
+    # frame of several materials) changes which lane shades a path, never its
+    # samples: every mode gives the oracle's samples bit for bit
+    s = scenes.large(width=48, height=32, instances=6, frequency=6, num_textures=2, tex_size=64, env_width=64,
+                     env_height=32, max_depth=8, spp=2, seed=7)
+    ds = DeviceScene(s)
+    p = s.param(frameNumber=4)
+    total = p.dimension[0] * p.dimension[1] * p.spp
+    sb = cuda.full((total * 3,), -7.0, dtype=cuda.float32, device="cuda")
+    pt = PathTracer(mode=abi.MODE_WAVEFRONT, profile=True, shade_sort=sort, tail_depth=100)
+    pt.execute(ds.desc(p, sb), total, 1, 0)
+    cuda.cuda.synchronize()
+    sorts = pt.kernel_times()["sort"][1]
+    assert pt.device_status() == 0
+    pt.close()
+    assert (sorts > 0) == (sort is True)
+    assert bits_equal_fraction(sb.cpu().numpy(), oracle.pathtrace(oracle.SceneView(s), p)) >= EXACT_BAR
+
+
 def test_serial_shadow_equals_overlapped(cuda):
     # STRELKA_PT_SERIAL_SHADOW runs each bounce's shadow queries on the
     # frame's stream instead of beside the next bounce's closest-hit queries:
