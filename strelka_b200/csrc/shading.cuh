@@ -707,8 +707,24 @@ __device__ __forceinline__ bool shade(const DevScene& s, const PathTracerParam& 
         }
         return false;
     }
+    // The instance's ids and the leaf's shading record do not depend on each
+    // other: all of them are requested before the light-id branch, so a
+    // shaded hit waits for one round of loads instead of two.
     const InstanceConstants* ic = &s.inst[hit.instId];
     const int32_t lightId = __ldg(&ic->lightId);
+    const int32_t materialId = __ldg(&ic->materialId);
+    const uint32_t leaf = hit.primId;
+    const bool recOk = leaf < s.numRec;
+    float4 a0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), a1 = a0, a2 = a0, a3 = a0, a4 = a0, a5 = a0;
+    if (recOk) {
+        const float4* r = &s.shadeRec[6 * (size_t)leaf];
+        a0 = __ldg(r);
+        a1 = __ldg(r + 1);
+        a2 = __ldg(r + 2);
+        a3 = __ldg(r + 3);
+        a4 = __ldg(r + 4);
+        a5 = __ldg(r + 5);
+    }
     if (lightId != -1 && (ps.depth == 0 || ps.specular)) {
         if ((uint32_t)lightId >= s.lightCapacity) { raise_status(s, STRELKA_DEV_LIGHT_OOB); return false; }
         const float4 lc = __ldg(&reinterpret_cast<const float4*>(&s.lights[lightId])[4]);  // color
@@ -717,13 +733,10 @@ __device__ __forceinline__ bool shade(const DevScene& s, const PathTracerParam& 
     }
     if (lightId != -1) return false;  // diffuse bounce reached an emitter (reference reads mdlMaterials[-1])
 
-    const uint32_t leaf = hit.primId;
-    if (leaf >= s.numRec) {
+    if (!recOk) {
         raise_status(s, STRELKA_DEV_NODE_OOB);
         return false;
     }
-    const float4* r = &s.shadeRec[6 * (size_t)leaf];
-    const float4 a0 = __ldg(r), a1 = __ldg(r + 1), a2 = __ldg(r + 2), a3 = __ldg(r + 3), a4 = __ldg(r + 4), a5 = __ldg(r + 5);
     const v3 p0 = xyz(a0), p1 = xyz(a1), p2 = xyz(a2);
     const v3 n0 = xyz(a3), n1 = xyz(a4), n2 = xyz(a5);
     const float uv0[2] = {a0.w, a1.w}, uv1[2] = {a2.w, a3.w}, uv2[2] = {a4.w, a5.w};
@@ -746,7 +759,7 @@ __device__ __forceinline__ bool shade(const DevScene& s, const PathTracerParam& 
     st.geom_normal = geomNormal;
     st.position = worldPosition;
     Mat m;
-    if (!load_material(s, __ldg(&ic->materialId), st, m)) {
+    if (!load_material(s, materialId, st, m)) {
         raise_status(s, STRELKA_DEV_MATERIAL_OOB);
         return false;
     }
