@@ -264,11 +264,34 @@ __device__ __forceinline__ float env_pdf(const StrelkaEnvMap& e, int texel, v3 d
     float texelSolidAngle = (SB_TWO_PI_F / (float)e.width) * (SB_PI_F / (float)e.height) * sinTheta;
     return pRow * pCol / texelSolidAngle;
 }
+// The index lo in [0, n) with cdf[lo] <= u < cdf[lo + 1] (lo = 0 below
+// cdf[1], n - 1 at or above cdf[n - 1]).  Both forms keep the invariant
+// "lo == 0 or cdf[lo] <= u, and hi == n or cdf[hi] > u" and stop at
+// hi == lo + 1, which for a non-decreasing CDF leaves one possible lo, so the
+// four-way form returns the binary search's index.  It compares u with three
+// cut points per level, loaded together: about half as many dependent loads
+// (11 instead of 19 for a 512-row marginal and a 1024-column row).
 __device__ __forceinline__ int upper_bound_cdf(const float* cdf, int n, float u)
 {
     int lo = 0, hi = n;
+    while (hi - lo > 4) {
+        const int step = (hi - lo) >> 2;
+        const int m1 = lo + step, m2 = m1 + step, m3 = m2 + step;
+        const float c1 = __ldg(&cdf[m1]), c2 = __ldg(&cdf[m2]), c3 = __ldg(&cdf[m3]);
+        if (c3 <= u) {
+            lo = m3;
+        } else if (c2 <= u) {
+            lo = m2;
+            hi = m3;
+        } else if (c1 <= u) {
+            lo = m1;
+            hi = m2;
+        } else {
+            hi = m1;
+        }
+    }
     while (lo + 1 < hi) {
-        int mid = (lo + hi) >> 1;
+        const int mid = (lo + hi) >> 1;
         if (__ldg(&cdf[mid]) <= u) lo = mid; else hi = mid;
     }
     return lo;
