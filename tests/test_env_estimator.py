@@ -1,0 +1,123 @@
+"""The environment light's estimator against its expectation computed
+independently by quadrature (CPU, the oracle's path tracer).
+
+Scene: one large Lambert quad of albedo a facing +y, lit only by a seeded
+piecewise-constant environment (64 x 32 texels, random radiance plus a bright
+patch), seen from above; maxDepth 2.  Every sample takes the path of
+pathTraceCameraRays (shaders/pathtracerMdl.hlsl:204-404) for one hit: a
+next-event sample of the environment and a cosine-sampled bounce that escapes
+to it, combined by the balance heuristic.  Nothing else is in the scene, so
+each sample is an independent estimate of
+
+    E = integral over the upper hemisphere of
+        a/pi * Le(w) * (c^2 p_L(w) + c p_B(w)) / (p_L(w) + p_B(w)) dw,
+
+c = cos(theta), p_B = (c + 1e-6)/pi (the sampled Lambert's pdf), p_L the
+environment's pdf (rows by the marginal CDF, columns by the row's CDF, over
+the texel's solid angle at sin(theta)).  The c^2 of the next-event term is
+the reference's: its radiance carries saturate(dot(N, L))
+(pathtracerMdl.hlsl:31-92) and the BSDF evaluation its own cosine.  The
+quadrature uses only the CDF tables and the texel radiances, not the
+sampler, so a sampler whose directions do not follow the pdf it reports, or
+a wrong MIS weight, moves the mean off E by many standard errors."""
+import ctypes as C
+
+import numpy as np
+
+import oracle
+from strelka_b200 import abi, scenes
+
+A = 0.7          # albedo
+EW, EH = 64, 32  # environment texels
+
+
+def _pack(fn, v):
+    arr = (C.c_float * len(v))(*v)
+    return getattr(abi.load(), fn)(arr)
+
+
+def _environment(seed):
+    rng = np.random.default_rng(seed)
+    env = np.zeros((EH, EW, 4), np.float32)
+    env[..., :3] = rng.uniform(0.05, 1.0, (EH, EW, 3)).astype(np.float32)
+    env[4:7, 20:24, :3] *= 40.0  # a bright patch above the horizon
+    env[..., 3] = 1.0
+    marg = np.zeros(EH + 1, np.float32)
+    cond = np.zeros(EH * (EW + 1), np.float32)
+    integral = C.c_float(0.0)
+    lib = abi.load()
+    assert lib.strelka_envmap_build_cdf_host(env.ctypes.data, EW, EH, marg.ctypes.data, cond.ctypes.data,
+                                             C.byref(integral)) == abi.OK
+    return env, marg, cond, float(integral.value)
+
+
+def _scene(seed):
+    S = 1000.0
+    pos = np.array([[-S, 0, -S], [-S, 0, S], [S, 0, S], [S, 0, -S]], np.float32)
+    vb = (abi.Vertex * 4)()
+    for i in range(4):
+        vb[i].position[:] = pos[i]
+        vb[i].normal = _pack("strelka_pack_normal", [0.0, 1.0, 0.0])
+        vb[i].tangent = _pack("strelka_pack_normal", [1.0, 0.0, 0.0])
+        vb[i].uv = _pack("strelka_pack_uv", [0.0, 0.0])
+    ib = np.array([0, 1, 2, 0, 2, 3], np.uint32)
+    inst = abi.InstanceConstants()
+    for m in (inst.objectToWorld, inst.worldToObject, inst.normalMatrix):
+        for k in range(4):
+            m.m[5 * k] = 1.0
+    inst.materialId, inst.indexOffset, inst.indexCount, inst.lightId = 0, 0, 6, -1
+    mat = abi.MdlMaterial(0, 0, abi.FN_LAMBERT, 0)
+    args = np.zeros(12, np.float32)
+    args[0:3] = A
+    args[3] = 1.0   # roughness
+    args[7] = 1.5   # ior
+    tri = pos[ib].reshape(-1, 3)
+    nodes = scenes.bvh_build(tri, np.zeros(6, np.uint32), np.repeat(np.arange(2, dtype=np.uint32), 3))
+    env, marg, cond, integral = _environment(seed)
+    hs = scenes.HostScene(
+        vb=np.frombuffer(bytes(vb), np.uint8).copy(), ib=ib,
+        instances=np.frombuffer(bytes(inst), np.uint8).copy(),
+        lights=np.zeros(112, np.uint8), num_lights=0,
+        materials=np.frombuffer(bytes(mat), np.uint8).copy(),
+        arg_block=args.view(np.uint8).copy(), resource_infos=np.zeros(16, np.uint8), textures=[],
+        env=env, env_marginal=marg, env_conditional=cond, env_integral=integral,
+        nodes=nodes, num_triangles=2, camera=abi.PathTracerParam())
+    return hs
+
+
+def _expectation(hs, sub=64):
+    """The integral above by the midpoint rule over each texel's rows (Le and
+    p_L do not vary with phi inside a texel)."""
+    env, marg, cond = hs.env, hs.env_marginal, hs.env_conditional.reshape(EH, EW + 1)
+    dphi = 2.0 * np.pi / EW
+    total = np.zeros(3)
+    for y in range(EH // 2):  # theta < pi/2
+        t = (y + (np.arange(sub) + 0.5) / sub) * np.pi / EH
+        dth = np.pi / EH / sub
+        c, s = np.cos(t), np.sin(t)
+        p_row = float(marg[y + 1]) - float(marg[y])
+        for x in range(EW):
+            p_col = float(cond[y, x + 1]) - float(cond[y, x])
+            p_l = p_row * p_col / ((2.0 * np.pi / EW) * (np.pi / EH) * s)
+            p_b = (c + 1e-6) / np.pi
+            w = (c * c * p_l + c * p_b) / (p_l + p_b)
+            total += env[y, x, :3].astype(np.float64) * (A / np.pi) * np.sum(w * s) * dth * dphi
+    return total
+
+
+def test_environment_estimator_matches_its_expectation():
+    hs = _scene(seed=3)
+    W = H = 64
+    spp = 32
+    p = hs.look_at(W, H, eye=(0.0, 10.0, 4.0), target=(0.0, 0.0, 0.0), fov_deg=40.0, spp=spp, maxDepth=2,
+                   numLights=0, frameNumber=1, stratifiedSamplingType=1)
+    samples = oracle.pathtrace(oracle.SceneView(hs), p).astype(np.float64).reshape(-1, 3)
+    n = samples.shape[0]
+    assert n == W * H * spp and np.isfinite(samples).all()
+    mean = samples.mean(0)
+    se = samples.std(0) / np.sqrt(n)
+    expect = _expectation(hs)
+    # 5 standard errors, plus 1e-4 relative for the 1e-6 in p_B and rounding
+    assert np.all(np.abs(mean - expect) <= 5.0 * se + 1e-4 * expect), (mean, expect, se)
+    # and the bound is tight enough to matter: a few percent of the value
+    assert np.all(5.0 * se < 0.03 * expect), (se, expect)
