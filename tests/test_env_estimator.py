@@ -51,7 +51,7 @@ def _environment(seed):
     return env, marg, cond, float(integral.value)
 
 
-def _scene(seed):
+def _scene(seed, fn=abi.FN_LAMBERT, base=(A, A, A), roughness=1.0):
     S = 1000.0
     pos = np.array([[-S, 0, -S], [-S, 0, S], [S, 0, S], [S, 0, -S]], np.float32)
     vb = (abi.Vertex * 4)()
@@ -66,10 +66,10 @@ def _scene(seed):
         for k in range(4):
             m.m[5 * k] = 1.0
     inst.materialId, inst.indexOffset, inst.indexCount, inst.lightId = 0, 0, 6, -1
-    mat = abi.MdlMaterial(0, 0, abi.FN_LAMBERT, 0)
-    args = np.zeros(12, np.float32)
-    args[0:3] = A
-    args[3] = 1.0   # roughness
+    mat = abi.MdlMaterial(0, 0, fn, 0)
+    args = np.zeros(12, np.float32)  # StrelkaMaterialArgs
+    args[0:3] = base
+    args[3] = roughness
     args[7] = 1.5   # ior
     tri = pos[ib].reshape(-1, 3)
     nodes = scenes.bvh_build(tri, np.zeros(6, np.uint32), np.repeat(np.arange(2, dtype=np.uint32), 3))
@@ -121,3 +121,72 @@ def test_environment_estimator_matches_its_expectation():
     assert np.all(np.abs(mean - expect) <= 5.0 * se + 1e-4 * expect), (mean, expect, se)
     # and the bound is tight enough to matter: a few percent of the value
     assert np.all(5.0 * se < 0.03 * expect), (se, expect)
+
+
+def _ggx_expectation(hs, k1, f0, roughness, sub=12):
+    """The GGX conductor's counterpart: next-event and sampled-reflection
+    terms of pathTraceCameraRays with the native conductor (D, Smith G from
+    G1, Schlick F; sampled half vectors with pdf D (n.h), reflected, so the
+    reported pdf D (n.h) / (4 v.h) is the density of the direction):
+
+        E = integral over n.l > 0 of Le f(v, l) (n.l) ((n.l) p_L + p_B) / (p_L + p_B) dl,
+        f = F D G / (4 (n.v)(n.l)).
+
+    Midpoint rule over sub x sub cells of every texel above the horizon."""
+    env, marg, cond = hs.env, hs.env_marginal, hs.env_conditional.reshape(EH, EW + 1)
+    alpha = max(roughness * roughness, 1e-3)
+    a2 = alpha * alpha
+    f0 = np.asarray(f0, np.float64)
+    nov = k1[1]
+
+    def g1(x):
+        return 2.0 * x / (x + np.sqrt(a2 + (1.0 - a2) * x * x))
+
+    total = np.zeros(3)
+    j = (np.arange(sub) + 0.5) / sub
+    for y in range(EH // 2):
+        t = (y + j[:, None]) * np.pi / EH                       # (sub, 1)
+        p_row = float(marg[y + 1]) - float(marg[y])
+        for x in range(EW):
+            ph = ((x + j[None, :]) / EW - 0.5) * 2.0 * np.pi     # (1, sub)
+            st, ct = np.sin(t), np.cos(t)
+            lx, ly, lz = st * np.sin(ph), ct + 0.0 * ph, -st * np.cos(ph)
+            hx, hy, hz = lx + k1[0], ly + k1[1], lz + k1[2]
+            hn = np.sqrt(hx * hx + hy * hy + hz * hz)
+            noh = np.clip(hy / hn, 0.0, 1.0)
+            voh = np.clip((hx * k1[0] + hy * k1[1] + hz * k1[2]) / hn, 0.0, 1.0)
+            nol = ly
+            tt = noh * noh * (a2 - 1.0) + 1.0
+            D = a2 / (np.pi * tt * tt)
+            G = g1(nov) * g1(nol)
+            w5 = np.clip(1.0 - voh, 0.0, 1.0) ** 5
+            p_col = float(cond[y, x + 1]) - float(cond[y, x])
+            p_l = p_row * p_col / ((2.0 * np.pi / EW) * (np.pi / EH) * st)
+            p_b = D * noh / (4.0 * voh)
+            common = D * G / (4.0 * nov) * (nol * p_l + p_b) / (p_l + p_b)  # f (n.l) without F, times the weights
+            dw = st * (np.pi / EH / sub) * (2.0 * np.pi / EW / sub)
+            for c in range(3):
+                F = f0[c] + (1.0 - f0[c]) * w5
+                total[c] += env[y, x, c] * np.sum(F * common * dw)
+    return total
+
+
+def test_ggx_conductor_estimator_matches_its_expectation():
+    # the native GGX conductor (parity against MDL is unpinned by
+    # construction): a far camera with a 0.5-degree field of view, so every
+    # sample sees the quad from nearly one direction v
+    f0, rough = (0.9, 0.6, 0.3), 0.6
+    hs = _scene(seed=5, fn=abi.FN_GGX_CONDUCTOR, base=f0, roughness=rough)
+    eye = np.array([0.0, 600.0, 800.0])
+    W = H = 64
+    spp = 32
+    p = hs.look_at(W, H, eye=tuple(eye), target=(0.0, 0.0, 0.0), fov_deg=0.5, spp=spp, maxDepth=2,
+                   numLights=0, frameNumber=2, stratifiedSamplingType=1)
+    samples = oracle.pathtrace(oracle.SceneView(hs), p).astype(np.float64).reshape(-1, 3)
+    n = samples.shape[0]
+    assert np.isfinite(samples).all()
+    mean = samples.mean(0)
+    se = samples.std(0) / np.sqrt(n)
+    expect = _ggx_expectation(hs, eye / np.linalg.norm(eye), f0, rough)
+    assert np.all(np.abs(mean - expect) <= 5.0 * se + 2e-3 * expect), (mean, expect, se)
+    assert np.all(5.0 * se < 0.05 * expect), (se, expect)
