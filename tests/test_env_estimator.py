@@ -190,3 +190,104 @@ def test_ggx_conductor_estimator_matches_its_expectation():
     expect = _ggx_expectation(hs, eye / np.linalg.norm(eye), f0, rough)
     assert np.all(np.abs(mean - expect) <= 5.0 * se + 2e-3 * expect), (mean, expect, se)
     assert np.all(5.0 * se < 0.05 * expect), (se, expect)
+
+
+def _fresnel_dielectric(c, eta):
+    sin2t = eta * eta * (1.0 - c * c)
+    cost = np.sqrt(np.clip(1.0 - sin2t, 0.0, 1.0))
+    rs = (c - eta * cost) / (c + eta * cost)
+    rp = (eta * c - cost) / (eta * c + cost)
+    return np.where(sin2t >= 1.0, 1.0, 0.5 * (rs * rs + rp * rp))
+
+
+def _env_texel_pdf(hs, d):
+    """Le and p_L of directions d (..., 3) as the miss and env_pdf read them."""
+    env, marg, cond = hs.env, hs.env_marginal, hs.env_conditional.reshape(EH, EW + 1)
+    u = np.arctan2(d[..., 0], -d[..., 2]) / (2.0 * np.pi) + 0.5
+    v = np.arccos(np.clip(d[..., 1], -1.0, 1.0)) / np.pi
+    x = np.clip((u * EW).astype(int), 0, EW - 1)
+    y = np.clip((v * EH).astype(int), 0, EH - 1)
+    st = np.sqrt(np.clip(1.0 - d[..., 1] ** 2, 0.0, 1.0))
+    p_l = ((marg[y + 1].astype(np.float64) - marg[y]) * (cond[y, x + 1].astype(np.float64) - cond[y, x])
+           / ((2.0 * np.pi / EW) * (np.pi / EH) * st))
+    return env[y, x, :3].astype(np.float64), p_l
+
+
+def _dielectric_expectation(hs, k1, tint, roughness, ior, n_theta=384, n_phi=768):
+    """The rough dielectric seen from outside (eta = 1 / ior):
+    reflection as the conductor with the dielectric's Fresnel and no tint
+    (evaluation and next-event sampling cover it), plus the transmitted
+    half: a half vector h drawn with pdf D (n.h), kept with probability
+    1 - F(v.h), the direction refracted through h (absorbed unless it goes
+    below the surface), weight tint G (v.h) / ((n.v)(n.h)), and the
+    environment below reached with the MIS weight of the pdf the sampler
+    reports, (1 - F) D (n.h), against p_L.  Both by the midpoint rule over
+    the half-vector hemisphere: E = sum over h of pdf(h) x value."""
+    alpha = max(roughness * roughness, 1e-3)
+    a2 = alpha * alpha
+    eta = 1.0 / ior
+    nov = k1[1]
+
+    def g1(x):
+        return 2.0 * x / (x + np.sqrt(a2 + (1.0 - a2) * x * x))
+
+    th = (np.arange(n_theta) + 0.5) / n_theta * (np.pi / 2)
+    ph = (np.arange(n_phi) + 0.5) / n_phi * (2.0 * np.pi)
+    T, P = np.meshgrid(th, ph, indexing="ij")
+    h = np.stack([np.sin(T) * np.cos(P), np.cos(T), np.sin(T) * np.sin(P)], -1)
+    dh = np.sin(T) * (np.pi / 2 / n_theta) * (2.0 * np.pi / n_phi)
+    noh = h[..., 1]
+    voh = h @ k1
+    tt = noh * noh * (a2 - 1.0) + 1.0
+    D = a2 / (np.pi * tt * tt)
+    pdf_h = D * noh * dh                         # probability of each cell
+    ok = voh > 0.0
+    F = _fresnel_dielectric(np.where(ok, voh, 1.0), eta)
+    total = np.zeros(3)
+    # reflection: k2 = 2 (v.h) h - v, kept when n.k2 > 0
+    k2 = 2.0 * voh[..., None] * h - k1
+    nol = k2[..., 1]
+    keep = ok & (nol > 0.0)
+    le, p_l = _env_texel_pdf(hs, k2)
+    G = g1(nov) * g1(np.where(keep, nol, 1.0))
+    w_b = G * voh / (nov * noh)                  # bsdf over pdf (F cancels the choice)
+    p_b = F * D * noh / (4.0 * np.where(ok, voh, 1.0))
+    bsdf_part = np.where(keep, F * w_b * p_b / (p_b + p_l), 0.0)          # sampled reflections
+    # next-event part, written over the same cells: f cos x cos x p_L / (p_L + p_B) per unit
+    # direction, and a direction cell is a half-vector cell times 4 (v.h)
+    nee_part = np.where(keep, F * D * G / (4.0 * nov) * nol * p_l / (p_l + p_b) * 4.0 * voh * dh, 0.0)
+    for c in range(3):
+        total[c] += np.sum(pdf_h * bsdf_part * le[..., c]) + np.sum(nee_part * le[..., c])
+    # transmission: refraction through h, kept when n.k2 < 0
+    sin2t = eta * eta * (1.0 - voh * voh)
+    c2 = np.sqrt(np.clip(1.0 - sin2t, 0.0, 1.0))
+    sc = eta * voh - c2
+    k2 = -eta * k1 + sc[..., None] * h
+    k2 = k2 / np.linalg.norm(k2, axis=-1, keepdims=True)
+    nol = k2[..., 1]
+    keep = ok & (nol < 0.0) & (sin2t < 1.0)
+    le, p_l = _env_texel_pdf(hs, k2)
+    G = g1(nov) * g1(np.where(keep, -nol, 1.0))
+    w_t = G * voh / (nov * noh)
+    p_rep = (1.0 - F) * D * noh
+    trans = np.where(keep, (1.0 - F) * w_t * p_rep / (p_rep + p_l), 0.0)
+    for c in range(3):
+        total[c] += np.sum(pdf_h * trans * tint[c] * le[..., c])
+    return total
+
+
+def test_ggx_dielectric_estimator_matches_its_expectation():
+    # the native rough dielectric from outside: reflected and transmitted
+    # halves, the latter escaping below the quad to the environment
+    tint, rough, ior = (0.9, 0.8, 0.7), 0.6, 1.5
+    hs = _scene(seed=6, fn=abi.FN_GGX_DIELECTRIC, base=tint, roughness=rough)
+    eye = np.array([0.0, 600.0, 800.0])
+    p = hs.look_at(64, 64, eye=tuple(eye), target=(0.0, 0.0, 0.0), fov_deg=0.5, spp=32, maxDepth=2,
+                   numLights=0, frameNumber=3, stratifiedSamplingType=1)
+    samples = oracle.pathtrace(oracle.SceneView(hs), p).astype(np.float64).reshape(-1, 3)
+    assert np.isfinite(samples).all()
+    mean = samples.mean(0)
+    se = samples.std(0) / np.sqrt(samples.shape[0])
+    expect = _dielectric_expectation(hs, eye / np.linalg.norm(eye), tint, rough, ior)
+    assert np.all(np.abs(mean - expect) <= 5.0 * se + 2e-3 * expect), (mean, expect, se)
+    assert np.all(5.0 * se < 0.05 * expect), (se, expect)
