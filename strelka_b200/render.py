@@ -193,7 +193,8 @@ class PathTracer:
         serial_shadow: shadow queries on the caller's stream after shading (STRELKA_PT_SERIAL_SHADOW)."""
         self.lib = abi.load()
         flags = ((abi.PT_PROFILE if profile else 0) | (abi.PT_COUNT if count else 0) |
-                 {"auto": 0, True: abi.PT_FORCE_SHADE_SORT, False: abi.PT_NO_SHADE_SORT}[shade_sort] | (abi.PT_SERIAL_SHADOW if serial_shadow else 0) |
+                 {"auto": 0, True: abi.PT_FORCE_SHADE_SORT, False: abi.PT_NO_SHADE_SORT}[shade_sort] |
+                 (abi.PT_SERIAL_SHADOW if serial_shadow else 0) |
                  {"auto": 0, "large": abi.PT_LARGE_SCENE_KERNELS, "small": abi.PT_SMALL_SCENE_KERNELS}[scene_kernels])
         cfg = abi.StrelkaPathTracerConfig(mode, chunk_paths, 0, flags, queue_chunk, tail_depth)
         h = C.c_void_p()
