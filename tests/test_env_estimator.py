@@ -51,7 +51,7 @@ def _environment(seed):
     return env, marg, cond, float(integral.value)
 
 
-def _scene(seed, fn=abi.FN_LAMBERT, base=(A, A, A), roughness=1.0):
+def _scene(seed, fn=abi.FN_LAMBERT, base=(A, A, A), roughness=1.0, environment=None):
     S = 1000.0
     pos = np.array([[-S, 0, -S], [-S, 0, S], [S, 0, S], [S, 0, -S]], np.float32)
     vb = (abi.Vertex * 4)()
@@ -73,7 +73,7 @@ def _scene(seed, fn=abi.FN_LAMBERT, base=(A, A, A), roughness=1.0):
     args[7] = 1.5   # ior
     tri = pos[ib].reshape(-1, 3)
     nodes = scenes.bvh_build(tri, np.zeros(6, np.uint32), np.repeat(np.arange(2, dtype=np.uint32), 3))
-    env, marg, cond, integral = _environment(seed)
+    env, marg, cond, integral = environment if environment is not None else _environment(seed)
     hs = scenes.HostScene(
         vb=np.frombuffer(bytes(vb), np.uint8).copy(), ib=ib,
         instances=np.frombuffer(bytes(inst), np.uint8).copy(),
@@ -291,3 +291,42 @@ def test_ggx_dielectric_estimator_matches_its_expectation():
     expect = _dielectric_expectation(hs, eye / np.linalg.norm(eye), tint, rough, ior)
     assert np.all(np.abs(mean - expect) <= 5.0 * se + 2e-3 * expect), (mean, expect, se)
     assert np.all(5.0 * se < 0.05 * expect), (se, expect)
+
+
+def _lambert_expectation(hs, sub=16):
+    """_expectation for an environment of any size, vectorised over columns."""
+    env = hs.env
+    eh, ew = env.shape[:2]
+    marg = hs.env_marginal.astype(np.float64)
+    cond = hs.env_conditional.reshape(eh, ew + 1).astype(np.float64)
+    p_col = cond[:, 1:] - cond[:, :-1]
+    dth, dphi = np.pi / eh / sub, 2.0 * np.pi / ew
+    total = np.zeros(3)
+    for y in range(eh // 2):
+        t = (y + (np.arange(sub) + 0.5) / sub) * np.pi / eh
+        c, s = np.cos(t), np.sin(t)
+        p_l = (marg[y + 1] - marg[y]) * p_col[y][:, None] / ((2.0 * np.pi / ew) * (np.pi / eh) * s[None, :])
+        p_b = (c + 1e-6) / np.pi
+        w = (c * c * p_l + c * p_b) / (p_l + p_b)
+        total += env[y, :, :3].astype(np.float64).T @ (w * s[None, :]).sum(1) * (A / np.pi) * dth * dphi
+    return total
+
+
+def test_environment_estimator_on_the_workload_environment():
+    # the large render's own 1024 x 512 environment with its sun lobe (the
+    # bench frame's only light), under the same Lambert quad
+    big = scenes.large(width=8, height=8, instances=1, frequency=2, num_textures=1, tex_size=16, env_width=1024,
+                       env_height=512, max_depth=2, spp=1, seed=0)
+    environment = (big.env, big.env_marginal, big.env_conditional, big.env_integral)
+    hs = _scene(seed=0, environment=environment)
+    p = hs.look_at(64, 64, eye=(0.0, 10.0, 4.0), target=(0.0, 0.0, 0.0), fov_deg=40.0, spp=32, maxDepth=2,
+                   numLights=0, frameNumber=7, stratifiedSamplingType=1)
+    samples = oracle.pathtrace(oracle.SceneView(hs), p).astype(np.float64).reshape(-1, 3)
+    assert np.isfinite(samples).all()
+    mean = samples.mean(0)
+    se = samples.std(0) / np.sqrt(samples.shape[0])
+    expect = _lambert_expectation(hs)
+    small = _scene(seed=3)
+    assert np.allclose(_lambert_expectation(small, sub=64), _expectation(small, sub=64), rtol=1e-9)
+    assert np.all(np.abs(mean - expect) <= 5.0 * se + 1e-4 * expect), (mean, expect, se)
+    assert np.all(5.0 * se < 0.03 * expect), (se, expect)
