@@ -330,3 +330,87 @@ def test_environment_estimator_on_the_workload_environment():
     assert np.allclose(_lambert_expectation(small, sub=64), _expectation(small, sub=64), rtol=1e-9)
     assert np.all(np.abs(mean - expect) <= 5.0 * se + 1e-4 * expect), (mean, expect, se)
     assert np.all(5.0 * se < 0.03 * expect), (se, expect)
+
+
+def _furnace(albedo, le):
+    """A closed box [-1, 1]^3 seen from inside: 12 inward-facing Lambert
+    triangles of the given albedo that also emit le, and a black environment
+    (present, so the loop of pathTraceCameraRays goes on past the first hit,
+    but contributing nothing)."""
+    faces = []
+    for axis in range(3):
+        for side in (-1.0, 1.0):
+            n = np.zeros(3)
+            n[axis] = -side                      # inward
+            u, v = [a for a in range(3) if a != axis]
+            quad = []
+            for cu, cv in ((-1, -1), (-1, 1), (1, 1), (1, -1)):
+                p = np.zeros(3)
+                p[axis], p[u], p[v] = side, cu, cv
+                quad.append(p)
+            for tri in ((0, 1, 2), (0, 2, 3)):
+                a, b, c = (quad[i] for i in tri)
+                if np.dot(np.cross(b - a, c - a), n) < 0:
+                    b, c = c, b
+                faces.append((a, b, c, n))
+    nv = 3 * len(faces)
+    vb = (abi.Vertex * nv)()
+    pos = np.zeros((nv, 3), np.float32)
+    for f, (a, b, c, n) in enumerate(faces):
+        for k, p in enumerate((a, b, c)):
+            i = 3 * f + k
+            pos[i] = p
+            vb[i].position[:] = p
+            vb[i].normal = _pack("strelka_pack_normal", list(n))
+            vb[i].tangent = _pack("strelka_pack_normal", list(np.roll(n, 1)))
+            vb[i].uv = _pack("strelka_pack_uv", [0.0, 0.0])
+    ib = np.arange(nv, dtype=np.uint32)
+    inst = abi.InstanceConstants()
+    for m in (inst.objectToWorld, inst.worldToObject, inst.normalMatrix):
+        for k in range(4):
+            m.m[5 * k] = 1.0
+    inst.materialId, inst.indexOffset, inst.indexCount, inst.lightId = 0, 0, nv, -1
+    mat = abi.MdlMaterial(0, 0, abi.FN_LAMBERT, 0)
+    args = np.zeros(12, np.float32)
+    args[0:3] = albedo
+    args[3] = 1.0
+    args[4:7] = le
+    args[7] = 1.5
+    prim = np.repeat(np.arange(len(faces), dtype=np.uint32), 3)
+    nodes = scenes.bvh_build(pos, np.zeros(nv, np.uint32), prim)
+    env = np.zeros((4, 8, 4), np.float32)
+    marg = np.zeros(5, np.float32)
+    cond = np.zeros(4 * 9, np.float32)
+    integral = C.c_float(0.0)
+    assert abi.load().strelka_envmap_build_cdf_host(env.ctypes.data, 8, 4, marg.ctypes.data, cond.ctypes.data,
+                                                    C.byref(integral)) == abi.OK
+    return scenes.HostScene(
+        vb=np.frombuffer(bytes(vb), np.uint8).copy(), ib=ib, instances=np.frombuffer(bytes(inst), np.uint8).copy(),
+        lights=np.zeros(112, np.uint8), num_lights=0, materials=np.frombuffer(bytes(mat), np.uint8).copy(),
+        arg_block=args.view(np.uint8).copy(), resource_infos=np.zeros(16, np.uint8), textures=[],
+        env=env, env_marginal=marg, env_conditional=cond, env_integral=float(integral.value),
+        nodes=nodes, num_triangles=len(faces), camera=abi.PathTracerParam())
+
+
+def test_white_furnace():
+    # every hit adds throughput * Le and every bounce multiplies the
+    # throughput by the albedo, so a path of maxDepth hits carries
+    # Le (1 - a^D) / (1 - a).  Without Russian roulette (D <= 4) that is
+    # every sample's value; with it (depth > 3, survival max(throughput),
+    # reweighted by 1 / (p + 1e-5)) it is the mean
+    albedo, le = (0.5, 0.7, 0.9), (1.0, 2.0, 0.5)
+    hs = _furnace(albedo, le)
+    view = oracle.SceneView(hs)
+    a, e = np.array(albedo), np.array(le)
+    for depth, spp in ((4, 4), (12, 32)):
+        p = hs.look_at(64, 64, eye=(0.1, 0.05, -0.2), target=(0.3, -0.2, 1.0), fov_deg=100.0, spp=spp,
+                       maxDepth=depth, numLights=0, frameNumber=depth, stratifiedSamplingType=1)
+        s = oracle.pathtrace(view, p).astype(np.float64).reshape(-1, 3)
+        expect = e * (1.0 - a ** depth) / (1.0 - a)
+        assert np.isfinite(s).all()
+        if depth <= 4:
+            assert np.allclose(s, expect, rtol=1e-5, atol=0.0), np.abs(s - expect).max(0)
+        else:
+            mean, se = s.mean(0), s.std(0) / np.sqrt(s.shape[0])
+            assert np.all(np.abs(mean - expect) <= 5.0 * se + 1e-4 * expect), (mean, expect, se)
+            assert np.all(5.0 * se < 0.02 * expect), (se, expect)
