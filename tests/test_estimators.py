@@ -1,7 +1,9 @@
-"""The environment light's estimator against its expectation computed
-independently by quadrature (CPU, the oracle's path tracer).
+"""The path tracer's estimators against expectations computed independently
+(CPU, the oracle's path tracer; the GPU kernels equal it bit for bit):
+the environment light under Lambert, GGX conductor and rough dielectric
+quads (quadrature), and a white furnace (closed form).
 
-Scene: one large Lambert quad of albedo a facing +y, lit only by a seeded
+Environment scenes: one large Lambert quad of albedo a facing +y, lit only by a seeded
 piecewise-constant environment (64 x 32 texels, random radiance plus a bright
 patch), seen from above; maxDepth 2.  Every sample takes the path of
 pathTraceCameraRays (shaders/pathtracerMdl.hlsl:204-404) for one hit: a
