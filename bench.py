@@ -130,10 +130,10 @@ class ClockSampler:
 
 def cpu_baseline(hs, args, budget_s: float, frame_number: int = 0):
     """Times the oracle (fast build, all host threads) on 64 evenly spaced,
-    non-overlapping runs of the frame's sample indices.  A first pass of 64
-    paths per run calibrates the rate; the timed pass then renders as many
-    paths per run as fit `budget_s`.  Returns (Mpaths/s, paths, threads,
-    seconds)."""
+    non-overlapping runs of the frame's sample indices.  Calibration passes
+    (64 paths per run, growing 4x until a pass takes a tenth of `budget_s`)
+    give the rate; the timed pass then renders as many paths per run as fit
+    `budget_s`.  Returns (Mpaths/s, paths, threads, seconds)."""
     import oracle
 
     view = oracle.SceneView(hs)
@@ -148,9 +148,17 @@ def cpu_baseline(hs, args, budget_s: float, frame_number: int = 0):
             oracle.pathtrace(view, p, threads=threads, first=(k * total) // slices, count=per, fast=True)
         return time.perf_counter() - t
 
-    cal = 64
-    rate = slices * cal / max(run(cal), 1e-6)
-    per = int(min(max(rate * budget_s / slices, cal), total // slices))
+    # calibration passes grow 4x until one takes a tenth of the budget: a
+    # short pass is mostly per-call overhead and would understate the rate
+    most = max(total // slices, 1)
+    per = min(64, most)
+    while True:
+        el = run(per)
+        if el >= 0.1 * budget_s or per >= most:
+            break
+        per = min(per * 4, most)
+    rate = slices * per / max(el, 1e-6)
+    per = int(min(max(rate * budget_s / slices, 64), most))
     el = run(per)
     done = slices * per
     return done / el / 1e6, done, threads, el
