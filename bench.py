@@ -128,12 +128,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(hs, args, budget_s: float, frame_number: int = 0):
+def cpu_baseline(hs, args, budget_s: float, frame_number: int = 0, per: int | None = None):
     """Times the oracle (fast build, all host threads) on 64 evenly spaced,
     non-overlapping runs of the frame's sample indices.  Calibration passes
     (64 paths per run, growing 4x until a pass takes a tenth of `budget_s`)
     give the rate; the timed pass then renders as many paths per run as fit
-    `budget_s`.  Returns (Mpaths/s, paths, threads, seconds)."""
+    `budget_s`.  `per` skips the calibration and renders that many paths per
+    run.  Returns (Mpaths/s, paths, threads, seconds)."""
     import oracle
 
     view = oracle.SceneView(hs)
@@ -148,17 +149,18 @@ def cpu_baseline(hs, args, budget_s: float, frame_number: int = 0):
             oracle.pathtrace(view, p, threads=threads, first=(k * total) // slices, count=per, fast=True)
         return time.perf_counter() - t
 
-    # calibration passes grow 4x until one takes a tenth of the budget: a
-    # short pass is mostly per-call overhead and would understate the rate
     most = max(total // slices, 1)
-    per = min(64, most)
-    while True:
-        el = run(per)
-        if el >= 0.1 * budget_s or per >= most:
-            break
-        per = min(per * 4, most)
-    rate = slices * per / max(el, 1e-6)
-    per = int(min(max(rate * budget_s / slices, 64), most))
+    if per is None:
+        # calibration passes grow 4x until one takes a tenth of the budget: a
+        # short pass is mostly per-call overhead and would understate the rate
+        per = min(64, most)
+        while True:
+            el = run(per)
+            if el >= 0.1 * budget_s or per >= most:
+                break
+            per = min(per * 4, most)
+        rate = slices * per / max(el, 1e-6)
+        per = int(min(max(rate * budget_s / slices, 64), most))
     el = run(per)
     done = slices * per
     return done / el / 1e6, done, threads, el
@@ -205,8 +207,10 @@ def run_reference(args):
     scenes.use_generator_library(oracle.workload())
     hs = make_scene(args)
     vals = []
+    per = None
     for step in range(args.warmup + args.steps):
-        v, n, threads, el = cpu_baseline(hs, args, budget_s=args.ref_step_seconds)
+        v, n, threads, el = cpu_baseline(hs, args, budget_s=args.ref_step_seconds, per=per)
+        per = n // 64  # the first step's calibrated size for every step
         if step >= args.warmup:
             vals.append((v, n, el))
     value = statistics.median(v for v, _, _ in vals)
